@@ -1,0 +1,249 @@
+/*
+ * fem_b200.h — C ABI of the B200 (sm_100a) matrix-free FEM solver path.
+ *
+ * Drop-in boundary for jax_fem_cfd's solver hot path. The reference has no
+ * FFI; its boundary is a set of Python callables (cited per entry point below,
+ * paths relative to the jax_fem_cfd project root). Each entry point here is the
+ * native implementation a binding (XLA FFI handler, ctypes, torch op) calls in
+ * place of the cited reference function.
+ *
+ * Conventions
+ *  - All array arguments are DEVICE pointers owned by the caller, FP64 unless
+ *    stated. Vector fields are stacked component-major [u; v; (w)] of length
+ *    ndim*nn, exactly as in the reference.
+ *  - Every call is asynchronous on the given stream and returns an int status:
+ *    FEM_OK or a negative FEM_E_* code for argument / CUDA errors detected at
+ *    launch. Solver outcomes (iterations, convergence flags) are written to
+ *    device memory (int32), like the reference's device-array iteration counts.
+ *  - Connectivity is implicit: meshes are the structured lattices of
+ *    setup/regular_mesh.py and kernels compute nconn on the fly.
+ *  - A context owns its mesh-resident data and solver workspace (allocated at
+ *    create / setup time, never on the solve path). One context is driven by
+ *    one stream at a time.
+ */
+#ifndef FEM_B200_H
+#define FEM_B200_H
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEM_OK 0
+#define FEM_E_ARG (-1)
+#define FEM_E_CUDA (-2)
+#define FEM_E_OOM (-3)
+#define FEM_E_STATE (-4)
+
+/* element families */
+#define FEM_KIND_Q1_2D 0 /* quad4  */
+#define FEM_KIND_Q2_2D 1 /* quad9  */
+#define FEM_KIND_HEX8 2  /* hex8   */
+/* shape-function families for fem_shape_functions */
+#define FEM_SHAPE_QUAD4 0
+#define FEM_SHAPE_QUAD9 1
+#define FEM_SHAPE_HEX8 2
+#define FEM_SHAPE_LIN2 3
+#define FEM_SHAPE_LIN3 4
+
+/* pressure preconditioners (solvers/standard.py:219-247) */
+#define FEM_PREC_NONE 0
+#define FEM_PREC_JACOBI 1
+#define FEM_PREC_APPROX_INV 2
+#define FEM_PREC_APPROX_INV_PT 3 /* passive_transport.py:409-418 variant */
+#define FEM_PREC_MG 4
+
+/* solver status bits written to the device status word */
+#define FEM_STATUS_BARRIER_TIMEOUT 1
+#define FEM_STATUS_NONFINITE 2
+#define FEM_STATUS_MAXITER 4
+#define FEM_STATUS_BREAKDOWN 8
+#define FEM_STATUS_WATCHDOG 32 /* a solve exceeded its 10 s device-side wall budget */
+
+typedef struct fem_mesh_desc {
+  int kind;     /* FEM_KIND_* */
+  int periodic; /* 2D only */
+  int nex, ney, nez;
+  double lx, ly, lz;
+} fem_mesh_desc;
+
+typedef struct fem_ctx fem_ctx;
+
+/* ---------------------------------------------------------------- mesh ---- */
+
+/* Node/element counts of a mesh (host only). */
+int fem_mesh_counts(const fem_mesh_desc* mesh, int* nn, int* ne, int* nen);
+
+/* Node coordinates (nn x dim) and connectivity (ne x nen, int64).
+ * Replaces setup/regular_mesh.py:6 create_mesh_2d, :46 create_mesh_3d,
+ * :108 create_mesh_2d_quad9, :150 create_periodic_mesh_2d,
+ * :183 create_periodic_mesh_2d_quad9. */
+int fem_mesh_generate(const fem_mesh_desc* mesh, double* node_coords, int64_t* nconn, cudaStream_t stream);
+
+/* Gauss-point data wq (q), N (q x I), Nderiv (q x dim x I) of one element
+ * with nodal coordinates coords (I x dim). Replaces core/shape_functions.py:11
+ * lin2, :27 quad4, :47 hex8, :89 lin3, :108 quad9 *_shape_functions. */
+int fem_shape_functions(int family, const double* coords, double* wq, double* N, double* Nderiv,
+                        cudaStream_t stream);
+
+/* ------------------------------------------------------------- context ---- */
+
+/* Create a context for a mesh: evaluates shape functions on element 0 and the
+ * shared element matrices Me, Le, Ge, the lumped mass M (ndim*nn) and diag(L)
+ * (core/element_calc.py:9 lumped_mass_matrix, :27 laplacian_element_calc,
+ * :34 gradient_element_calc, :99 laplacian_diag; solvers/standard.py:211-214),
+ * all on the device. */
+int fem_ctx_create(const fem_mesh_desc* mesh, int device, fem_ctx** out);
+void fem_ctx_destroy(fem_ctx* ctx);
+
+/* nn, ne, nen, ndim, nq of the context mesh (host). */
+int fem_ctx_dims(const fem_ctx* ctx, int* nn, int* ne, int* nen, int* ndim, int* nq);
+
+/* Copy the element data out (device pointers, any may be NULL):
+ * wq (nq), N (nq*nen), Nderiv (nq*ndim*nen), Me, Le (nen*nen), Ge (ndim*nen*nen),
+ * M_lumped (ndim*nn), L_diag (nn). */
+int fem_ctx_element_data(const fem_ctx* ctx, double* wq, double* N, double* Nderiv, double* Me, double* Le,
+                         double* Ge, double* M_lumped, double* L_diag, cudaStream_t stream);
+
+/* Boundary sets. dmask: uint8 (ndim*nn), 1 on gamma_d entries
+ * (setup/simulation.py:169-173). pmask: uint8 (nn), 1 on gamma_p nodes (outlet
+ * nodes, or node 0 when there is no outlet: setup/simulation.py:178-181).
+ * set_zeroP selects pinned (1) or mean-zero (0) pressure (StandardSolverConfig). */
+int fem_ctx_set_bc(fem_ctx* ctx, const uint8_t* dmask, const uint8_t* pmask, int set_zeroP, cudaStream_t stream);
+
+/* Multigrid hierarchy (core/multigrid.py:9-88): nlev levels obtained by halving
+ * nex, ney; level_pmasks is the concatenation over levels of the uint8 gamma_p
+ * masks of each level mesh (NULL: node 0 of every level). coarse_tol is the
+ * coarsest-level CG tolerance (the reference passes solver_tol). */
+int fem_ctx_setup_multigrid(fem_ctx* ctx, int nlev, const uint8_t* level_pmasks, double coarse_tol,
+                            cudaStream_t stream);
+
+/* Level metadata of the hierarchy: nn and full lattice extents per level. */
+int fem_ctx_level_info(const fem_ctx* ctx, int level, int* nn, int* nnx_full, int* nny_full, int* nex, int* ney);
+
+/* ---------------------------------------------------- element products ---- */
+
+/* y_c = sum_e P_e^T (alpha*A + beta*B_e (B_e^T if transB) + gamma*C_e) P_e x_c
+ * for c < ncomp (x_c = x + c*nn). A: shared nen x nen, B/C: per element
+ * (ne x nen x nen); any may be NULL. Covers core/element_mult.py:11
+ * consistent_mass_mult, :38 laplacian_element_mult, :79 visc_conv_mult,
+ * :106 stabilized_visc_conv_mult, :159 scalar_visc_conv_mult,
+ * :174 scalar_stabilized_visc_conv_mult, :190 scalar_consistent_mass_SUPG_mult. */
+int fem_ebe_apply(fem_ctx* ctx, int ncomp, const double* x, double* y, double alpha, const double* A, double beta,
+                  const double* B, int transB, double gamma, const double* C, cudaStream_t stream);
+
+/* y = [G_1 P; ...; G_ndim P] (core/element_mult.py:51 gradient_element_mult). */
+int fem_grad_apply(fem_ctx* ctx, const double* P, const double* Ge, double* y, cudaStream_t stream);
+
+/* y = sum_i G_i^T u_i (core/element_mult.py:133 divergence_element_mult). */
+int fem_div_apply(fem_ctx* ctx, const double* U, const double* Ge, double* y, cudaStream_t stream);
+
+/* Quadrature arguments: wq (q), N (q x I), Nderiv (q x dim x I) of the element
+ * (the reference evaluates them on element 0); NULL selects the context's own. */
+
+/* Ce (ne x nen x nen) from U (core/element_calc.py:165 conservative_convec_elem_calc). */
+int fem_convection_build(fem_ctx* ctx, const double* U, double beta, const double* wq, const double* N,
+                         const double* Nderiv, double* Ce, cudaStream_t stream);
+
+/* Ctau_tilde (ne x nen x nen) (core/element_calc.py:188 Ctau_tilde_elem_calc). */
+int fem_ctau_tilde_build(fem_ctx* ctx, const double* U, const double* wq, const double* N, const double* Nderiv,
+                         double* Ct, cudaStream_t stream);
+
+/* Per-element SUPG tau (core/element_calc.py:202 calculate_tau). */
+int fem_supg_tau(fem_ctx* ctx, const double* U, const double* Ce, const double* Ct, double D, double dt, double r,
+                 const double* N, double* tau, cudaStream_t stream);
+
+/* Shared element matrices from quadrature data (nq points, nen nodes, dim):
+ * Me = sum_q w N(x)N (core/element_calc.py:13), Le = sum_q w dN^T dN (:27-32),
+ * Ge[i] = sum_q w N (x) dN_i (:34-40). Any output may be NULL except scratch
+ * use: Le_off (nen x nen) receives Le with a zero diagonal (core/multigrid.py:66). */
+int fem_element_matrices(int nq, int nen, int dim, const double* wq, const double* N, const double* Nderiv,
+                         double* Me, double* Le, double* Le_off, double* Ge, cudaStream_t stream);
+
+/* Assembled diagonals on the context mesh: M = assemble(rowsum(Me)) tiled
+ * ndim times (core/element_calc.py:9-25) and L_diag = assemble(diag(Le))
+ * (:99-109). Me / Le may be NULL (skip that output). */
+int fem_assemble_diag(fem_ctx* ctx, const double* Me, const double* Le, int ndim, double* M, double* L_diag,
+                      cudaStream_t stream);
+
+/* ------------------------------------------------------------ multigrid ---- */
+
+/* Lattice-bilinear prolongation of xH on the (nnH_x, nnH_y) lattice to the
+ * (nnh_x, nnh_y) lattice; extents include the periodic duplicate row/column
+ * (core/multigrid.py:90 interpolation_operator). */
+int fem_lattice_interpolate(int nnH_x, int nnH_y, int nnh_x, int nnh_y, int periodic, const double* xH, double* xh,
+                            cudaStream_t stream);
+/* Restriction R = I^T (core/multigrid.py:142 restriction_operator). */
+int fem_lattice_restrict(int nnh_x, int nnh_y, int nnH_x, int nnH_y, int periodic, const double* xh, double* xH,
+                         cudaStream_t stream);
+/* z = one V-cycle applied to r (core/multigrid.py:231 v_cycle). */
+int fem_mg_vcycle(fem_ctx* ctx, const double* r, double* z, cudaStream_t stream);
+
+/* -------------------------------------------------------------- solvers ---- */
+
+/* Pressure Poisson solve by (P)CG on the context Laplacian, one persistent
+ * launch (solvers/standard.py:85 solve_pressure with utils/
+ * jax_iterative_solvers.py:214 cg). Pinned rows (set_zeroP) or mean-zero
+ * handling follow the context's boundary setup. center_rhs subtracts mean(b)
+ * first; post applies the final pin/mean fix of solve_pressure. x holds x0 on
+ * entry and the solution on exit. iters/status: device int32. */
+int fem_pressure_solve(fem_ctx* ctx, const double* b, double* x, double tol, double atol, int maxiter, int precond,
+                       int center_rhs, int post, int* iters, int* status, cudaStream_t stream);
+
+/* General EBE-operator BiCGSTAB (utils/jax_iterative_solvers.py:685 bicgstab)
+ * on A = alpha*Ash + beta*B_e + gamma*C_e with identity rows where mask != 0
+ * (solvers/standard.py:20-28 lhs_operator). ncomp components share the element
+ * matrices; mask (uint8, ncomp*nn) may be NULL. maxiter <= 0 selects the
+ * reference default 10*size. x holds x0 on entry, the solution on exit;
+ * iters is the reference's iteration count (negative on breakdown). */
+int fem_bicgstab_solve(fem_ctx* ctx, int ncomp, double alpha, const double* Ash, double beta, const double* B,
+                       double gamma, const double* C, const uint8_t* mask, const double* b, double* x, double tol,
+                       double atol, int maxiter, int* iters, int* status, cudaStream_t stream);
+
+/* One 4-step projection time step (solvers/standard.py:148 four_step_timestep
+ * as called by setup_solver.timestep_loaded :264): Ce(U_n), momentum
+ * BiCGSTAB, U*, pressure PCG, projection, Dirichlet values. U_d_full is the
+ * ndim*nn vector holding U_d on gamma_d entries; F_p (nn) and F (ndim*nn) may
+ * be NULL for zero. iters: device int32[2] = {U_iters, P_iters}. */
+int fem_step4(fem_ctx* ctx, const double* U_n, const double* P_n, double dt, double rho, double mu,
+              const double* U_d_full, const double* F_p, const double* F, double tol, int precond, double* U_out,
+              double* P_out, int* iters, int* status, cudaStream_t stream);
+
+/* Passive-scalar step after the NS step (solvers/passive_transport.py:64
+ * timestep, phi part :80-95): builds Ce(U_n, 1), Ce(U, 1) and, with supg,
+ * Ctau_tilde/tau, then BiCGSTAB for phi. phi_mask (uint8 nn) / phi_d_full may
+ * be NULL. iters: device int32 (phi iterations). */
+int fem_transport_phi(fem_ctx* ctx, const double* U_n, const double* U, const double* phi_n, double dt, double D,
+                      int supg, const uint8_t* phi_mask, const double* phi_d_full, double tol, double* phi_out,
+                      int* iters, int* status, cudaStream_t stream);
+
+/* F_p = int_Gamma_d q (u_d . n) over the boundary edges/faces listed in bconn
+ * (nb x I, int32, I = 2 lin2, 3 lin3, 4 quad4 faces) with outward normals nvec
+ * (nb x dim) and Dirichlet values at their nodes U_b (ndim*nn, full vector)
+ * (core/element_calc.py:111 u_dot_n_boundary_integral_1d, :137 _2d). */
+int fem_boundary_flux(fem_ctx* ctx, const int32_t* bconn, const double* nvec, int nb, int nodes_per_face,
+                      const double* U_full, double* F_p, cudaStream_t stream);
+
+/* out[idx[k]] = vals[k] for k < n (idx int64; vals NULL writes `value`),
+ * the functional x.at[idx].set(v) of the reference. */
+int fem_scatter(const int64_t* idx, const double* vals, double value, int n, double* out, cudaStream_t stream);
+/* mask[idx[k]] = 1 for k < n (mask uint8, cleared to len first). */
+int fem_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cudaStream_t stream);
+
+/* Deterministic dot product and axpby helpers used by host-driven generic
+ * solver loops: out[0] = x . y (device), y = a*x + b*y. */
+int fem_dot(fem_ctx* ctx, const double* x, const double* y, int n, double* out, cudaStream_t stream);
+int fem_axpby(fem_ctx* ctx, double a, const double* x, double b, double* y, int n, cudaStream_t stream);
+
+/* Number of this library's kernel launches issued so far in this process. */
+long long fem_launch_count(void);
+
+/* Last CUDA error string recorded by the library (host, static storage). */
+const char* fem_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEM_B200_H */

@@ -1,0 +1,92 @@
+// Kernel argument structs and host launcher declarations of libfemb200.
+#pragma once
+#include <stdint.h>
+#include "fem_solvers.cuh"
+
+#define FEM_THREADS 512
+#define FEM_OP_THREADS 256
+
+struct BiArgs {
+  FemSync sync;
+  FemGrid g;
+  MatCombo op;
+  const uint8_t* mask;  // ncomp*nn identity rows, or null
+  const double* b;
+  double* x;
+  double *r, *rhat, *p0, *p1, *q0, *q1, *t;
+  double tol, atol;
+  int maxiter;
+  int* iters;
+  int* status;
+};
+
+struct StepArgs {
+  FemGrid g;
+  int ndim;
+  double dt, rho, mu, theta;
+  const double *Me, *Le, *Ge, *M;  // shared element matrices and lumped mass
+  const double* Ce;
+  const uint8_t* dmask;             // ndim*nn
+  const uint8_t* pmask;             // nn (pinned pressure)
+  int pinned;
+};
+
+
+// ----------------------------------------------------------------------------
+// Host launchers (one translation unit per kernel family; fem_capi.cu drives them)
+// ----------------------------------------------------------------------------
+int fem_after_launch(const char* what);  // records launch count / error; 0 or FEM_E_CUDA
+
+int fem_launch_mesh_generate(const FemGrid& g, double dx, double dy, double dz, double* coords, int64_t* nconn,
+                             cudaStream_t s);
+int fem_launch_shape_functions(int family, const double* coords, double* wq, double* N, double* dN, cudaStream_t s);
+int fem_launch_element_matrices(int nq, int nen, int dim, const double* wq, const double* N, const double* dN,
+                                double* Me, double* Le, double* Leoff, double* Ge, cudaStream_t s);
+int fem_launch_assemble_diag(const FemGrid& g, int ndim, const double* Me, const double* Le, double* M, double* Ldiag,
+                             cudaStream_t s);
+int fem_launch_level_sums(const FemGrid& g, const FemLattice& lat, const double* diag, double* out, cudaStream_t s);
+
+int fem_launch_ebe(int ncomp, const FemGrid& g, const MatCombo& m, const double* x, double* y, cudaStream_t s);
+int fem_launch_grad(int ndim, const FemGrid& g, const double* Ge, const double* P, double* y, cudaStream_t s);
+int fem_launch_div(int ndim, const FemGrid& g, const double* Ge, const double* U, double* y, cudaStream_t s);
+int fem_launch_convection(const FemGrid& g, const FemQuad& Q, const double* U, double beta, int mode, double* out,
+                          cudaStream_t s);
+int fem_launch_supg_tau(const FemGrid& g, const FemQuad& Q, const double* U, const double* Ce, const double* Ct,
+                        double D, double dt, double r, double* tau, cudaStream_t s);
+int fem_launch_scale_elem(int ne, int nen, const double* tau, const double* X, int trans, double* out, cudaStream_t s);
+int fem_launch_elem_combine(size_t n, double s_m, const double* Mt, double s_c, const double* C, const double* Ct,
+                            double* out, cudaStream_t s);
+int fem_launch_lincomb(int n, double a, const double* X, double b, const double* Y, double* out, cudaStream_t s);
+int fem_launch_interp(const FemLattice& H, const FemLattice& h, const double* xH, double* xh, cudaStream_t s);
+int fem_launch_restrict(const FemLattice& h, const FemLattice& H, const double* xh, double* xH, cudaStream_t s);
+int fem_launch_boundary(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
+                        const double* U, int nn, double* Fe, double* Fp, cudaStream_t s);
+int fem_launch_dot(const double* x, const double* y, int n, double* part, double* out, cudaStream_t s);
+int fem_launch_axpby(double a, const double* x, double b, double* y, int n, cudaStream_t s);
+int fem_launch_scatter(const int64_t* idx, const double* vals, double value, int n, double* out, cudaStream_t s);
+int fem_launch_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cudaStream_t s);
+
+int fem_coop_occupancy_cg(int* occ);
+int fem_coop_occupancy_bi(int* occ);
+int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s);
+int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s);
+int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s);
+
+int fem_launch_mom_rhs(const StepArgs& S, const double* Un, const double* Pn, const double* Ud, const double* F,
+                       double* rhs, double* x0, double* gPn, cudaStream_t s);
+int fem_launch_ustar(int n, double c, const double* Uh, const double* gPn, const double* M, double* Us,
+                     cudaStream_t s);
+int fem_launch_p_rhs(const StepArgs& S, const double* Us, const double* Fp, const double* Pn, double* rhs, double* x0,
+                     cudaStream_t s);
+int fem_launch_ufinal(const StepArgs& S, const double* Us, const double* P, const double* Ud, double* U,
+                      cudaStream_t s);
+int fem_launch_phi_rhs(const FemGrid& g, const double* Me, const double* Le, double dt, double D, const double* Mt,
+                       const double* Cn, const double* Ct, const double* phin, const uint8_t* mask,
+                       const double* phid, double* rhs, double* x0, cudaStream_t s);
+
+static inline int fem_nblocks(long long n, int threads, int cap = 148 * 16) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}

@@ -1,0 +1,816 @@
+// Host side of libfemb200: contexts, workspace, cooperative launches and the
+// extern "C" entry points declared in include/fem_b200.h.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "fem_b200.h"
+#include "fem_args.cuh"
+
+static std::atomic<long long> g_launches{0};
+static thread_local char g_err[256] = "";
+
+static int set_err(const char* where, cudaError_t e) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+  return FEM_E_CUDA;
+}
+#define FEM_CHECK(call)                             \
+  do {                                              \
+    cudaError_t _e = (call);                        \
+    if (_e != cudaSuccess) return set_err(#call, _e); \
+  } while (0)
+int fem_after_launch(const char* what) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(what, e);
+  return FEM_OK;
+}
+#define FEM_TRY(call)      \
+  do {                     \
+    int _rc = (call);      \
+    if (_rc) return _rc;   \
+  } while (0)
+
+static inline int nblocks(long long n, int threads, int cap = 148 * 16) { return fem_nblocks(n, threads, cap); }
+
+static bool make_grid(int kind, int periodic, int nex, int ney, int nez, FemGrid& g) {
+  if (nex < 1 || ney < 1) return false;
+  memset(&g, 0, sizeof(g));
+  g.kind = kind;
+  g.periodic = periodic ? 1 : 0;
+  g.nex = nex;
+  g.ney = ney;
+  g.nez = 1;
+  if (kind == FEM_Q1_2D) {
+    g.nnx = periodic ? nex : nex + 1;
+    g.nny = periodic ? ney : ney + 1;
+    g.nnz = 1;
+    g.nen = 4;
+  } else if (kind == FEM_Q2_2D) {
+    g.nnx = periodic ? 2 * nex : 2 * nex + 1;
+    g.nny = periodic ? 2 * ney : 2 * ney + 1;
+    g.nnz = 1;
+    g.nen = 9;
+  } else if (kind == FEM_HEX8) {
+    if (periodic || nez < 1) return false;
+    g.nez = nez;
+    g.nnx = nex + 1;
+    g.nny = ney + 1;
+    g.nnz = nez + 1;
+    g.nen = 8;
+  } else {
+    return false;
+  }
+  const long long nn = (long long)g.nnx * g.nny * g.nnz, ne = (long long)nex * ney * g.nez;
+  if (nn > (1LL << 31) - 1 || ne * g.nen > (1LL << 31) - 1) return false;
+  g.nn = (int)nn;
+  g.ne = (int)ne;
+  return true;
+}
+
+static FemLattice lattice_of(const FemGrid& g) {
+  FemLattice L;
+  const int s = (g.kind == FEM_Q2_2D) ? 2 : 1;
+  L.nx = s * g.nex + 1;
+  L.ny = s * g.ney + 1;
+  L.periodic = g.periodic;
+  return L;
+}
+
+struct CtxLevel {
+  FemGrid g;
+  double *Le = nullptr, *Leoff = nullptr, *diag = nullptr, *x = nullptr, *r = nullptr, *t = nullptr;
+  uint8_t* pin = nullptr;
+  double sum_invD = 0.0, sum_colw = 0.0;
+};
+
+struct fem_ctx {
+  int device = 0, sms = 148;
+  FemGrid g;
+  int ndim = 2, nq = 4;
+  double lx = 1, ly = 1, lz = 1;
+  // element data
+  double *coords = nullptr, *wq = nullptr, *N = nullptr, *dN = nullptr;
+  double *Me = nullptr, *Le = nullptr, *Leoff = nullptr, *Ge = nullptr, *M = nullptr, *Ldiag = nullptr;
+  double* Kd = nullptr;  // combined shared matrix of a solve (nen*nen)
+  // boundary sets
+  uint8_t *dmask = nullptr, *pmask = nullptr, *aipin = nullptr;
+  int has_dmask = 0, set_zeroP = 1;
+  // multigrid
+  int nlev = 0, block_from = 0;
+  double coarse_tol = 1e-8;
+  CtxLevel lv[FEM_MAX_LEVELS];
+  double *cr = nullptr, *cp = nullptr, *cq = nullptr;  // coarse CG scratch
+  // barrier / reduction state
+  unsigned int* bar = nullptr;
+  int* err = nullptr;
+  double* partials = nullptr;
+  int max_coop = 148;
+  // vectors (nn or ndim*nn)
+  double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pAp = nullptr, *pb = nullptr;  // CG
+  double *br = nullptr, *brh = nullptr, *bp0 = nullptr, *bp1 = nullptr, *bq0 = nullptr, *bq1 = nullptr,
+         *bt = nullptr;                                                                      // BiCGSTAB
+  double *rhsU = nullptr, *Uhat = nullptr, *gPn = nullptr, *Ustar = nullptr, *rhsP = nullptr;  // step
+  double *Ce = nullptr, *Ce2 = nullptr, *Ct = nullptr, *Mt = nullptr, *Ek = nullptr, *tau = nullptr;  // per element
+  double *dotpart = nullptr, *Fe = nullptr;
+  int Fe_cap = 0;
+  int* flags = nullptr;  // device scratch ints
+};
+
+template <class T>
+static int dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    set_err("cudaMalloc", e);
+    return FEM_E_OOM;
+  }
+  return FEM_OK;
+}
+#define FEM_ALLOC(p, n)                 \
+  do {                                  \
+    int _r = dalloc(&(p), (size_t)(n)); \
+    if (_r) return _r;                  \
+  } while (0)
+
+static int ctx_grid_for(const fem_ctx* c, long long work) {
+  // enough CTAs for ~1 node per thread, capped by co-residency
+  return nblocks(work, FEM_THREADS, c->max_coop);
+}
+
+// --------------------------------------------------------------- mesh ----
+
+extern "C" int fem_mesh_counts(const fem_mesh_desc* m, int* nn, int* ne, int* nen) {
+  if (!m) return FEM_E_ARG;
+  FemGrid g;
+  if (!make_grid(m->kind, m->periodic, m->nex, m->ney, m->nez, g)) return FEM_E_ARG;
+  if (nn) *nn = g.nn;
+  if (ne) *ne = g.ne;
+  if (nen) *nen = g.nen;
+  return FEM_OK;
+}
+
+static void spacings(const fem_mesh_desc* m, double& dx, double& dy, double& dz) {
+  dx = m->lx / m->nex;
+  dy = m->ly / m->ney;
+  dz = (m->kind == FEM_HEX8) ? m->lz / m->nez : 0.0;
+}
+
+extern "C" int fem_mesh_generate(const fem_mesh_desc* m, double* coords, int64_t* nconn, cudaStream_t s) {
+  if (!m || !coords) return FEM_E_ARG;
+  FemGrid g;
+  if (!make_grid(m->kind, m->periodic, m->nex, m->ney, m->nez, g)) return FEM_E_ARG;
+  double dx, dy, dz;
+  spacings(m, dx, dy, dz);
+  FEM_TRY(fem_launch_mesh_generate(g, dx, dy, dz, coords, nconn, s));
+  return FEM_OK;
+}
+
+extern "C" int fem_shape_functions(int family, const double* coords, double* wq, double* N, double* Nderiv,
+                                   cudaStream_t s) {
+  if (family < 0 || family > 4 || !coords || !wq || !N || !Nderiv) return FEM_E_ARG;
+  return fem_launch_shape_functions(family, coords, wq, N, Nderiv, s);
+}
+
+// element-0 coordinates of a structured mesh (host computed, tiny)
+static void elem0_coords(const FemGrid& g, double dx, double dy, double dz, double* out) {
+  const int s = (g.kind == FEM_Q2_2D) ? 2 : 1;
+  const int dim = (g.kind == FEM_HEX8) ? 3 : 2;
+  static const int q2i[9] = {0, 1, 2, 2, 2, 1, 0, 0, 1}, q2j[9] = {0, 0, 0, 1, 2, 2, 2, 1, 1};
+  static const int q1i[4] = {0, 1, 1, 0}, q1j[4] = {0, 0, 1, 1};
+  for (int a = 0; a < g.nen; ++a) {
+    int i, j, k;
+    if (g.kind == FEM_Q2_2D) {
+      i = q2i[a]; j = q2j[a]; k = 0;
+    } else {
+      i = q1i[a & 3]; j = q1j[a & 3]; k = a >> 2;
+    }
+    if (s == 2) {
+      out[a * dim + 0] = i * dx / 2;
+      out[a * dim + 1] = j * dy / 2;
+    } else {
+      out[a * dim + 0] = i * dx;
+      out[a * dim + 1] = j * dy;
+      if (dim == 3) out[a * 3 + 2] = k * dz;
+    }
+  }
+}
+
+// Element data of a grid: shape functions on element 0, Me, Le, Le_off, Ge, diag.
+static int element_setup(const FemGrid& g, double dx, double dy, double dz, double* tmp_coords, double* wq,
+                         double* N, double* dN, double* Me, double* Le, double* Leoff, double* Ge, double* M,
+                         double* Ldiag, int ndim, cudaStream_t s) {
+  double hc[27];
+  elem0_coords(g, dx, dy, dz, hc);
+  const int dim = (g.kind == FEM_HEX8) ? 3 : 2;
+  FEM_CHECK(cudaMemcpyAsync(tmp_coords, hc, sizeof(double) * g.nen * dim, cudaMemcpyHostToDevice, s));
+  const int family = g.kind == FEM_Q1_2D ? 0 : (g.kind == FEM_Q2_2D ? 1 : 2);
+  FEM_TRY(fem_launch_shape_functions(family, tmp_coords, wq, N, dN, s));
+  FEM_TRY(fem_launch_element_matrices(g.nen, g.nen, dim, wq, N, dN, Me, Le, Leoff, Ge, s));
+  FEM_TRY(fem_launch_assemble_diag(g, ndim, Me, Le, M, Ldiag, s));
+  // the copy source hc lives on this stack frame: finish before returning
+  FEM_CHECK(cudaStreamSynchronize(s));
+  return FEM_OK;
+}
+
+// ------------------------------------------------------------ context ----
+
+extern "C" void fem_ctx_destroy(fem_ctx* c) {
+  if (!c) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
+                  c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
+                  c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
+                  c->rhsU, c->Uhat, c->gPn, c->Ustar, c->rhsP, c->Ce, c->Ce2, c->Ct, c->Mt, c->Ek, c->tau,
+                  c->dotpart, c->Fe, c->flags};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
+    CtxLevel& L = c->lv[l];
+    void* lp[] = {L.Le, L.Leoff, L.diag, L.x, L.t, L.pin, (l > 0) ? L.r : nullptr};
+    for (void* p : lp)
+      if (p) cudaFree(p);
+  }
+  cudaSetDevice(prev);
+  delete c;
+}
+
+static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
+  if (!make_grid(m->kind, m->periodic, m->nex, m->ney, m->nez, c->g)) return FEM_E_ARG;
+  c->device = device;
+  FEM_CHECK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  FEM_CHECK(cudaGetDeviceProperties(&prop, device));
+  c->sms = prop.multiProcessorCount;
+  int occ_cg = 0, occ_bi = 0;
+  if (fem_coop_occupancy_cg(&occ_cg) || fem_coop_occupancy_bi(&occ_bi)) return set_err("occupancy", cudaGetLastError());
+  const int occ = std::max(1, std::min(occ_cg, occ_bi));
+  c->max_coop = c->sms * occ;
+  const char* ev = getenv("FEM_MAX_CTAS");
+  if (ev && atoi(ev) > 0) c->max_coop = std::min(c->max_coop, atoi(ev));
+  const FemGrid& g = c->g;
+  c->ndim = (g.kind == FEM_HEX8) ? 3 : 2;
+  c->nq = g.nen;
+  c->lx = m->lx;
+  c->ly = m->ly;
+  c->lz = m->lz;
+  const int nen = g.nen, nd = c->ndim;
+  const size_t nn = g.nn, vn = (size_t)nd * nn, per = (size_t)nen * nen;
+  FEM_ALLOC(c->coords, nn * nd);
+  FEM_ALLOC(c->wq, c->nq);
+  FEM_ALLOC(c->N, c->nq * nen);
+  FEM_ALLOC(c->dN, c->nq * nd * nen);
+  FEM_ALLOC(c->Me, per);
+  FEM_ALLOC(c->Le, per);
+  FEM_ALLOC(c->Leoff, per);
+  FEM_ALLOC(c->Ge, nd * per);
+  FEM_ALLOC(c->Kd, per);
+  FEM_ALLOC(c->M, vn);
+  FEM_ALLOC(c->Ldiag, nn);
+  FEM_ALLOC(c->dmask, vn);
+  FEM_ALLOC(c->pmask, nn);
+  FEM_ALLOC(c->aipin, nn);
+  FEM_ALLOC(c->bar, 2);
+  FEM_ALLOC(c->err, 1);
+  FEM_ALLOC(c->partials, (size_t)FEM_NSLOTS * c->max_coop);
+  FEM_ALLOC(c->flags, 16);
+  for (double** p : {&c->pr, &c->pz, &c->pp0, &c->pp1, &c->pAp, &c->pb, &c->rhsP}) FEM_ALLOC(*p, nn);
+  for (double** p : {&c->br, &c->brh, &c->bp0, &c->bp1, &c->bq0, &c->bq1, &c->bt, &c->rhsU, &c->Uhat, &c->gPn,
+                     &c->Ustar})
+    FEM_ALLOC(*p, vn);
+  FEM_ALLOC(c->Ce, (size_t)g.ne * per);
+  FEM_ALLOC(c->dotpart, 4096);
+  cudaStream_t s = 0;
+  FEM_CHECK(cudaMemset(c->bar, 0, 2 * sizeof(unsigned int)));
+  FEM_CHECK(cudaMemset(c->err, 0, sizeof(int)));
+  FEM_CHECK(cudaMemset(c->dmask, 0, vn));
+  FEM_CHECK(cudaMemset(c->pmask, 0, nn));
+  FEM_CHECK(cudaMemset(c->aipin, 0, nn));
+  FEM_CHECK(cudaMemset(c->pmask, 1, 1));  // default gamma_p = node 0 (setup/simulation.py:181)
+  FEM_CHECK(cudaMemset(c->aipin, 1, 1));
+  double dx, dy, dz;
+  spacings(m, dx, dy, dz);
+  FEM_TRY(fem_launch_mesh_generate(g, dx, dy, dz, c->coords, nullptr, s));
+  double* tmp;
+  FEM_ALLOC(tmp, 32);
+  int rc = element_setup(g, dx, dy, dz, tmp, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag,
+                         nd, s);
+  cudaFree(tmp);
+  if (rc) return rc;
+  // level 0 of the hierarchy is the mesh itself (used by the plain CG path too)
+  CtxLevel& L0 = c->lv[0];
+  L0.g = g;
+  L0.Le = nullptr;  // level 0 aliases the context matrices
+  FEM_ALLOC(L0.x, nn);
+  FEM_ALLOC(L0.t, nn);
+  L0.r = c->pr;
+  c->nlev = 1;
+  FEM_CHECK(cudaDeviceSynchronize());
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_create(const fem_mesh_desc* m, int device, fem_ctx** out) {
+  if (!m || !out) return FEM_E_ARG;
+  fem_ctx* c = new (std::nothrow) fem_ctx();
+  if (!c) return FEM_E_OOM;
+  int rc = ctx_create_impl(m, device, c);
+  if (rc) {
+    fem_ctx_destroy(c);
+    *out = nullptr;
+    return rc;
+  }
+  *out = c;
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_dims(const fem_ctx* c, int* nn, int* ne, int* nen, int* ndim, int* nq) {
+  if (!c) return FEM_E_ARG;
+  if (nn) *nn = c->g.nn;
+  if (ne) *ne = c->g.ne;
+  if (nen) *nen = c->g.nen;
+  if (ndim) *ndim = c->ndim;
+  if (nq) *nq = c->nq;
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_element_data(const fem_ctx* c, double* wq, double* N, double* Nderiv, double* Me, double* Le,
+                                    double* Ge, double* M, double* Ldiag, cudaStream_t s) {
+  if (!c) return FEM_E_ARG;
+  const size_t per = (size_t)c->g.nen * c->g.nen, d = sizeof(double);
+  struct {
+    double* dst;
+    const double* src;
+    size_t n;
+  } cp[] = {{wq, c->wq, (size_t)c->nq},
+            {N, c->N, (size_t)c->nq * c->g.nen},
+            {Nderiv, c->dN, (size_t)c->nq * c->ndim * c->g.nen},
+            {Me, c->Me, per},
+            {Le, c->Le, per},
+            {Ge, c->Ge, c->ndim * per},
+            {M, c->M, (size_t)c->ndim * c->g.nn},
+            {Ldiag, c->Ldiag, (size_t)c->g.nn}};
+  for (auto& e : cp)
+    if (e.dst) FEM_CHECK(cudaMemcpyAsync(e.dst, e.src, e.n * d, cudaMemcpyDeviceToDevice, s));
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_set_bc(fem_ctx* c, const uint8_t* dmask, const uint8_t* pmask, int set_zeroP,
+                              cudaStream_t s) {
+  if (!c) return FEM_E_ARG;
+  const size_t nn = c->g.nn;
+  if (dmask) {
+    FEM_CHECK(cudaMemcpyAsync(c->dmask, dmask, c->ndim * nn, cudaMemcpyDeviceToDevice, s));
+    c->has_dmask = 1;
+  } else {
+    FEM_CHECK(cudaMemsetAsync(c->dmask, 0, c->ndim * nn, s));
+    c->has_dmask = 0;
+  }
+  if (pmask) {
+    FEM_CHECK(cudaMemcpyAsync(c->pmask, pmask, nn, cudaMemcpyDeviceToDevice, s));
+    FEM_CHECK(cudaMemcpyAsync(c->aipin, pmask, nn, cudaMemcpyDeviceToDevice, s));
+  }
+  c->set_zeroP = set_zeroP ? 1 : 0;
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* level_pmasks, double coarse_tol,
+                                       cudaStream_t s) {
+  if (!c || nlev < 1 || nlev > FEM_MAX_LEVELS || c->g.kind == FEM_HEX8) return FEM_E_ARG;
+  FEM_CHECK(cudaSetDevice(c->device));
+  FEM_CHECK(cudaStreamSynchronize(s));
+  const FemGrid& g0 = c->g;
+  for (int l = 1; l < nlev; ++l)
+    if ((g0.nex >> l) < 1 || (g0.ney >> l) < 1) return FEM_E_ARG;
+  // release previous levels
+  for (int l = 1; l < FEM_MAX_LEVELS; ++l) {
+    CtxLevel& L = c->lv[l];
+    void* lp[] = {L.Le, L.Leoff, L.diag, L.x, L.t, L.pin, L.r};
+    for (void* p : lp)
+      if (p) cudaFree(p);
+    L = CtxLevel();
+  }
+  if (c->lv[0].pin) cudaFree(c->lv[0].pin);
+  c->lv[0].pin = nullptr;
+  if (c->cr) cudaFree(c->cr), cudaFree(c->cp), cudaFree(c->cq);
+  c->cr = c->cp = c->cq = nullptr;
+  double* tmp;
+  FEM_ALLOC(tmp, 64);
+  double *wq, *N, *dN, *Me, *Ge, *Mtmp;
+  FEM_ALLOC(wq, 9);
+  FEM_ALLOC(N, 81);
+  FEM_ALLOC(dN, 162);
+  FEM_ALLOC(Me, 81);
+  FEM_ALLOC(Ge, 162);
+  size_t off = 0;
+  int rc = FEM_OK;
+  double* sums;
+  FEM_ALLOC(sums, 2 * FEM_MAX_LEVELS);
+  for (int l = 0; l < nlev && rc == FEM_OK; ++l) {
+    CtxLevel& L = c->lv[l];
+    if (l == 0) {
+      L.g = g0;
+    } else if (!make_grid(g0.kind, g0.periodic, g0.nex >> l, g0.ney >> l, 1, L.g)) {
+      rc = FEM_E_ARG;
+      break;
+    }
+    const size_t nn = L.g.nn;
+    if (l > 0) {
+      rc |= dalloc(&L.Le, 81);
+      rc |= dalloc(&L.Leoff, 81);
+      rc |= dalloc(&L.diag, nn);
+      rc |= dalloc(&L.x, nn);
+      rc |= dalloc(&L.r, nn);
+      rc |= dalloc(&L.t, nn);
+      if (rc) break;
+      rc |= dalloc(&Mtmp, 2 * nn);
+      if (rc) break;
+      const double dx = c->lx / L.g.nex, dy = c->ly / L.g.ney;
+      rc = element_setup(L.g, dx, dy, 0.0, tmp, wq, N, dN, Me, L.Le, L.Leoff, Ge, Mtmp, L.diag, 2, s);
+      cudaFree(Mtmp);
+      if (rc) break;
+    }
+    rc |= dalloc(&L.pin, nn);
+    if (rc) break;
+    if (level_pmasks) {
+      FEM_CHECK(cudaMemcpyAsync(L.pin, level_pmasks + off, nn, cudaMemcpyDeviceToDevice, s));
+    } else {
+      FEM_CHECK(cudaMemsetAsync(L.pin, 0, nn, s));
+      FEM_CHECK(cudaMemsetAsync(L.pin, 1, 1, s));
+    }
+    off += nn;
+    const double* diag = (l == 0) ? c->Ldiag : L.diag;
+    FEM_TRY(fem_launch_level_sums(L.g, lattice_of(L.g), diag, sums + 2 * l, s));
+  }
+  double hs[2 * FEM_MAX_LEVELS];
+  if (rc == FEM_OK) {
+    FEM_CHECK(cudaMemcpyAsync(hs, sums, sizeof(double) * 2 * nlev, cudaMemcpyDeviceToHost, s));
+    FEM_CHECK(cudaStreamSynchronize(s));
+  }
+  cudaFree(tmp);
+  cudaFree(wq);
+  cudaFree(N);
+  cudaFree(dN);
+  cudaFree(Me);
+  cudaFree(Ge);
+  cudaFree(sums);
+  if (rc) return rc;
+  for (int l = 0; l < nlev; ++l) {
+    c->lv[l].sum_invD = hs[2 * l];
+    c->lv[l].sum_colw = hs[2 * l + 1];
+  }
+  c->nlev = nlev;
+  c->coarse_tol = coarse_tol;
+  // coarse scratch for the in-CTA CG
+  const size_t ncn = c->lv[nlev - 1].g.nn;
+  FEM_ALLOC(c->cr, ncn);
+  FEM_ALLOC(c->cp, ncn);
+  FEM_ALLOC(c->cq, ncn);
+  // first level handled by CTA 0 alone
+  int small = 4096;
+  const char* ev = getenv("FEM_MG_BLOCK_NN");
+  if (ev) small = atoi(ev);
+  int bf = nlev - 1;
+  for (int l = 0; l < nlev; ++l)
+    if (c->lv[l].g.nn <= small) {
+      bf = l;
+      break;
+    }
+  c->block_from = bf;
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_level_info(const fem_ctx* c, int level, int* nn, int* nnx, int* nny, int* nex, int* ney) {
+  if (!c || level < 0 || level >= c->nlev) return FEM_E_ARG;
+  const FemGrid& g = c->lv[level].g;
+  FemLattice L = lattice_of(g);
+  if (nn) *nn = g.nn;
+  if (nnx) *nnx = L.nx;
+  if (nny) *nny = L.ny;
+  if (nex) *nex = g.nex;
+  if (ney) *ney = g.ney;
+  return FEM_OK;
+}
+
+// ------------------------------------------------------- element products ----
+
+extern "C" int fem_ebe_apply(fem_ctx* c, int ncomp, const double* x, double* y, double alpha, const double* A,
+                             double beta, const double* B, int transB, double gamma, const double* C,
+                             cudaStream_t s) {
+  if (!c || !x || !y || ncomp < 1 || ncomp > 3) return FEM_E_ARG;
+  const MatCombo m{A, alpha, B, beta, transB, C, gamma};
+  return fem_launch_ebe(ncomp, c->g, m, x, y, s);
+}
+
+extern "C" int fem_grad_apply(fem_ctx* c, const double* P, const double* Ge, double* y, cudaStream_t s) {
+  if (!c || !P || !y) return FEM_E_ARG;
+  if (!Ge) Ge = c->Ge;
+  return fem_launch_grad(c->ndim, c->g, Ge, P, y, s);
+}
+
+extern "C" int fem_div_apply(fem_ctx* c, const double* U, const double* Ge, double* y, cudaStream_t s) {
+  if (!c || !U || !y) return FEM_E_ARG;
+  if (!Ge) Ge = c->Ge;
+  return fem_launch_div(c->ndim, c->g, Ge, U, y, s);
+}
+
+static FemQuad quad_of(const fem_ctx* c) { return FemQuad{c->wq, c->N, c->dN, c->nq, c->g.nen, c->ndim}; }
+static FemQuad quad_with(const fem_ctx* c, const double* wq, const double* N, const double* dN) {
+  FemQuad Q = quad_of(c);
+  if (wq) Q.wq = wq;
+  if (N) Q.N = N;
+  if (dN) Q.dN = dN;
+  return Q;
+}
+
+extern "C" int fem_convection_build(fem_ctx* c, const double* U, double beta, const double* wq, const double* N,
+                                    const double* dN, double* Ce, cudaStream_t s) {
+  if (!c || !U || !Ce) return FEM_E_ARG;
+  return fem_launch_convection(c->g, quad_with(c, wq, N, dN), U, beta, 0, Ce, s);
+}
+
+extern "C" int fem_ctau_tilde_build(fem_ctx* c, const double* U, const double* wq, const double* N, const double* dN,
+                                    double* Ct, cudaStream_t s) {
+  if (!c || !U || !Ct) return FEM_E_ARG;
+  return fem_launch_convection(c->g, quad_with(c, wq, N, dN), U, 0.0, 1, Ct, s);
+}
+
+extern "C" int fem_supg_tau(fem_ctx* c, const double* U, const double* Ce, const double* Ct, double D, double dt,
+                            double r, const double* N, double* tau, cudaStream_t s) {
+  if (!c || !U || !Ce || !Ct || !tau) return FEM_E_ARG;
+  return fem_launch_supg_tau(c->g, quad_with(c, nullptr, N, nullptr), U, Ce, Ct, D, dt, r, tau, s);
+}
+
+extern "C" int fem_element_matrices(int nq, int nen, int dim, const double* wq, const double* N, const double* dN,
+                                    double* Me, double* Le, double* Leoff, double* Ge, cudaStream_t s) {
+  if (nq < 1 || nq > 27 || nen < 1 || nen > 9 || dim < 1 || dim > 3 || !wq || !N || !dN || !Me || !Le || !Leoff ||
+      !Ge)
+    return FEM_E_ARG;
+  return fem_launch_element_matrices(nq, nen, dim, wq, N, dN, Me, Le, Leoff, Ge, s);
+}
+
+extern "C" int fem_assemble_diag(fem_ctx* c, const double* Me, const double* Le, int ndim, double* M, double* Ldiag,
+                                 cudaStream_t s) {
+  if (!c || ndim < 1 || ndim > 3 || (Me && !M) || (Le && !Ldiag) || (!Me && !Le)) return FEM_E_ARG;
+  return fem_launch_assemble_diag(c->g, ndim, Me, Le, Me ? M : nullptr, Le ? Ldiag : nullptr, s);
+}
+
+// ------------------------------------------------------------ multigrid ----
+
+static bool lattice_ok(int Hx, int Hy, int hx, int hy) {
+  return Hx >= 2 && Hy >= 2 && hx == 2 * Hx - 1 && hy == 2 * Hy - 1;
+}
+
+extern "C" int fem_lattice_interpolate(int nHx, int nHy, int nhx, int nhy, int periodic, const double* xH, double* xh,
+                                       cudaStream_t s) {
+  if (!xH || !xh || !lattice_ok(nHx, nHy, nhx, nhy)) return FEM_E_ARG;
+  return fem_launch_interp(FemLattice{nHx, nHy, periodic ? 1 : 0}, FemLattice{nhx, nhy, periodic ? 1 : 0}, xH, xh, s);
+}
+
+extern "C" int fem_lattice_restrict(int nhx, int nhy, int nHx, int nHy, int periodic, const double* xh, double* xH,
+                                    cudaStream_t s) {
+  if (!xH || !xh || !lattice_ok(nHx, nHy, nhx, nhy)) return FEM_E_ARG;
+  return fem_launch_restrict(FemLattice{nhx, nhy, periodic ? 1 : 0}, FemLattice{nHx, nHy, periodic ? 1 : 0}, xh, xH, s);
+}
+
+static void fill_cg_args(fem_ctx* c, CgArgs& A) {
+  memset(&A, 0, sizeof(A));
+  A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS};
+  A.nlev = c->nlev;
+  A.block_from = c->block_from;
+  A.pinned = c->set_zeroP;
+  A.coarse_maxiter = 1000;
+  A.coarse_tol = c->coarse_tol;
+  A.r = c->pr;
+  A.z = c->pz;
+  A.p0 = c->pp0;
+  A.p1 = c->pp1;
+  A.Ap = c->pAp;
+  A.bwork = c->pb;
+  A.ai_pin = c->aipin;
+  for (int l = 0; l < c->nlev; ++l) {
+    CtxLevel& L = c->lv[l];
+    MgLevel& M = A.lv[l];
+    M.g = L.g;
+    M.lat = lattice_of(L.g);
+    M.Le = (l == 0) ? c->Le : L.Le;
+    M.Le_off = (l == 0) ? c->Leoff : L.Leoff;
+    M.diag = (l == 0) ? c->Ldiag : L.diag;
+    M.pin = (l == 0) ? (L.pin ? L.pin : c->pmask) : L.pin;
+    M.sum_invD = L.sum_invD;
+    M.sum_colw = L.sum_colw;
+    M.x = L.x;
+    M.r = (l == 0) ? c->pr : L.r;
+    M.t = L.t;
+  }
+  // level 0 pins of the plain (non-multigrid) solve are the context gamma_p
+  if (c->nlev == 1 || !c->lv[0].pin) A.lv[0].pin = c->pmask;
+}
+
+static int reset_sync(fem_ctx* c, cudaStream_t s) {
+  FEM_CHECK(cudaMemsetAsync(c->bar, 0, sizeof(unsigned int), s));  // arrival count only
+  FEM_CHECK(cudaMemsetAsync(c->err, 0, sizeof(int), s));
+  return FEM_OK;
+}
+
+static int run_cg(fem_ctx* c, const double* b, double* x, double tol, double atol, int maxiter, int precond,
+                  int center, int post, int* iters, int* status, cudaStream_t s) {
+  CgArgs A;
+  fill_cg_args(c, A);
+  A.prec = precond;
+  A.center_rhs = center;
+  A.post = post;
+  A.maxiter = maxiter;
+  A.tol = tol;
+  A.atol = atol;
+  A.b = b;
+  A.x = x;
+  A.iters = iters;
+  A.status = status;
+  A.final_rr = nullptr;
+  FEM_TRY(reset_sync(c, s));
+  const int grid = ctx_grid_for(c, c->g.nn);
+  double* cr = c->cr ? c->cr : c->pz;
+  double* cp = c->cp ? c->cp : c->pz;
+  double* cq = c->cq ? c->cq : c->pz;
+  return fem_launch_cg(A, grid, cr, cp, cq, s);
+}
+
+extern "C" int fem_pressure_solve(fem_ctx* c, const double* b, double* x, double tol, double atol, int maxiter,
+                                  int precond, int center_rhs, int post, int* iters, int* status, cudaStream_t s) {
+  if (!c || !b || !x || !iters || !status || precond < 0 || precond > 4 || maxiter < 0) return FEM_E_ARG;
+  if (precond == FEM_PREC_MG && c->nlev < 2) return FEM_E_STATE;
+  return run_cg(c, b, x, tol, atol, maxiter, precond, center_rhs, post, iters, status, s);
+}
+
+extern "C" int fem_mg_vcycle(fem_ctx* c, const double* r, double* z, cudaStream_t s) {
+  if (!c || !r || !z || c->nlev < 2) return FEM_E_ARG;
+  CgArgs A;
+  fill_cg_args(c, A);
+  FEM_CHECK(cudaMemcpyAsync(c->pr, r, sizeof(double) * c->g.nn, cudaMemcpyDeviceToDevice, s));
+  FEM_TRY(reset_sync(c, s));
+  return fem_launch_vcycle(A, ctx_grid_for(c, c->g.nn), c->cr, c->cp, c->cq, z, s);
+}
+
+static int run_bicgstab(fem_ctx* c, int ncomp, const MatCombo& op, const uint8_t* mask, const double* b, double* x,
+                        double tol, double atol, int maxiter, int* iters, int* status, cudaStream_t s) {
+  if (ncomp < 1 || ncomp > c->ndim) return FEM_E_ARG;  // workspace holds ndim*nn per vector
+  BiArgs A;
+  memset(&A, 0, sizeof(A));
+  A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS};
+  A.g = c->g;
+  A.op = op;
+  A.mask = mask;
+  A.b = b;
+  A.x = x;
+  A.r = c->br;
+  A.rhat = c->brh;
+  A.p0 = c->bp0;
+  A.p1 = c->bp1;
+  A.q0 = c->bq0;
+  A.q1 = c->bq1;
+  A.t = c->bt;
+  A.tol = tol;
+  A.atol = atol;
+  A.maxiter = maxiter > 0 ? maxiter : 10 * ncomp * c->g.nn;  // utils/jax_iterative_solvers.py:181-183
+  A.iters = iters;
+  A.status = status;
+  FEM_TRY(reset_sync(c, s));
+  return fem_launch_bicgstab(ncomp, A, ctx_grid_for(c, c->g.nn), s);
+}
+
+extern "C" int fem_bicgstab_solve(fem_ctx* c, int ncomp, double alpha, const double* Ash, double beta,
+                                  const double* B, double gamma, const double* C, const uint8_t* mask,
+                                  const double* b, double* x, double tol, double atol, int maxiter, int* iters,
+                                  int* status, cudaStream_t s) {
+  if (!c || !b || !x || !iters || !status) return FEM_E_ARG;
+  const MatCombo op{Ash, alpha, B, beta, 0, C, gamma};
+  return run_bicgstab(c, ncomp, op, mask, b, x, tol, atol, maxiter, iters, status, s);
+}
+
+extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double dt, double rho, double mu,
+                         const double* Ud, const double* Fp, const double* F, double tol, int precond, double* Uo,
+                         double* Po, int* iters, int* status, cudaStream_t s) {
+  if (!c || !Un || !Pn || !Uo || !Po || !iters || !status) return FEM_E_ARG;
+  if (c->has_dmask && !Ud) return FEM_E_ARG;
+  if (precond < 0 || precond > 4) return FEM_E_ARG;
+  if (precond == FEM_PREC_MG && c->nlev < 2) return FEM_E_STATE;
+  const FemGrid& g = c->g;
+  const int nd = c->ndim, nen = g.nen;
+  const double theta = 0.5;
+  // 1. Ce(U_n), beta = 1/2 (solvers/standard.py:152)
+  FEM_TRY(fem_launch_convection(g, quad_of(c), Un, 0.5, 0, c->Ce, s));
+  // 2. momentum rhs, x0 and G P_n (solvers/standard.py:31-37)
+  StepArgs S;
+  S.g = g;
+  S.ndim = nd;
+  S.dt = dt;
+  S.rho = rho;
+  S.mu = mu;
+  S.theta = theta;
+  S.Me = c->Me;
+  S.Le = c->Le;
+  S.Ge = c->Ge;
+  S.M = c->M;
+  S.Ce = c->Ce;
+  S.dmask = c->has_dmask ? c->dmask : nullptr;
+  S.pmask = c->pmask;
+  S.pinned = c->set_zeroP;
+  FEM_TRY(fem_launch_mom_rhs(S, Un, Pn, Ud, F, c->rhsU, c->Uhat, c->gPn, s));
+  // 3. BiCGSTAB on (rho/dt) Me + theta (rho Ce + mu Le), identity rows on gamma_d (:20-28, :41)
+  FEM_TRY(fem_launch_lincomb(nen * nen, rho / dt, c->Me, theta * mu, c->Le, c->Kd, s));
+  const MatCombo op{c->Kd, 1.0, c->Ce, theta * rho, 0, nullptr, 0.0};
+  FEM_TRY(run_bicgstab(c, nd, op, S.dmask, c->rhsU, c->Uhat, tol, 0.0, 0, iters, status, s));
+  // 4. U* = U_hat + (dt/rho) G P_n / M (:156)
+  FEM_TRY(fem_launch_ustar(nd * g.nn, dt / rho, c->Uhat, c->gPn, c->M, c->Ustar, s));
+  // 5. PPE rhs and x0 (:97-107)
+  FEM_TRY(fem_launch_p_rhs(S, c->Ustar, Fp, Pn, c->rhsP, Po, s));
+  // 6. pressure (P)CG, maxiter 1000 (:115-123)
+  FEM_TRY(run_cg(c, c->rhsP, Po, tol, 0.0, 1000, precond, c->set_zeroP ? 0 : 1, 1, iters + 1, status + 1, s));
+  // 7. projection and Dirichlet values (:160-163)
+  return fem_launch_ufinal(S, c->Ustar, Po, Ud, Uo, s);
+}
+
+extern "C" int fem_transport_phi(fem_ctx* c, const double* Un, const double* U, const double* phin, double dt,
+                                 double D, int supg, const uint8_t* phi_mask, const double* phid, double tol,
+                                 double* phio, int* iters, int* status, cudaStream_t s) {
+  if (!c || !Un || !U || !phin || !phio || !iters || !status) return FEM_E_ARG;
+  if (phi_mask && !phid) return FEM_E_ARG;
+  const FemGrid& g = c->g;
+  const size_t per = (size_t)g.nen * g.nen, ntot = (size_t)g.ne * per;
+  if (!c->Ce2) {
+    FEM_ALLOC(c->Ce2, ntot);
+    FEM_ALLOC(c->Ct, ntot);
+    FEM_ALLOC(c->Mt, ntot);
+    FEM_ALLOC(c->Ek, ntot);
+    FEM_ALLOC(c->tau, g.ne);
+  }
+  const FemQuad Q = quad_of(c);
+  // Ce(U_n, 1) -> Ce, Ce(U, 1) -> Ce2 (solvers/passive_transport.py:80-81)
+  FEM_TRY(fem_launch_convection(g, Q, Un, 1.0, 0, c->Ce, s));
+  FEM_TRY(fem_launch_convection(g, Q, U, 1.0, 0, c->Ce2, s));
+  if (supg) {
+    // Ctau_tilde(U_n); tau(U_n, Ce(U), Ct); Ctau = tau Ct; Mtau = tau Ce_n^T (:84-88)
+    FEM_TRY(fem_launch_convection(g, Q, Un, 0.0, 1, c->Ct, s));
+    FEM_TRY(fem_launch_supg_tau(g, Q, Un, c->Ce2, c->Ct, D, dt, 2.0, c->tau, s));
+    FEM_TRY(fem_launch_scale_elem(g.ne, g.nen, c->tau, c->Ct, 0, c->Ct, s));
+    FEM_TRY(fem_launch_scale_elem(g.ne, g.nen, c->tau, c->Ce, 1, c->Mt, s));
+  } else {
+    FEM_CHECK(cudaMemsetAsync(c->Ct, 0, ntot * sizeof(double), s));
+    FEM_CHECK(cudaMemsetAsync(c->Mt, 0, ntot * sizeof(double), s));
+  }
+  // rhs and x0 (:294-301 / :318-325)
+  FEM_TRY(fem_launch_phi_rhs(g, c->Me, c->Le, dt, D, c->Mt, c->Ce, c->Ct, phin, phi_mask, phid, c->rhsP, phio, s));
+  // lhs: [(1/dt) Me + 0.5 D Le] + [(1/dt) Mtau + 0.5 (Ce + Ctau)]
+  FEM_TRY(fem_launch_lincomb(g.nen * g.nen, 1.0 / dt, c->Me, 0.5 * D, c->Le, c->Kd, s));
+  FEM_TRY(fem_launch_elem_combine(ntot, 1.0 / dt, c->Mt, 0.5, c->Ce2, c->Ct, c->Ek, s));
+  const MatCombo op{c->Kd, 1.0, c->Ek, 1.0, 0, nullptr, 0.0};
+  return run_bicgstab(c, 1, op, phi_mask, c->rhsP, phio, tol, 0.0, 0, iters, status, s);
+}
+
+extern "C" int fem_boundary_flux(fem_ctx* c, const int32_t* bconn, const double* nvec, int nb, int npf,
+                                 const double* U, double* Fp, cudaStream_t s) {
+  if (!c || !bconn || !nvec || !U || !Fp || nb < 0 || npf < 2 || npf > 4) return FEM_E_ARG;
+  if (nb * npf > c->Fe_cap) {
+    FEM_CHECK(cudaStreamSynchronize(s));
+    if (c->Fe) cudaFree(c->Fe);
+    c->Fe = nullptr;
+    FEM_ALLOC(c->Fe, (size_t)nb * npf);
+    c->Fe_cap = nb * npf;
+  }
+  return fem_launch_boundary(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, c->Fe, Fp, s);
+}
+
+extern "C" int fem_scatter(const int64_t* idx, const double* vals, double value, int n, double* out,
+                           cudaStream_t s) {
+  if (n < 0 || (n > 0 && (!idx || !out))) return FEM_E_ARG;
+  if (n == 0) return FEM_OK;
+  return fem_launch_scatter(idx, vals, value, n, out, s);
+}
+
+extern "C" int fem_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cudaStream_t s) {
+  if (n < 0 || len < 0 || !mask || (n > 0 && !idx)) return FEM_E_ARG;
+  FEM_CHECK(cudaMemsetAsync(mask, 0, (size_t)len, s));
+  if (n == 0) return FEM_OK;
+  return fem_launch_make_mask(idx, n, len, mask, s);
+}
+
+extern "C" int fem_dot(fem_ctx* c, const double* x, const double* y, int n, double* out, cudaStream_t s) {
+  if (!c || !x || !y || !out || n < 0) return FEM_E_ARG;
+  return fem_launch_dot(x, y, n, c->dotpart, out, s);
+}
+
+extern "C" int fem_axpby(fem_ctx* c, double a, const double* x, double b, double* y, int n, cudaStream_t s) {
+  if (!c || !x || !y || n < 0) return FEM_E_ARG;
+  return fem_launch_axpby(a, x, b, y, n, s);
+}
+
+extern "C" long long fem_launch_count(void) { return g_launches.load(); }
+extern "C" const char* fem_last_error(void) { return g_err; }

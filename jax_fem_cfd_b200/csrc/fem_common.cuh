@@ -1,0 +1,321 @@
+// Common device-side building blocks for the B200 matrix-free FEM path.
+//
+// Meshes are the structured lattices of jax_fem_cfd setup/regular_mesh.py
+// (quad4 / quad9 2D, periodic or not, hex8 3D). Connectivity is never read
+// from memory: a node's incident elements and its local index in each are
+// computed from its lattice coordinates, and an element's nodes from the
+// element's lattice coordinates. This reproduces nconn of regular_mesh.py
+// exactly (local node order, periodic wrap) at zero connectivity bytes.
+//
+// Every assembled product y = sum_e P_e^T A_e P_e x is evaluated node-centrically:
+// the thread that owns output node n sums the rows of its incident elements in a
+// fixed order, so results are bitwise reproducible run to run without atomics or
+// element colouring (the reference's segment_sum is an atomic scatter on GPU).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define FEM_Q1_2D 0
+#define FEM_Q2_2D 1
+#define FEM_HEX8 2
+
+#define FEM_MAX_NEN 9
+
+struct FemGrid {
+  int kind;       // FEM_Q1_2D | FEM_Q2_2D | FEM_HEX8
+  int periodic;   // 2D only
+  int nex, ney, nez;
+  int nnx, nny, nnz;  // unique-node lattice extents (periodic drops the duplicate row/column)
+  int nn, ne, nen;
+};
+
+// local node a of an element sits at lattice offset (di[a], dj[a], dk[a]) from
+// (s*ie, s*je, ke), s = 2 for quad9 (setup/regular_mesh.py:24-26, 68-73, 119-126).
+// Tables are bit-packed constants (2 bits per entry) so they stay in registers.
+//   quad9 di = 0,1,2,2,2,1,0,0,1   dj = 0,0,0,1,2,2,2,1,1
+//   quad4 di = 0,1,1,0             dj = 0,0,1,1   (hex8: same, dk = a >> 2)
+#define FEM_Q2_DI 0x106A4u  // entries a = 0..8 at bits 2a
+#define FEM_Q2_DJ 0x16A40u
+#define FEM_Q1_DI 0x14u
+#define FEM_Q1_DJ 0x50u
+__device__ __forceinline__ void fem_local_offset(int kind, int a, int& di, int& dj, int& dk) {
+  if (kind == FEM_Q2_2D) {
+    di = (FEM_Q2_DI >> (2 * a)) & 3;
+    dj = (FEM_Q2_DJ >> (2 * a)) & 3;
+    dk = 0;
+  } else {
+    di = (FEM_Q1_DI >> (2 * (a & 3))) & 3;
+    dj = (FEM_Q1_DJ >> (2 * (a & 3))) & 3;
+    dk = (kind == FEM_HEX8) ? (a >> 2) : 0;
+  }
+}
+
+// Inverse tables, indexed [dj][di]: quad9 {0,1,2,7,8,3,6,5,4} (4 bits per
+// entry), quad4 {0,1,3,2} (2 bits per entry).
+#define FEM_Q2_INV 0x456387210ull
+#define FEM_Q1_INV 0xB4u
+__device__ __forceinline__ int fem_local_index(int kind, int di, int dj, int dk) {
+  if (kind == FEM_Q2_2D) return (int)((FEM_Q2_INV >> (4 * (dj * 3 + di))) & 15ull);
+  return (int)((FEM_Q1_INV >> (2 * (dj * 2 + di))) & 3u) + 4 * dk;
+}
+
+struct FemElem {
+  int ie, je, ke;
+  int e;
+};
+
+__device__ __forceinline__ int fem_node_at(const FemGrid& g, int i, int j, int k) {
+  if (g.periodic) {
+    if (i >= g.nnx) i -= g.nnx;
+    if (j >= g.nny) j -= g.nny;
+  }
+  return (k * g.nny + j) * g.nnx + i;
+}
+
+// Global node index of local node b of element (ie, je, ke).
+__device__ __forceinline__ int fem_elem_node(const FemGrid& g, int ie, int je, int ke, int b) {
+  int di, dj, dk;
+  fem_local_offset(g.kind, b, di, dj, dk);
+  const int s = (g.kind == FEM_Q2_2D) ? 2 : 1;
+  return fem_node_at(g, s * ie + di, s * je + dj, ke + dk);
+}
+
+__device__ __forceinline__ void fem_node_ijk(const FemGrid& g, int n, int& i, int& j, int& k) {
+  i = n % g.nnx;
+  int t = n / g.nnx;
+  j = t % g.nny;
+  k = t / g.nny;
+}
+
+// Candidate (element coordinate, local offset) pairs along one lattice axis for
+// lattice coordinate c: (e0, d0) and, when the count is 2, (e1, d1). The
+// element on the low side (node is its last node along the axis) comes first.
+__device__ __forceinline__ int fem_axis_candidates(int kind, int periodic, int c, int nel, int& e0, int& d0,
+                                                   int& e1, int& d1) {
+  int h = c, dl = 1;
+  if (kind == FEM_Q2_2D) {
+    if (c & 1) {
+      e0 = (c - 1) >> 1;
+      d0 = 1;
+      return 1;
+    }
+    h = c >> 1;
+    dl = 2;
+  }
+  const bool has_lo = (h >= 1) || periodic;
+  const int elo = (h >= 1) ? h - 1 : nel - 1;
+  const bool has_hi = h < nel;
+  if (has_lo && has_hi) {
+    e0 = elo; d0 = dl; e1 = h; d1 = 0;
+    return 2;
+  }
+  if (has_lo) {
+    e0 = elo; d0 = dl;
+    return 1;
+  }
+  e0 = h; d0 = 0;
+  return 1;
+}
+
+// Iterate over (element, local index) pairs incident to node n and call
+// f(ie, je, ke, e, a). Order: k-candidates outer, then j, then i.
+template <class F>
+__device__ __forceinline__ void fem_for_incident(const FemGrid& g, int n, F&& f) {
+  int i, j, k;
+  fem_node_ijk(g, n, i, j, k);
+  int ei0, ei1 = 0, di0, di1 = 0, ej0, ej1 = 0, dj0, dj1 = 0, ek0 = 0, ek1 = 0, dk0 = 0, dk1 = 0;
+  const int ni = fem_axis_candidates(g.kind, g.periodic, i, g.nex, ei0, di0, ei1, di1);
+  const int nj = fem_axis_candidates(g.kind, g.periodic, j, g.ney, ej0, dj0, ej1, dj1);
+  int nk = 1;
+  if (g.kind == FEM_HEX8) nk = fem_axis_candidates(FEM_HEX8, 0, k, g.nez, ek0, dk0, ek1, dk1);
+  const int cnt = ni * nj * nk;
+#pragma unroll 1
+  for (int z = 0; z < cnt; ++z) {
+    const int zi = z % ni, zj = (z / ni) % nj, zk = z / (ni * nj);
+    const int ei = zi ? ei1 : ei0, di = zi ? di1 : di0;
+    const int ej = zj ? ej1 : ej0, dj = zj ? dj1 : dj0;
+    const int ek = zk ? ek1 : ek0, dk = zk ? dk1 : dk0;
+    const int e = (ek * g.ney + ej) * g.nex + ei;
+    f(ei, ej, ek, e, fem_local_index(g.kind, di, dj, dk));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Teams: a set of threads that executes one solver phase, with its own barrier
+// and deterministic reductions. GridTeam = every thread of a cooperative
+// (co-resident) launch; BlockTeam = the threads of one CTA (coarse levels).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long fem_globaltimer_early() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+#define FEM_ERR_BARRIER_TIMEOUT 1
+#define FEM_ERR_NONFINITE 2
+#define FEM_ERR_MAXITER 4
+#define FEM_ERR_BREAKDOWN 8
+#define FEM_ERR_BAD_ARG 16
+#define FEM_ERR_WATCHDOG 32
+
+// Wall-clock budget of one persistent solve. CTA 0 raises FEM_ERR_WATCHDOG
+// before a barrier once it is exceeded; every CTA sees the flag after that
+// barrier and leaves the loop at the same iteration.
+#define FEM_WATCHDOG_NS 10000000000ull
+__device__ __forceinline__ void fem_watchdog_arm(int* err, unsigned long long t0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && fem_globaltimer_early() - t0 > FEM_WATCHDOG_NS) atomicOr(err, FEM_ERR_WATCHDOG);
+}
+__device__ __forceinline__ bool fem_watchdog_fired(const int* err) {
+  return (*(volatile const int*)err & FEM_ERR_WATCHDOG) != 0;
+}
+
+struct FemSync {
+  unsigned int* count;    // arrivals in the current barrier generation
+  unsigned int* gen;      // barrier generation
+  int* err;               // sticky error flags (FEM_ERR_*)
+  double* partials;       // [slot][cta] partial sums
+  int nslots;
+};
+
+__device__ __forceinline__ unsigned int fem_ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fem_st_release(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long fem_globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Barrier wait limit: a wait that exceeds it sets FEM_ERR_BARRIER_TIMEOUT and
+// every CTA leaves the kernel at its next barrier instead of hanging the GPU.
+#define FEM_BARRIER_TIMEOUT_NS 2000000000ull
+
+struct GridTeam {
+  FemSync s;
+  __device__ __forceinline__ int rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+  __device__ __forceinline__ int size() const { return gridDim.x * blockDim.x; }
+  __device__ __forceinline__ bool leader_block() const { return blockIdx.x == 0; }
+  // Returns false if the kernel must stop (timeout or error raised elsewhere).
+  __device__ bool sync() const {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int ok = 1;
+      const unsigned int g0 = fem_ld_acquire(s.gen);
+      __threadfence();
+      const unsigned int arrived = atomicAdd(s.count, 1u);
+      if (arrived == gridDim.x - 1) {
+        atomicExch(s.count, 0u);
+        __threadfence();
+        fem_st_release(s.gen, g0 + 1u);
+      } else {
+        const unsigned long long t0 = fem_globaltimer();
+        unsigned int polls = 0;
+        while (fem_ld_acquire(s.gen) == g0) {
+          if (((++polls) & 63u) == 0u) {
+            if (*(volatile int*)s.err & FEM_ERR_BARRIER_TIMEOUT) { ok = 0; break; }
+            if (fem_globaltimer() - t0 > FEM_BARRIER_TIMEOUT_NS) {
+              atomicOr(s.err, FEM_ERR_BARRIER_TIMEOUT);
+              ok = 0;
+              break;
+            }
+          }
+        }
+      }
+      __threadfence();
+      if (*(volatile int*)s.err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
+      s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+  }
+};
+
+struct BlockTeam {
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ int size() const { return blockDim.x; }
+  __device__ __forceinline__ bool sync() const {
+    __syncthreads();
+    return true;
+  }
+};
+
+// Deterministic block-wide sum of K values (fixed shuffle tree + fixed warp order).
+template <int K>
+__device__ __forceinline__ void fem_block_sum(double (&v)[K], double* smem /* >= 32*K */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < K; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < K; ++q) smem[q * 32 + warp] = v[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    double t = (lane < nw) ? smem[q * 32 + lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    v[q] = t;
+  }
+}
+
+// Reduction handles. reduce() is called by every thread of the team inside a
+// phase; totals are read by result() after the team's next sync().
+struct GridReducer {
+  FemSync s;
+  template <int K>
+  __device__ __forceinline__ void reduce(double (&v)[K], int slot, double* smem) const {
+    fem_block_sum<K>(v, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < K; ++q) s.partials[(size_t)(slot + q) * gridDim.x + blockIdx.x] = v[q];
+  }
+  // Sum of per-CTA partials in CTA order (identical in every CTA).
+  template <int K>
+  __device__ __forceinline__ void result(double (&out)[K], int slot, double* smem) const {
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        double t = 0.0;
+        for (int c = threadIdx.x; c < (int)gridDim.x; c += 32)
+          t += __ldcg(&s.partials[(size_t)(slot + q) * gridDim.x + c]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) smem[q] = t;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = smem[q];
+    __syncthreads();
+  }
+};
+
+struct BlockReducer {
+  double* store;  // shared memory, >= nslots doubles
+  template <int K>
+  __device__ __forceinline__ void reduce(double (&v)[K], int slot, double* smem) const {
+    fem_block_sum<K>(v, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < K; ++q) store[slot + q] = v[q];
+  }
+  template <int K>
+  __device__ __forceinline__ void result(double (&out)[K], int slot, double*) const {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = store[slot + q];
+  }
+};
+
+__device__ __forceinline__ bool fem_isfinite(double x) { return isfinite(x); }

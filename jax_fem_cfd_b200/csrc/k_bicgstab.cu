@@ -1,0 +1,202 @@
+// Persistent cooperative BiCGSTAB kernel on element-by-element operators.
+#include "fem_args.cuh"
+
+
+template <int NC, class Src>
+__device__ __forceinline__ void bi_apply(const BiArgs& A, int i, const Src& src, double (&y)[NC]) {
+  const FemGrid& g = A.g;
+  const int nen = g.nen;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) y[c] = 0.0;
+  fem_for_incident(g, i, [&](int ie, int je, int ke, int e, int a) {
+    double part[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) part[c] = 0.0;
+    for (int b = 0; b < nen; ++b) {
+      const double coef = A.op(e, a, b, nen);
+      const int j = fem_elem_node(g, ie, je, ke, b);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) part[c] += coef * src(j, c);
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) y[c] += part[c];
+  });
+  if (A.mask) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      if (A.mask[i + (size_t)c * g.nn]) y[c] = src(i, c);
+  }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
+  __shared__ double smem[128];
+  const GridTeam gt{A.sync};
+  const GridReducer gr{A.sync};
+  const int nn = A.g.nn;
+  const size_t N = nn;
+  int k = 0;
+  double rr = 0.0;
+  fem_zero_partials(A.sync);
+  if (!gt.sync()) goto done;
+  {
+    {
+      double a[2] = {0.0, 0.0};
+      for (int i = gt.rank(); i < nn; i += gt.size()) {
+        double Ax[NC];
+        bi_apply<NC>(A, i, [&](int j, int c) { return A.x[j + c * N]; }, Ax);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const double bi = A.b[i + c * N], ri = bi - Ax[c];
+          A.r[i + c * N] = ri;
+          A.rhat[i + c * N] = ri;
+          A.p0[i + c * N] = ri;
+          A.q0[i + c * N] = ri;
+          a[0] += bi * bi;
+          a[1] += ri * ri;
+        }
+      }
+      gr.reduce<2>(a, SL_BB, smem);
+      if (!gt.sync()) goto done;
+    }
+    double bb[2];
+    gr.result<2>(bb, SL_BB, smem);
+    rr = bb[1];
+    double rhr = bb[1];
+    const double atol2 = fmax(A.tol * A.tol * bb[0], A.atol * A.atol);
+    double rho = 1.0, alpha = 1.0, omega = 1.0;
+    int cur = 0;
+    const unsigned long long t_start = fem_globaltimer_early();
+    while (rr > atol2 && k < A.maxiter && k >= 0) {
+      if (fem_watchdog_fired(A.sync.err)) break;
+      const double rho_ = rhr;
+      const double beta = rho_ / rho * alpha / omega;
+      double* __restrict__ pold = cur ? A.p1 : A.p0;
+      double* __restrict__ pnew = cur ? A.p0 : A.p1;
+      double* __restrict__ qold = cur ? A.q1 : A.q0;
+      double* __restrict__ qnew = cur ? A.q0 : A.q1;
+      const double* __restrict__ r = A.r;
+      {
+        auto pn = [&](int j, int c) {
+          const size_t o = j + c * N;
+          return r[o] + beta * (pold[o] - omega * qold[o]);
+        };
+        double a[1] = {0.0};
+        for (int i = gt.rank(); i < nn; i += gt.size()) {
+          double q[NC];
+          bi_apply<NC>(A, i, pn, q);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            pnew[i + c * N] = pn(i, c);
+            qnew[i + c * N] = q[c];
+            a[0] += A.rhat[i + c * N] * q[c];
+          }
+        }
+        gr.reduce<1>(a, SL_BI + 1, smem);
+        if (!gt.sync()) goto done;
+      }
+      double rq[1];
+      gr.result<1>(rq, SL_BI + 1, smem);
+      const double alpha_ = rho_ / rq[0];
+      auto sv = [&](int j, int c) {
+        const size_t o = j + c * N;
+        return r[o] - alpha_ * qnew[o];
+      };
+      {
+        double a[3] = {0.0, 0.0, 0.0};
+        for (int i = gt.rank(); i < nn; i += gt.size()) {
+          double tv[NC];
+          bi_apply<NC>(A, i, sv, tv);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            const double s = sv(i, c);
+            A.t[i + c * N] = tv[c];
+            a[0] += s * s;
+            a[1] += tv[c] * s;
+            a[2] += tv[c] * tv[c];
+          }
+        }
+        gr.reduce<3>(a, SL_BI + 2, smem);
+        if (!gt.sync()) goto done;
+      }
+      double st[3];
+      gr.result<3>(st, SL_BI + 2, smem);
+      const double omega_ = st[1] / st[2];
+      const bool exit_early = st[0] < atol2;
+      {
+        double a[2] = {0.0, 0.0};
+        for (int i = gt.rank(); i < nn; i += gt.size()) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            const size_t o = i + c * N;
+            const double s = sv(i, c);
+            double xn, rn;
+            if (exit_early) {
+              xn = A.x[o] + alpha_ * pnew[o];
+              rn = s;
+            } else {
+              xn = A.x[o] + (alpha_ * pnew[o] + omega_ * s);
+              rn = s - omega_ * A.t[o];
+            }
+            A.x[o] = xn;
+            A.r[o] = rn;
+            a[0] += rn * rn;
+            a[1] += A.rhat[o] * rn;
+          }
+        }
+        gr.reduce<2>(a, SL_RR, smem);  // SL_RR, SL_RSUM (= rhat.r)
+        fem_watchdog_arm(A.sync.err, t_start);
+        if (!gt.sync()) goto done;
+      }
+      double nr[2];
+      gr.result<2>(nr, SL_RR, smem);
+      rr = nr[0];
+      rhr = nr[1];
+      int k_ = (omega_ == 0.0 || alpha_ == 0.0) ? -11 : k + 1;
+      if (rho_ == 0.0) k_ = -10;
+      k = k_;
+      rho = rho_;
+      alpha = alpha_;
+      omega = omega_;
+      cur ^= 1;
+    }
+  }
+done:
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int st = *(volatile int*)A.sync.err & (FEM_ERR_BARRIER_TIMEOUT | FEM_ERR_WATCHDOG);
+    if (!isfinite(rr)) st |= FEM_ERR_NONFINITE;
+    if (k >= A.maxiter) st |= FEM_ERR_MAXITER;
+    if (k < 0) st |= FEM_ERR_BREAKDOWN;
+    *A.iters = k;
+    *A.status = st;
+  }
+}
+
+
+
+int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s) {
+  BiArgs a = A;
+  void* args[] = {&a};
+  const void* fn = ncomp == 1 ? (const void*)k_bicgstab<1>
+                              : (ncomp == 2 ? (const void*)k_bicgstab<2> : (const void*)k_bicgstab<3>);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(FEM_THREADS);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelExC(&cfg, fn, args);
+  return fem_after_launch("k_bicgstab");
+}
+int fem_coop_occupancy_bi(int* occ) {
+  int a = 0, b = 0, c = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_bicgstab<1>, FEM_THREADS, 0) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_bicgstab<2>, FEM_THREADS, 0) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_bicgstab<3>, FEM_THREADS, 0) != cudaSuccess) return -1;
+  int m = a < b ? a : b;
+  *occ = m < c ? m : c;
+  return 0;
+}

@@ -1,0 +1,278 @@
+// Persistent cooperative (P)CG kernel with the multigrid V-cycle preconditioner.
+#include "fem_args.cuh"
+
+
+// Preconditioner application z = M r; returns gamma = r . z.
+__device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer& gr, const CgArgs& A, double* smem,
+                              double* bstore, double* cg_r, double* cg_p, double* cg_q, double rr, double r2d,
+                              double& gamma, double& mz) {
+  const MgLevel& L0 = A.lv[0];
+  const int nn = L0.g.nn;
+  mz = 0.0;
+  if (A.prec == FEM_PREC_NONE) {
+    gamma = rr;
+    return true;
+  }
+  if (A.prec == FEM_PREC_JACOBI) {
+    gamma = r2d;
+    return true;
+  }
+  if (A.prec == FEM_PREC_MG) {
+    if (!mg_vcycle(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return false;
+    double s[2];
+    gr.result<2>(s, SL_X(0), smem);
+    if (A.pinned) {
+      gamma = s[1];
+    } else {
+      double rs[2];
+      gr.result<2>(rs, SL_R(0), smem);
+      mz = s[0] / nn;
+      gamma = s[1] - mz * rs[0];
+    }
+    return true;
+  }
+  // approximate inverse: 2-term Neumann series
+  const bool pt = (A.prec == FEM_PREC_APPROX_INV_PT);
+  const double* __restrict__ r = A.r;
+  const double* __restrict__ D = L0.diag;
+  const uint8_t* __restrict__ ap = A.ai_pin;
+  double* __restrict__ T = L0.t;
+  for (int i = gt.rank(); i < nn; i += gt.size()) {
+    double d1l = fem_gather_fn(L0.g, i, MatShared{L0.Le, 1.0}, [&](int j) { return r[j] / D[j]; }) / D[i];
+    if (ap && ap[i]) d1l = pt ? r[i] / D[i] : 0.0;
+    T[i] = d1l;
+  }
+  if (!gt.sync()) return false;
+  double acc[1] = {0.0};
+  for (int i = gt.rank(); i < nn; i += gt.size()) {
+    double t = fem_gather_fn(L0.g, i, MatShared{L0.Le, 1.0}, [&](int j) { return T[j]; });
+    if (ap && ap[i]) t = pt ? T[i] : 0.0;
+    const double zi = 3 * (r[i] / D[i]) - 3 * T[i] + t / D[i];
+    A.z[i] = zi;
+    acc[0] += r[i] * zi;
+  }
+  gr.reduce<1>(acc, SL_RZ, smem);
+  if (!gt.sync()) return false;
+  double s[1];
+  gr.result<1>(s, SL_RZ, smem);
+  gamma = s[0];
+  return true;
+}
+
+__global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q) {
+  __shared__ double smem[128];
+  __shared__ double bstore[FEM_NSLOTS];
+  __shared__ __align__(16) CgArgs sA;
+  fem_stage_args(Aparam, &sA);
+  const CgArgs& A = sA;
+  const GridTeam gt{A.sync};
+  const GridReducer gr{A.sync};
+  const MgLevel& L0 = A.lv[0];
+  const FemGrid& g = L0.g;
+  const int nn = g.nn;
+  const uint8_t* pin0 = A.pinned ? L0.pin : nullptr;
+  const double* __restrict__ D = L0.diag;
+  int k = 0;
+  double rr = 0.0;
+  fem_zero_partials(A.sync);
+  if (!gt.sync()) goto done;
+  {
+    const double* b = A.b;
+    if (A.center_rhs) {
+      double a[1] = {0.0};
+      for (int i = gt.rank(); i < nn; i += gt.size()) a[0] += b[i];
+      gr.reduce<1>(a, SL_BSUM, smem);
+      if (!gt.sync()) goto done;
+      double s[1];
+      gr.result<1>(s, SL_BSUM, smem);
+      const double m = s[0] / nn;
+      for (int i = gt.rank(); i < nn; i += gt.size()) A.bwork[i] = b[i] - m;
+      b = A.bwork;
+    }
+    // r0 = b - A x0
+    {
+      double a2[2] = {0.0, 0.0}, a3[2] = {0.0, 0.0}, a1[1] = {0.0};
+      for (int i = gt.rank(); i < nn; i += gt.size()) {
+        double Ax = fem_gather_fn(g, i, MatShared{L0.Le, 1.0}, [&](int j) { return A.x[j]; });
+        if (pin0 && pin0[i]) Ax = 0.0;
+        const double bi = b[i], ri = bi - Ax;
+        A.r[i] = ri;
+        a2[0] += bi * bi;
+        a2[1] += ri * ri;
+        a3[0] += ri;
+        a3[1] += ri / D[i];
+        a1[0] += ri * ri / D[i];
+      }
+      gr.reduce<2>(a2, SL_BB, smem);
+      gr.reduce<2>(a3, SL_R(0), smem);
+      gr.reduce<1>(a1, SL_RZ, smem);
+      if (!gt.sync()) goto done;
+    }
+    double bb_rr[2], r2d[1];
+    gr.result<2>(bb_rr, SL_BB, smem);
+    gr.result<1>(r2d, SL_RZ, smem);
+    rr = bb_rr[1];
+    const double atol2 = fmax(A.tol * A.tol * bb_rr[0], A.atol * A.atol);
+    double gamma, mz;
+    if (!cg_apply_prec(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, r2d[0], gamma, mz)) goto done;
+    double beta = 0.0;
+    bool have_p = false;
+    int cur = 0;
+    double rs = (A.prec == FEM_PREC_NONE) ? gamma : rr;
+    const unsigned long long t_start = fem_globaltimer_early();
+    while (rs > atol2 && k < A.maxiter) {
+      if (fem_watchdog_fired(A.sync.err)) break;
+      double* __restrict__ pold = cur ? A.p1 : A.p0;
+      double* __restrict__ pnew = cur ? A.p0 : A.p1;
+      const int prec = A.prec;
+      const double* __restrict__ r = A.r;
+      const double* __restrict__ zs = (prec == FEM_PREC_MG) ? L0.x : A.z;
+      auto zval = [&](int j) -> double {
+        if (prec == FEM_PREC_NONE) return r[j];
+        if (prec == FEM_PREC_JACOBI) return r[j] / D[j];
+        if (prec == FEM_PREC_MG) return zs[j] - mz;
+        return zs[j];
+      };
+      auto pz = [&](int j) -> double { return have_p ? zval(j) + beta * pold[j] : zval(j); };
+      {
+        double a[1] = {0.0};
+        for (int i = gt.rank(); i < nn; i += gt.size()) {
+          const double pn = pz(i);
+          pnew[i] = pn;
+          double q = fem_gather_fn(g, i, MatShared{L0.Le, 1.0}, pz);
+          if (pin0 && pin0[i]) q = 0.0;
+          A.Ap[i] = q;
+          a[0] += pn * q;
+        }
+        gr.reduce<1>(a, SL_PAP, smem);
+        if (!gt.sync()) goto done;
+      }
+      double pap[1];
+      gr.result<1>(pap, SL_PAP, smem);
+      const double alpha = gamma / pap[0];
+      {
+        double a2[2] = {0.0, 0.0}, a3[2] = {0.0, 0.0}, a1[1] = {0.0};
+        for (int i = gt.rank(); i < nn; i += gt.size()) {
+          A.x[i] = A.x[i] + alpha * pnew[i];
+          const double ri = A.r[i] - alpha * A.Ap[i];
+          A.r[i] = ri;
+          a2[1] += ri * ri;
+          a3[0] += ri;
+          a3[1] += ri / D[i];
+          a1[0] += ri * ri / D[i];
+        }
+        gr.reduce<2>(a2, SL_BB, smem);
+        gr.reduce<2>(a3, SL_R(0), smem);
+        gr.reduce<1>(a1, SL_RZ, smem);
+        fem_watchdog_arm(A.sync.err, t_start);
+        if (!gt.sync()) goto done;
+      }
+      ++k;
+      double t2[2], t1[1];
+      gr.result<2>(t2, SL_BB, smem);
+      gr.result<1>(t1, SL_RZ, smem);
+      rr = t2[1];
+      double gamma_;
+      if (prec == FEM_PREC_NONE) {
+        gamma_ = rr;
+      } else if (prec == FEM_PREC_JACOBI) {
+        gamma_ = t1[0];
+      } else {
+        if (!(rr > atol2 && k < A.maxiter)) break;  // z of a final iteration is never used
+        if (!cg_apply_prec(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, t1[0], gamma_, mz)) goto done;
+      }
+      beta = gamma_ / gamma;
+      gamma = gamma_;
+      have_p = true;
+      cur ^= 1;
+      rs = (prec == FEM_PREC_NONE) ? gamma : rr;
+      if (!isfinite(rs)) break;
+    }
+    // final modification of solvers/standard.py:119-123
+    if (A.post) {
+      if (A.pinned) {
+        for (int i = gt.rank(); i < nn; i += gt.size())
+          if (pin0 && pin0[i]) A.x[i] = 0.0;
+      } else {
+        double a[1] = {0.0};
+        for (int i = gt.rank(); i < nn; i += gt.size()) a[0] += A.x[i];
+        gr.reduce<1>(a, SL_BSUM, smem);
+        if (!gt.sync()) goto done;
+        double s[1];
+        gr.result<1>(s, SL_BSUM, smem);
+        const double m = s[0] / nn;
+        for (int i = gt.rank(); i < nn; i += gt.size()) A.x[i] = A.x[i] - m;
+      }
+    }
+  }
+done:
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int st = *(volatile int*)A.sync.err & (FEM_ERR_BARRIER_TIMEOUT | FEM_ERR_WATCHDOG);
+    if (!isfinite(rr)) st |= FEM_ERR_NONFINITE;
+    if (k >= A.maxiter) st |= FEM_ERR_MAXITER;
+    *A.iters = k;
+    *A.status = st;
+    if (A.final_rr) *A.final_rr = rr;
+  }
+}
+
+
+
+__global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q,
+                                                            double* z) {
+  __shared__ double smem[128];
+  __shared__ double bstore[FEM_NSLOTS];
+  __shared__ __align__(16) CgArgs sA;
+  fem_stage_args(Aparam, &sA);
+  const CgArgs& A = sA;
+  const GridTeam gt{A.sync};
+  const GridReducer gr{A.sync};
+  const MgLevel& L0 = A.lv[0];
+  const int nn = L0.g.nn;
+  fem_zero_partials(A.sync);
+  if (!gt.sync()) return;
+  double a[2] = {0.0, 0.0};
+  for (int i = gt.rank(); i < nn; i += gt.size()) {
+    a[0] += L0.r[i];
+    a[1] += L0.r[i] / L0.diag[i];
+  }
+  gr.reduce<2>(a, SL_R(0), smem);
+  if (!gt.sync()) return;
+  if (!mg_vcycle(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return;
+  double sx[2];
+  gr.result<2>(sx, SL_X(0), smem);
+  const double mz = A.pinned ? 0.0 : sx[0] / nn;
+  for (int i = gt.rank(); i < nn; i += gt.size()) z[i] = L0.x[i] - mz;
+}
+
+static int coop_launch(const void* fn, int grid, void** args, cudaStream_t s, const char* what) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(FEM_THREADS);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelExC(&cfg, fn, args);
+  return fem_after_launch(what);
+}
+
+int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s) {
+  CgArgs a = A;
+  void* args[] = {&a, &cr, &cp, &cq};
+  return coop_launch((const void*)k_cg, grid, args, s, "k_cg");
+}
+int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s) {
+  CgArgs a = A;
+  void* args[] = {&a, &cr, &cp, &cq, &z};
+  return coop_launch((const void*)k_vcycle, grid, args, s, "k_vcycle");
+}
+int fem_coop_occupancy_cg(int* occ) {
+  int a = 0, b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg, FEM_THREADS, 0) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_vcycle, FEM_THREADS, 0) != cudaSuccess) return -1;
+  *occ = a < b ? a : b;
+  return 0;
+}

@@ -1,0 +1,317 @@
+// Element-product, element-matrix, transfer, boundary and blas-1 kernels.
+#include "fem_args.cuh"
+
+
+template <int NC>
+__global__ void __launch_bounds__(FEM_OP_THREADS) k_ebe_apply(FemGrid g, MatCombo m, const double* __restrict__ x,
+                                                              double* __restrict__ y) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    double v[NC];
+    fem_gather<NC>(g, n, m, x, g.nn, v);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) y[n + (size_t)c * g.nn] = v[c];
+  }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(FEM_OP_THREADS) k_grad(FemGrid g, const double* __restrict__ Ge,
+                                                         const double* __restrict__ P, double* __restrict__ y) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    double v[ND];
+    fem_gather_grad<ND>(g, n, Ge, P, v);
+#pragma unroll
+    for (int d = 0; d < ND; ++d) y[n + (size_t)d * g.nn] = v[d];
+  }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(FEM_OP_THREADS) k_div(FemGrid g, const double* __restrict__ Ge,
+                                                        const double* __restrict__ U, double* __restrict__ y) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x)
+    y[n] = fem_gather_div<ND>(g, n, Ge, U, g.nn);
+}
+
+// Ce / Ctau_tilde build, FEM_CE_EPB elements per CTA.
+__global__ void __launch_bounds__(FEM_OP_THREADS) k_convection(FemGrid g, FemQuad Q, const double* __restrict__ U,
+                                                               double beta, int mode, double* __restrict__ Ce) {
+  __shared__ double s_uq[FEM_CE_EPB * 9 * 3];
+  __shared__ double s_div[FEM_CE_EPB * 9];
+  __shared__ double s_T[FEM_CE_EPB * 9 * 9];
+  for (int e0 = blockIdx.x * FEM_CE_EPB; e0 < g.ne; e0 += gridDim.x * FEM_CE_EPB)
+    fem_convection_block(g, Q, U, beta, Ce, e0, mode, s_uq, s_div, s_T);
+}
+
+// core/element_calc.py:202-229 (per-element tau, r-norm blend).
+__global__ void k_supg_tau(FemGrid g, FemQuad Q, const double* __restrict__ U, const double* __restrict__ Ce,
+                           const double* __restrict__ Ct, double D, double dt, double r, double* __restrict__ tau) {
+  const int nen = g.nen, nq = Q.nq, nd = Q.ndim, per = nen * nen;
+  D = D + 1e-6;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.ne; e += gridDim.x * blockDim.x) {
+    const int ie = e % g.nex, rr = e / g.nex, je = rr % g.ney, ke = rr / g.ney;
+    double ce2 = 0.0, kt2 = 0.0;
+    for (int t = 0; t < per; ++t) {
+      const double c = Ce[(size_t)e * per + t], k = Ct[(size_t)e * per + t];
+      ce2 += c * c;
+      kt2 += k * k;
+    }
+    const double ce_n = sqrt(ce2), kt_n = sqrt(kt2);
+    double un2 = 0.0;
+    for (int q = 0; q < nq; ++q) {
+      double s = 0.0;
+      for (int d = 0; d < nd; ++d) {
+        double uq = 0.0;
+        for (int I = 0; I < nen; ++I) uq += Q.N[q * nen + I] * U[fem_elem_node(g, ie, je, ke, I) + (size_t)d * g.nn];
+        s += uq * uq;
+      }
+      un2 += s;
+    }
+    un2 /= nq;
+    const double Re = (un2 * ce_n) / (D * kt_n);
+    const double t1 = ce_n / kt_n, t2 = dt / 2, t3 = t1 * Re;
+    tau[e] = pow(1 / pow(t1, r) + 1 / pow(t2, r) + 1 / pow(t3, r), -1 / r);
+  }
+}
+
+// Combined per-element matrix for the SUPG scalar operator:
+// out_e = s_m * tau_e * Cn_e^T + s_c * (C_e + tau_e * Ct_e)   (transport lhs/rhs).
+__global__ void k_supg_combine(int ne, int nen, const double* __restrict__ tau, const double* __restrict__ Cn,
+                               const double* __restrict__ C, const double* __restrict__ Ct, double s_m, double s_c,
+                               double* __restrict__ out) {
+  const int per = nen * nen;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)ne * per; t += gridDim.x * blockDim.x) {
+    const size_t e = t / per;
+    const int ab = (int)(t % per), a = ab / nen, b = ab % nen;
+    out[t] = s_m * (tau[e] * Cn[e * per + b * nen + a]) + s_c * (C[t] + tau[e] * Ct[t]);
+  }
+}
+
+// ------------------------------------------------------------- transfers ----
+__global__ void k_interp(FemLattice H, FemLattice h, const double* __restrict__ xH, double* __restrict__ xh) {
+  const int ux = h.ux(), n = ux * h.uy();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    xh[i] = fem_interp_at(H, i / ux, i % ux, [&](int I) { return xH[I]; });
+}
+
+__global__ void k_restrict(FemLattice h, FemLattice H, const double* __restrict__ xh, double* __restrict__ xH) {
+  const int ux = H.ux(), n = ux * H.uy();
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x)
+    xH[I] = fem_restrict_at(h, I / ux, I % ux, [&](int j) { return xh[j]; });
+}
+
+// ------------------------------------------------------------- boundary flux --
+// Per boundary face: Fe_I = sum_q (N w)[q][I] (n . U_q); then a single-thread
+// scatter in face order (segment_sum order of core/element_calc.py:131-133).
+__global__ void k_boundary_fe(const double* __restrict__ coords, int dim, const int32_t* __restrict__ bconn,
+                              const double* __restrict__ nvec, int nb, int npf, const double* __restrict__ U, int nn,
+                              double* __restrict__ Fe) {
+  const double s3 = 1.0 / sqrt(3.0), g35 = sqrt(3.0 / 5.0);
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nb; f += gridDim.x * blockDim.x) {
+    const int32_t* nd = bconn + (size_t)f * npf;
+    double nrm[3] = {nvec[f * dim], nvec[f * dim + 1], dim == 3 ? nvec[f * dim + 2] : 0.0};
+    double Ub[4][3];
+    for (int I = 0; I < npf; ++I)
+      for (int d = 0; d < 3; ++d) Ub[I][d] = (d < dim) ? U[nd[I] + (size_t)d * nn] : 0.0;
+    double out[4] = {0, 0, 0, 0};
+    if (npf == 2) {  // lin2
+      const double ddx = coords[nd[1] * dim] - coords[nd[0] * dim], ddy = coords[nd[1] * dim + 1] - coords[nd[0] * dim + 1];
+      const double h = sqrt(ddx * ddx + ddy * ddy);
+      for (int q = 0; q < 2; ++q) {
+        const double xi = (q == 0 ? -1.0 : 1.0) * s3;
+        const double Nq[2] = {(1 - xi) / 2, (1 + xi) / 2};
+        const double w = 1.0 * (h / 2);
+        double un = 0.0;
+        for (int d = 0; d < 2; ++d) un += nrm[d] * (Nq[0] * Ub[0][d] + Nq[1] * Ub[1][d]);
+        for (int I = 0; I < 2; ++I) out[I] += (Nq[I] * w) * un;
+      }
+    } else if (npf == 3) {  // lin3
+      const double gp[3] = {-g35, 0.0, g35}, w1[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+      for (int q = 0; q < 3; ++q) {
+        const double xi = gp[q];
+        const double Nq[3] = {xi * (xi - 1) / 2, 1 - xi * xi, xi * (xi + 1) / 2};
+        const double dv[3] = {(2 * xi - 1) / 2, -2 * xi, (2 * xi + 1) / 2};
+        double jx = 0, jy = 0;
+        for (int a = 0; a < 3; ++a) {
+          jx += dv[a] * coords[nd[a] * dim];
+          jy += dv[a] * coords[nd[a] * dim + 1];
+        }
+        const double w = w1[q] * sqrt(jx * jx + jy * jy);
+        double un = 0.0;
+        for (int d = 0; d < 2; ++d) un += nrm[d] * (Nq[0] * Ub[0][d] + Nq[1] * Ub[1][d] + Nq[2] * Ub[2][d]);
+        for (int I = 0; I < 3; ++I) out[I] += (Nq[I] * w) * un;
+      }
+    } else {  // quad4 face of a hex: in-plane axes are those orthogonal to the normal
+      int ax[2], na = 0;
+      for (int d = 0; d < 3 && na < 2; ++d)
+        if (nrm[d] == 0.0) ax[na++] = d;
+      const double sx[4] = {-1, 1, 1, -1}, sy[4] = {-1, -1, 1, 1};
+      for (int q = 0; q < 4; ++q) {
+        const double xi = sx[q] * s3, eta = sy[q] * s3;
+        double Nq[4], dxi[4], deta[4];
+        for (int a = 0; a < 4; ++a) {
+          Nq[a] = (1 + sx[a] * xi) * (1 + sy[a] * eta) / 4;
+          dxi[a] = sx[a] * (1 + sy[a] * eta) / 4;
+          deta[a] = sy[a] * (1 + sx[a] * xi) / 4;
+        }
+        double J[2][2] = {{0, 0}, {0, 0}};
+        for (int a = 0; a < 4; ++a)
+          for (int d = 0; d < 2; ++d) {
+            J[0][d] += dxi[a] * coords[nd[a] * dim + ax[d]];
+            J[1][d] += deta[a] * coords[nd[a] * dim + ax[d]];
+          }
+        const double w = fabs(J[0][0] * J[1][1] - J[0][1] * J[1][0]);
+        double un = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          double uq = 0.0;
+          for (int a = 0; a < 4; ++a) uq += Nq[a] * Ub[a][d];
+          un += nrm[d] * uq;
+        }
+        for (int I = 0; I < 4; ++I) out[I] += (Nq[I] * w) * un;
+      }
+    }
+    for (int I = 0; I < npf; ++I) Fe[(size_t)f * npf + I] = out[I];
+  }
+}
+
+__global__ void k_boundary_scatter(const int32_t* __restrict__ bconn, int nb, int npf, const double* __restrict__ Fe,
+                                   int nn, double* __restrict__ F) {
+  // one CTA: zero, then a serial scatter in face order (deterministic)
+  for (int i = threadIdx.x; i < nn; i += blockDim.x) F[i] = 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int t = 0; t < nb * npf; ++t) F[bconn[t]] += Fe[t];
+}
+
+// ---------------------------------------------------------------- blas-1 ----
+__global__ void k_dot_partial(const double* __restrict__ x, const double* __restrict__ y, int n,
+                              double* __restrict__ part) {
+  __shared__ double smem[96];
+  double a[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[0] += x[i] * y[i];
+  fem_block_sum<1>(a, smem);
+  if (threadIdx.x == 0) part[blockIdx.x] = a[0];
+}
+__global__ void k_dot_final(const double* __restrict__ part, int np, double* __restrict__ out) {
+  __shared__ double smem[96];
+  double a[1] = {0.0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x) a[0] += part[i];
+  fem_block_sum<1>(a, smem);
+  if (threadIdx.x == 0) out[0] = a[0];
+}
+__global__ void k_axpby(double a, const double* __restrict__ x, double b, double* __restrict__ y, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * x[i] + b * y[i];
+}
+
+
+__global__ void k_lincomb(int n, double a, const double* __restrict__ X, double b, const double* __restrict__ Y,
+                          double* __restrict__ out) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) out[i] = a * X[i] + b * Y[i];
+}
+
+__global__ void k_scale_elem(int ne, int nen, const double* __restrict__ tau, const double* __restrict__ X, int trans,
+                             double* __restrict__ out) {
+  const int per = nen * nen;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)ne * per; t += gridDim.x * blockDim.x) {
+    const size_t e = t / per;
+    const int ab = (int)(t % per), a = ab / nen, b = ab % nen;
+    out[t] = tau[e] * (trans ? X[e * per + b * nen + a] : X[t]);
+  }
+}
+
+// out = s_m * Mt + s_c * (C + Ct)   (per element, flat)
+__global__ void k_elem_combine(size_t n, double s_m, const double* __restrict__ Mt, double s_c,
+                               const double* __restrict__ C, const double* __restrict__ Ct, double* __restrict__ out) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    out[t] = s_m * Mt[t] + s_c * (C[t] + Ct[t]);
+}
+
+int fem_launch_ebe(int ncomp, const FemGrid& g, const MatCombo& m, const double* x, double* y, cudaStream_t s) {
+  const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
+  if (ncomp == 1) k_ebe_apply<1><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
+  else if (ncomp == 2) k_ebe_apply<2><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
+  else k_ebe_apply<3><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
+  return fem_after_launch("k_ebe_apply");
+}
+int fem_launch_grad(int ndim, const FemGrid& g, const double* Ge, const double* P, double* y, cudaStream_t s) {
+  const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
+  if (ndim == 2) k_grad<2><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, P, y);
+  else k_grad<3><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, P, y);
+  return fem_after_launch("k_grad");
+}
+int fem_launch_div(int ndim, const FemGrid& g, const double* Ge, const double* U, double* y, cudaStream_t s) {
+  const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
+  if (ndim == 2) k_div<2><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, U, y);
+  else k_div<3><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, U, y);
+  return fem_after_launch("k_div");
+}
+int fem_launch_convection(const FemGrid& g, const FemQuad& Q, const double* U, double beta, int mode, double* out,
+                          cudaStream_t s) {
+  const int nb = fem_nblocks((g.ne + FEM_CE_EPB - 1) / FEM_CE_EPB, 1, 148 * 32);
+  k_convection<<<nb, FEM_OP_THREADS, 0, s>>>(g, Q, U, beta, mode, out);
+  return fem_after_launch("k_convection");
+}
+int fem_launch_supg_tau(const FemGrid& g, const FemQuad& Q, const double* U, const double* Ce, const double* Ct,
+                        double D, double dt, double r, double* tau, cudaStream_t s) {
+  k_supg_tau<<<fem_nblocks(g.ne, 128), 128, 0, s>>>(g, Q, U, Ce, Ct, D, dt, r, tau);
+  return fem_after_launch("k_supg_tau");
+}
+int fem_launch_scale_elem(int ne, int nen, const double* tau, const double* X, int trans, double* out, cudaStream_t s) {
+  k_scale_elem<<<fem_nblocks((long long)ne * nen * nen, 256), 256, 0, s>>>(ne, nen, tau, X, trans, out);
+  return fem_after_launch("k_scale_elem");
+}
+int fem_launch_elem_combine(size_t n, double s_m, const double* Mt, double s_c, const double* C, const double* Ct,
+                            double* out, cudaStream_t s) {
+  k_elem_combine<<<fem_nblocks((long long)n, 256), 256, 0, s>>>(n, s_m, Mt, s_c, C, Ct, out);
+  return fem_after_launch("k_elem_combine");
+}
+int fem_launch_lincomb(int n, double a, const double* X, double b, const double* Y, double* out, cudaStream_t s) {
+  k_lincomb<<<1, 128, 0, s>>>(n, a, X, b, Y, out);
+  return fem_after_launch("k_lincomb");
+}
+int fem_launch_interp(const FemLattice& H, const FemLattice& h, const double* xH, double* xh, cudaStream_t s) {
+  k_interp<<<fem_nblocks((long long)h.nx * h.ny, 256), 256, 0, s>>>(H, h, xH, xh);
+  return fem_after_launch("k_interp");
+}
+int fem_launch_restrict(const FemLattice& h, const FemLattice& H, const double* xh, double* xH, cudaStream_t s) {
+  k_restrict<<<fem_nblocks((long long)H.nx * H.ny, 256), 256, 0, s>>>(h, H, xh, xH);
+  return fem_after_launch("k_restrict");
+}
+int fem_launch_boundary(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
+                        const double* U, int nn, double* Fe, double* Fp, cudaStream_t s) {
+  if (nb > 0) {
+    k_boundary_fe<<<fem_nblocks(nb, 128), 128, 0, s>>>(coords, dim, bconn, nvec, nb, npf, U, nn, Fe);
+    if (int rc = fem_after_launch("k_boundary_fe")) return rc;
+  }
+  k_boundary_scatter<<<1, 512, 0, s>>>(bconn, nb, npf, Fe, nn, Fp);
+  return fem_after_launch("k_boundary_scatter");
+}
+int fem_launch_dot(const double* x, const double* y, int n, double* part, double* out, cudaStream_t s) {
+  const int nb = fem_nblocks(n, 256, 1024);
+  k_dot_partial<<<nb, 256, 0, s>>>(x, y, n, part);
+  if (int rc = fem_after_launch("k_dot_partial")) return rc;
+  k_dot_final<<<1, 256, 0, s>>>(part, nb, out);
+  return fem_after_launch("k_dot_final");
+}
+int fem_launch_axpby(double a, const double* x, double b, double* y, int n, cudaStream_t s) {
+  k_axpby<<<fem_nblocks(n, 256), 256, 0, s>>>(a, x, b, y, n);
+  return fem_after_launch("k_axpby");
+}
+
+__global__ void k_scatter(const int64_t* __restrict__ idx, const double* __restrict__ vals, double value, int n,
+                          double* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    out[idx[k]] = vals ? vals[k] : value;
+}
+__global__ void k_make_mask(const int64_t* __restrict__ idx, int n, int len, uint8_t* __restrict__ mask) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int64_t i = idx[k];
+    if (i >= 0 && i < len) mask[i] = 1;
+  }
+}
+int fem_launch_scatter(const int64_t* idx, const double* vals, double value, int n, double* out, cudaStream_t s) {
+  k_scatter<<<fem_nblocks(n, 256), 256, 0, s>>>(idx, vals, value, n, out);
+  return fem_after_launch("k_scatter");
+}
+int fem_launch_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cudaStream_t s) {
+  k_make_mask<<<fem_nblocks(n, 256), 256, 0, s>>>(idx, n, len, mask);
+  return fem_after_launch("k_make_mask");
+}

@@ -1,0 +1,258 @@
+"""GPU parity: every hot-path operator and solver of jax_fem_cfd_b200 (through the
+C ABI) against the CPU oracle on the same seeded inputs, FP64.
+
+Tolerances: element data and single products 1e-13 relative (summation order
+differs from numpy's); tolerance-terminated solves 1e-10 relative with equal
+iteration counts (the bar of the FP64 path)."""
+import numpy as np
+import pytest
+import torch
+
+from tests.conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+OPS_TOL = 1e-13
+SOLVE_TOL = 1e-10
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+    b = b.detach().cpu().numpy() if isinstance(b, torch.Tensor) else np.asarray(b)
+    a, b = a.astype(float), b.astype(float)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def np_(t):
+    return t.detach().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+
+
+MESHES = [("create_mesh_2d", (5, 4, 2.0, 1.0)), ("create_mesh_2d_quad9", (4, 3, 1.0, 1.5)),
+          ("create_periodic_mesh_2d", (6, 4, 2 * np.pi, 2 * np.pi)),
+          ("create_periodic_mesh_2d_quad9", (4, 4, 2 * np.pi, 2 * np.pi)), ("create_mesh_3d", (3, 3, 2, 1.0, 1.0, 0.5))]
+
+
+@pytest.mark.parametrize("fn,args", MESHES)
+def test_mesh_generation(fn, args):
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from oracle import mesh as om
+    nc, nconn, sn, bc, nv = getattr(rm, fn)(*args)
+    onc, onconn, osn, obc, onv = getattr(om, fn)(*args)
+    np.testing.assert_array_equal(np_(nconn), onconn)
+    np.testing.assert_allclose(np_(nc), onc, rtol=0, atol=1e-15)
+    if osn is not None:
+        for f in range(len(osn)):
+            np.testing.assert_array_equal(np_(sn[f]), osn[f])
+    if fn != "create_mesh_3d" and obc is not None:
+        for f in range(len(obc)):
+            np.testing.assert_array_equal(np_(bc[f]), obc[f])
+
+
+@pytest.mark.parametrize("key", ["q1", "q2", "q1p", "q2p", "hex"])
+def test_element_data_and_products(key):
+    """Element matrices, Ce / Ctau / tau and every element product vs the goldens."""
+    from jax_fem_cfd_b200.core import element_calc as ec
+    from jax_fem_cfd_b200.core import element_mult as em
+    from jax_fem_cfd_b200.core import shape_functions as sf
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    g = load_golden(f"elem_{key}")
+    fn, args = dict(q1=MESHES[0], q2=MESHES[1], q1p=MESHES[2], q2p=MESHES[3], hex=MESHES[4])[key]
+    nc, nconn, *_ = getattr(rm, fn)(*args)
+    nn, ndim = int(g["nn"]), int(g["ndim"])
+    shp = {"q1": sf.quad4_shape_functions, "q2": sf.quad9_shape_functions, "q1p": sf.quad4_shape_functions,
+           "q2p": sf.quad9_shape_functions, "hex": sf.hex8_shape_functions}[key]
+    wq, N, Nd = shp(nc[nconn[0]])
+    assert rel(wq, g["wq"]) < OPS_TOL and rel(N, g["N"]) < OPS_TOL and rel(Nd, g["Nderiv"]) < OPS_TOL
+    Le = ec.laplacian_element_calc(wq, Nd)
+    Ge = ec.gradient_element_calc(wq, N, Nd, ndim)
+    M, Me = ec.lumped_mass_matrix(nconn, wq, N, nn, ndim)
+    out = dict(Le=Le, Ge=Ge, M=M, Me=Me, L_diag=ec.laplacian_diag(Le, nconn, nn))
+    U, P, phi = g["U"], g["P"], g["phi"]
+    Ce05 = ec.conservative_convec_elem_calc(nconn, U, wq, N, Nd, nn, ndim, 0.5)
+    Ce1 = ec.conservative_convec_elem_calc(nconn, U, wq, N, Nd, nn, ndim, 1)
+    out.update(Ce05=Ce05, Ce1=Ce1, lap=em.laplacian_element_mult(P, Le, nconn, nn),
+               grad=em.gradient_element_mult(P, Ge, nconn, nn, ndim),
+               div=em.divergence_element_mult(U, Ge, nconn, nn, ndim),
+               viscconv=em.visc_conv_mult(U, Ce05, Le, 0.013, 1.7, nconn, nn, ndim),
+               scalar_vc=em.scalar_visc_conv_mult(phi, Ce1, Le, 1e-3, nconn, nn),
+               mass1=em.consistent_mass_mult(phi, Me, nconn, nn, 1))
+    if ndim == 2:
+        Ct = ec.Ctau_tilde_elem_calc(nconn, U, wq, N, Nd, nn, ndim)
+        tau = ec.calculate_tau(nconn, U, Ce1, Ct, N, nn, ndim, 1e-4, 1e-2, 2)
+        tau_np = np_(tau)
+        Mtau = torch.as_tensor(tau_np[:, None, None] * np_(Ce1).transpose(0, 2, 1)).cuda()
+        Ctau = torch.as_tensor(tau_np[:, None, None] * np_(Ct)).cuda()
+        out.update(mass=em.consistent_mass_mult(U, Me, nconn, nn, ndim), Ctau_tilde=Ct, tau=tau,
+                   stab_vc=em.scalar_stabilized_visc_conv_mult(phi, Ce1, Ctau, Le, 1e-3, nconn, nn),
+                   supg_mass=em.scalar_consistent_mass_SUPG_mult(phi, Mtau, Me, nconn, nn))
+    for name, val in out.items():
+        err = rel(val.reshape(g[name].shape), g[name])
+        assert err < OPS_TOL, (key, name, err)
+
+
+@pytest.mark.parametrize("key", ["q1", "q2", "q1p", "q2p"])
+def test_multigrid_transfers_and_vcycle(key):
+    from jax_fem_cfd_b200.core import multigrid as mg
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from jax_fem_cfd_b200.core import shape_functions as sf
+    g = load_golden(f"mg_{key}")
+    order, periodic, setzero = int(g["order"]), bool(g["periodic"]), bool(g["setzero"])
+    lvl = tuple(tuple(int(v) for v in r) for r in g["lvl_nums"])
+    assert rel(mg.interpolation_operator(g["xH"], lvl[2][1], lvl[2][2], lvl[1][1], lvl[1][2], periodic),
+               g["interp"]) < OPS_TOL
+    assert rel(mg.restriction_operator(g["xh"], lvl[1][1], lvl[1][2], lvl[2][1], lvl[2][2], periodic),
+               g["restrict"]) < OPS_TOL
+    if order == 1:
+        mf, shp = (rm.create_periodic_mesh_2d if periodic else rm.create_mesh_2d), sf.quad4_shape_functions
+    else:
+        mf, shp = (rm.create_periodic_mesh_2d_quad9 if periodic else rm.create_mesh_2d_quad9), sf.quad9_shape_functions
+    data = mg.multigrid_setup(list(g["nel"]), list(g["fmg"]), list(g["dom"]), [], mf, shp, order, None)
+    assert data[0] == lvl
+    assert rel(data[1], g["Le_lvls"]) < OPS_TOL and rel(data[3], g["L_diag_lvls"]) < OPS_TOL
+    np.testing.assert_array_equal(np_(data[2]), g["nconn_lvls"])
+    z = mg.v_cycle(g["r"], *data, 1e-8, periodic, setzero)
+    assert rel(z, g["z"]) < (1e-9 if setzero else 1e-12), rel(z, g["z"])
+
+
+def test_generic_krylov_callables():
+    """utils.iterative_solvers.cg / bicgstab with callable operators vs the goldens."""
+    from jax_fem_cfd_b200.core import element_calc as ec
+    from jax_fem_cfd_b200.core import element_mult as em
+    from jax_fem_cfd_b200.core import shape_functions as sf
+    from jax_fem_cfd_b200.context import scatter_set
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from jax_fem_cfd_b200.utils import iterative_solvers as its
+    g = load_golden("krylov")
+    nc, nconn, sn, *_ = rm.create_mesh_2d(10, 10, 1.0, 1.0)
+    nn = nc.shape[0]
+    wq, N, Nd = sf.quad4_shape_functions(nc[nconn[0]])
+    Le = ec.laplacian_element_calc(wq, Nd)
+    _, Me = ec.lumped_mass_matrix(nconn, wq, N, nn, 2)
+    gp = g["gp"]
+
+    def lap(x):
+        return scatter_set(em.laplacian_element_mult(x, Le, nconn, nn), gp, 0.0)
+
+    x, k = its.cg(lap, g["b"], tol=1e-10, maxiter=1000)
+    assert k == int(g["k_cg"]) and rel(x, g["x_cg"]) < SOLVE_TOL
+    Ce = ec.conservative_convec_elem_calc(nconn, g["U"], wq, N, Nd, nn, 2, 0.5)
+
+    def mom(x):
+        a = em.consistent_mass_mult(x, Me, nconn, nn, 2)
+        b = em.visc_conv_mult(x, Ce, Le, 0.01, 1.0, nconn, nn, 2)
+        return its._lin(0.5, b, 100.0, a)
+
+    x, k = its.bicgstab(mom, g["bm"], tol=1e-10)
+    assert k == int(g["k_bi"]) and rel(x, g["x_bi"]) < SOLVE_TOL
+
+
+def _ns_cfg(mod, nel, dom, order, periodic, dfaces, precond, setzero, tol, fmg, outlet=()):
+    return mod.Config(mesh="simple", solver="standard",
+                      mesh_config=mod.SimpleMeshConfig(num_elem=nel, domain_size=dom, shape_func_ord=order,
+                                                       periodic=periodic),
+                      solver_config=mod.StandardSolverConfig(dirichlet_faces=dfaces, symmetry_faces=[],
+                                                             outlet_faces=list(outlet), streamline_diff=False,
+                                                             solver_tol=tol, set_zeroP=setzero,
+                                                             pressure_precond=precond, final_multigrid_mesh=fmg))
+
+
+STEP_CASES = {
+    "cavity_q1_mg": (([16, 16], [1, 1], 1, False, [0, 1, 2, 3], "multigrid", True, 1e-8, [4, 4]), "corners", 3,
+                     0.01, 0.01),
+    "cavity_q2_jacobi": (([8, 8], [1, 1], 2, False, [0, 1, 2, 3], "jacobi", True, 1e-8, None), "interior", 2, 0.01,
+                         0.01),
+    "cavity_q1_approxinv": (([12, 12], [1, 1], 1, False, [0, 1, 2, 3], "approx_inv", True, 1e-8, None), "corners",
+                            2, 0.01, 0.01),
+    "tg_q2p_mg": (([16, 16], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]), None, 3, 1e-3,
+                  0.01),
+    "tg_q1p_none": (([16, 16], [2 * np.pi, 2 * np.pi], 1, True, [], None, False, 1e-8, None), None, 2, 1e-2, 0.01),
+    "cavity64_q1_mg": (([64, 64], [1, 1], 1, False, [0, 1, 2, 3], "multigrid", True, 1e-8, [4, 4]), "corners", 5,
+                       0.01, 0.01),
+    "tg64_q2p_mg": (([64, 64], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]), None, 3,
+                    1e-3, 0.01),
+}
+
+
+def _run_steps(mod, args, lid, steps, dt, mu):
+    compute, timestep, nc, sn, h, nn, gd, Ud = mod.setup(_ns_cfg(mod, *args))
+    ncn = nc.detach().cpu().numpy() if isinstance(nc, torch.Tensor) else nc
+    if lid is not None:
+        nodes = sn[2] if lid == "corners" else sn[2][1:-1]
+        Ud = mod.set_face_velocity(Ud, nodes, gd, 1.0, nn, var=1)
+        U, P = np.zeros(2 * nn), np.zeros(nn)
+    else:
+        x, y = ncn[:, 0], ncn[:, 1]
+        U = np.concatenate([np.sin(x) * np.cos(y), -np.cos(x) * np.sin(y)])
+        P = 0.25 * (np.cos(2 * x) + np.cos(2 * y))
+        P = P - P.mean()
+    its = []
+    for s in range(steps):
+        Fp, F = compute(Ud, None, s * dt, (s + 1) * dt)
+        U, P, ui, pi = timestep(U, P, dt, 1.0, mu, Ud, Fp, F)
+        its.append((int(ui), int(pi)))
+    return np_(U), np_(P), its
+
+
+@pytest.mark.parametrize("case", list(STEP_CASES))
+def test_ns_step_parity(case):
+    """fem_step4 (one Ce build, one persistent BiCGSTAB, one persistent PCG per
+    step) vs the oracle's four_step_timestep: equal iteration counts, 1e-10."""
+    import oracle.simulation as osim
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    args, lid, steps, dt, mu = STEP_CASES[case]
+    Ug, Pg, ig = _run_steps(gsim, args, lid, steps, dt, mu)
+    Uo, Po, io = _run_steps(osim, args, lid, steps, dt, mu)
+    assert ig == io, (ig, io)
+    assert rel(Ug, Uo) < SOLVE_TOL, rel(Ug, Uo)
+    assert rel(Pg, Po) < SOLVE_TOL, rel(Pg, Po)
+
+
+@pytest.mark.parametrize("supg", [True, False])
+def test_passive_transport_step(supg):
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    g = load_golden(f"step_transport_{'supg' if supg else 'plain'}")
+    cfg = gsim.Config(mesh="simple", solver="passive_transport",
+                      mesh_config=gsim.SimpleMeshConfig(num_elem=[12, 12], domain_size=[1, 1], shape_func_ord=1,
+                                                        periodic=False),
+                      solver_config=gsim.PassiveTransportConfig(
+                          gsim.StandardSolverConfig(dirichlet_faces=[0, 1, 2, 3], symmetry_faces=[], outlet_faces=[],
+                                                    streamline_diff=False, solver_tol=1e-8, set_zeroP=True,
+                                                    pressure_precond="multigrid", final_multigrid_mesh=[3, 3]),
+                          gsim.ADEConfig(phi_dirichlet_faces=[], phi_SUPG=supg)))
+    compute, timestep, nc, sn, h, nn, nnx, nny, gd, Ud, gdp = gsim.setup(cfg)
+    U, P, phi = g["U0"], np.zeros(nn), g["phi0"]
+    for s in range(2):
+        Fp, F = compute(Ud, None, 0, 0)
+        U, P, phi, ui, pi, fi = timestep(U, P, phi, 0.01, 1.0, 0.01, 1e-4, Ud, None, Fp, F, None)
+        assert (int(ui), int(pi), int(fi)) == tuple(g["iters"][s])
+    assert rel(U, g["U"]) < SOLVE_TOL and rel(P, g["P"]) < SOLVE_TOL and rel(phi, g["phi"]) < SOLVE_TOL
+
+
+def test_channel_outlet_step():
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    g = load_golden("step_channel_q1_outlet")
+    cfg = _ns_cfg(gsim, [16, 8], [2.0, 1.0], 1, False, [0, 2, 3], "multigrid", True, 1e-8, [4, 2], outlet=[1])
+    compute, timestep, nc, sn, h, nn, gd, Ud = gsim.setup(cfg)
+    yL = np_(nc)[np_(sn[3]), 1]
+    Ud = gsim.set_face_velocity(Ud, sn[3], gd, torch.as_tensor(4 * yL * (1 - yL)), nn, var=1)
+    Fp, F = compute(Ud, None, 0.0, 0.01)
+    assert rel(Fp, g["F_p"]) < OPS_TOL
+    U, P, ui, pi = timestep(np.zeros(2 * nn), np.zeros(nn), 0.01, 1.0, 0.02, Ud, Fp, F)
+    assert (int(ui), int(pi)) == (int(g["U_iters"][0]), int(g["P_iters"][0]))
+    assert rel(U, g["U"]) < SOLVE_TOL and rel(P, g["P"]) < SOLVE_TOL
+
+
+def test_step_is_deterministic():
+    """Node-centric gathers and fixed-order reductions: bitwise-equal reruns."""
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    args, lid, steps, dt, mu = STEP_CASES["tg_q2p_mg"]
+    a = _run_steps(gsim, args, lid, 2, dt, mu)
+    b = _run_steps(gsim, args, lid, 2, dt, mu)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
