@@ -49,7 +49,7 @@ def i64(x):
         if x.device.type != "cuda":
             x = x.to(device())
         return x.to(torch.int64).contiguous()
-    return torch.as_tensor(np.asarray(x, dtype=np.int64)).reshape(-1).to(device()).contiguous()
+    return torch.as_tensor(np.asarray(x, dtype=np.int64)).to(device()).contiguous()
 
 
 def empty(n, dtype=torch.float64):

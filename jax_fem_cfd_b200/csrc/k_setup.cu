@@ -202,14 +202,16 @@ __global__ void k_assemble_diag(FemGrid g, int ndim, const double* __restrict__ 
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
     double m = 0.0, l = 0.0;
     fem_for_incident(g, n, [&](int, int, int, int, int a) {
-      double rs = 0.0;
-      for (int b = 0; b < nen; ++b) rs += Me[a * nen + b];
-      m += rs;
-      l += Le[a * nen + a];
+      if (Me) {
+        double rs = 0.0;
+        for (int b = 0; b < nen; ++b) rs += Me[a * nen + b];
+        m += rs;
+      }
+      if (Le) l += Le[a * nen + a];
     });
-    if (M)
+    if (M && Me)
       for (int c = 0; c < ndim; ++c) M[n + (size_t)c * g.nn] = m;
-    if (Ldiag) Ldiag[n] = l;
+    if (Ldiag && Le) Ldiag[n] = l;
   }
 }
 
