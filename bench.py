@@ -1,0 +1,433 @@
+"""Benchmark: NS steps/s of the 4-step projection on the periodic Taylor-Green
+vortex, 256x256 Q2 elements (262,144 unique nodes), FP64, multigrid-PCG
+pressure (final mesh 4x4, tol 1e-8), BiCGSTAB momentum (tol 1e-8).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). Under torchrun (N > 1) every rank runs an
+independent replica of the workload on its own GPU (a single solve does not
+shard: replicas only); the step time is the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(workload="taylor_green_periodic_q2_256x256", nex=256, ney=256, order=2, domain="[0,2pi]^2",
+                nu=0.01, rho=1.0, dt=1e-3, pressure_precond="multigrid", final_multigrid_mesh=[4, 4],
+                solver_tol=1e-8, set_zeroP=False)
+STAGES = ["convection_build", "momentum_rhs", "momentum_bicgstab", "u_star", "ppe_rhs", "pressure_pcg",
+          "projection"]
+KERNEL_OF_STAGE = {"pressure_pcg": "k_cg", "momentum_bicgstab": "k_bicgstab<2>", "convection_build": "k_convection"}
+
+
+def tg_config(sim, n):
+    return sim.Config(mesh="simple", solver="standard",
+                      mesh_config=sim.SimpleMeshConfig(num_elem=[n, n], domain_size=[2 * np.pi, 2 * np.pi],
+                                                       shape_func_ord=2, periodic=True),
+                      solver_config=sim.StandardSolverConfig(dirichlet_faces=[], symmetry_faces=[], outlet_faces=[],
+                                                             streamline_diff=False, solver_tol=1e-8, set_zeroP=False,
+                                                             pressure_precond="multigrid",
+                                                             final_multigrid_mesh=[4, 4]))
+
+
+def tg_initial(node_coords):
+    x, y = node_coords[:, 0], node_coords[:, 1]
+    U = np.concatenate([np.sin(x) * np.cos(y), -np.cos(x) * np.sin(y)])
+    P = 0.25 * (np.cos(2 * x) + np.cos(2 * y))
+    return U, P - P.mean()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        load = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def cg_algorithmic_bytes(level_nn, iters, block_from):
+    """Algorithmic DRAM bytes of one k_cg launch (MG-PCG, mean-zero). Per phase:
+    the nn-length vectors it must read and write once (FP64), stencil re-reads
+    excluded. Init: b, x0 -> r (+centred rhs copy): 5 nn. Per iteration: p/Ap
+    phase reads z, p_old, writes p_new, Ap (4 nn); x/r update reads x, p, r, Ap,
+    diag and writes x, r (7 nn). Per V-cycle level n: pre-smooth+residual
+    reads r, diag, writes x, t (4 nn_n); restriction reads t and diag_{n+1},
+    writes r_{n+1} (nn_n + 2 nn_{n+1}); prolongation reads x_{n+1}, x, writes
+    t (2 nn_n + nn_{n+1}); post-smooth reads t, r, diag, writes x (4 nn_n).
+    The V-cycle of the final iteration is skipped (its z is never used)."""
+    w = 8
+    L = len(level_nn)
+    vcyc = 0
+    for n in range(L - 1):
+        vcyc += 11 * level_nn[n] + 3 * level_nn[n + 1]
+    vcyc += 3 * level_nn[-1]
+    nn = level_nn[0]
+    total = 5 * nn + vcyc + iters * (11 * nn) + max(iters - 1, 0) * vcyc + 2 * nn
+    return total * w
+
+
+def bicgstab_algorithmic_bytes(nn, ne, nen, ndim, iters):
+    """k_bicgstab: per operator apply the per-element Ce (ne*nen^2) plus the
+    vectors of the phase; 3 phases per iteration (see fem_solvers kernels)."""
+    w = 8
+    vec = ndim * nn
+    ce = ne * nen * nen
+    init = ce + 6 * vec
+    per_it = (ce + 6 * vec) + (ce + 4 * vec) + 7 * vec
+    return (init + iters * per_it) * w
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import jax_fem_cfd_b200 as fem
+    import jax_fem_cfd_b200.setup.simulation as sim
+    from jax_fem_cfd_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.size
+    compute, timestep, nc, sn, h, nn, gd, Ud = sim.setup(tg_config(sim, n))
+    solver = timestep.solver
+    ctx = solver.ctx
+    U0, P0 = tg_initial(nc.cpu().numpy())
+    dt, rho, mu = 1e-3, 1.0, 0.01
+    U = torch.as_tensor(U0, device=dev)
+    P = torch.as_tensor(P0, device=dev)
+    Fp, F = compute(Ud, None, 0.0, dt)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    _lib.call("fem_ctx_enable_timing", ctx.handle, 1)
+    for _ in range(args.warmup):
+        U, P, ui, pi = timestep(U, P, dt, rho, mu, Ud, Fp, F)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stage_ms = np.zeros(len(STAGES))
+    iters = []
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = _lib.launch_count()
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            U, P, ui, pi = timestep(U, P, dt, rho, mu, Ud, Fp, F)
+            ends[k].record(stream)
+            st = (ctypes.c_float * 16)()
+            nst = _lib.load().fem_ctx_stage_times(ctx.handle, st, 16)
+            stage_ms[:nst] += np.array(st[:nst])
+            iters.append((int(ui), int(pi)))
+        torch.cuda.synchronize()
+    launches = _lib.launch_count() - launches0
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    total_ms = max_over_ranks(total_ms, world)
+    # --- end to end through the public API with host buffers ---
+    U_h = torch.as_tensor(U0).pin_memory()
+    P_h = torch.as_tensor(P0).pin_memory()
+    Uo_h = torch.empty_like(U_h).pin_memory()
+    Po_h = torch.empty_like(P_h).pin_memory()
+    e_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    _lib.call("fem_ctx_enable_timing", ctx.handle, 0)
+    for k in range(min(args.warmup, 2)):
+        Ug, Pg = U_h.to(dev, non_blocking=True), P_h.to(dev, non_blocking=True)
+        Fp, F = compute(Ud, None, 0.0, dt)
+        Ug, Pg, _, _ = timestep(Ug, Pg, dt, rho, mu, Ud, Fp, F)
+        Uo_h.copy_(Ug, non_blocking=True)
+        Po_h.copy_(Pg, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    for k in range(args.steps):
+        flush.zero_()
+        e_s[k].record(stream)
+        Ug, Pg = U_h.to(dev, non_blocking=True), P_h.to(dev, non_blocking=True)
+        Fp, F = compute(Ud, None, k * dt, (k + 1) * dt)
+        Ug, Pg, _, _ = timestep(Ug, Pg, dt, rho, mu, Ud, Fp, F)
+        Uo_h.copy_(Ug, non_blocking=True)
+        Po_h.copy_(Pg, non_blocking=True)
+        e_e[k].record(stream)
+        U_h, Uo_h = Uo_h, U_h
+        P_h, Po_h = Po_h, P_h
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(float(sum(s.elapsed_time(e) for s, e in zip(e_s, e_e))), world)
+    h2d = (U0.size + P0.size) * 8
+    d2h = h2d
+    res = dict(total_ms=total_ms, step_ms=step_ms, stage_ms=(stage_ms / args.steps).tolist(), iters=iters,
+               launches=launches, clocks=clk.summary(), e2e_ms=e2e_ms, h2d=h2d, d2h=d2h, nn=nn, ctx=ctx,
+               level_nn=[ctx.level_info(l)[0] for l in range(ctx.nlev)], block_from=None)
+    return res
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.ones(1, device="cuda")
+        dist.all_reduce(t)
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def poisson_and_matvec(args):
+    """Reference-published GPU figures on their own sizes (README.md:28-41):
+    MG-PCG Poisson solve on 1024x1024 Q1 elements and the EBE matvec on
+    4096x4096 Q1 elements (beyond L2: a true HBM-roofline kernel)."""
+    import torch
+
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import Context, Mesh, make_mask, ptr, stream
+    from jax_fem_cfd_b200.core import multigrid as mg
+    out = {}
+    hbm, _ = measured_peaks()
+    # Poisson: pinned node 0, random rhs (seeded), x0 = 0, tol 1e-8, final mesh 4x4
+    n = 1024
+    ctx = Context(Mesh(0, False, n, n, 1, 1.0, 1.0))
+    pm = make_mask(np.array([0]), ctx.nn)
+    ctx.set_bc(None, pm, True)
+    nlev = int(np.log2(n // 4)) + 1
+    mg.Hierarchy(ctx, nlev, [np.array([0])] * nlev, 1e-8)
+    rng = np.random.default_rng(0)
+    b = torch.as_tensor(rng.standard_normal(ctx.nn), device="cuda")
+    b[0] = 0.0
+    x = torch.zeros_like(b)
+    it = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    times = []
+    for k in range(8):
+        x.zero_()
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.call("fem_pressure_solve", ctx.handle, ptr(b), ptr(x), 1e-8, 0.0, 1000, 4, 0, 1, ptr(it), ptr(stt),
+                  stream())
+        e.record()
+        torch.cuda.synchronize()
+        if k >= 3:
+            times.append(s.elapsed_time(e))
+    ms = float(np.median(times))
+    out["poisson_1024x1024_q1"] = {"metric": "Poisson solves/s (MG-PCG, tol 1e-8)", "value": 1000.0 / ms,
+                                   "ms_per_solve": ms, "iterations": int(it.item()), "elements": n * n,
+                                   "reference_published_ms_unnamed_gpu": 28.0}
+    del ctx
+    # EBE Laplacian matvec, 4096x4096 Q1 (16.8M elements, 134 MB per vector)
+    n = 4096
+    ctx = Context(Mesh(0, False, n, n, 1, 1.0, 1.0))
+    Le = ctx.element_data()[4].reshape(-1).contiguous()
+    xv = torch.as_tensor(rng.standard_normal(ctx.nn), device="cuda")
+    yv = torch.empty_like(xv)
+    for _ in range(3):
+        _lib.call("fem_ebe_apply", ctx.handle, 1, ptr(xv), ptr(yv), 1.0, ptr(Le), 0.0, None, 0, 0.0, None, stream())
+    times = []
+    for _ in range(10):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.call("fem_ebe_apply", ctx.handle, 1, ptr(xv), ptr(yv), 1.0, ptr(Le), 0.0, None, 0, 0.0, None, stream())
+        e.record()
+        torch.cuda.synchronize()
+        times.append(s.elapsed_time(e))
+    ms = float(np.median(times))
+    byts = 2 * ctx.nn * 8
+    out["ebe_matvec_4096x4096_q1"] = {"ms_per_apply": ms, "elements": n * n, "algorithmic_bytes": byts,
+                                      "achieved_gbs": byts / ms / 1e6, "frac_of_hbm": byts / ms / 1e6 / hbm,
+                                      "reference_published_ms_unnamed_gpu": 4.5}
+    del ctx
+    return out
+
+
+def cpu_baseline(n, steps):
+    """The oracle (numpy FP64 restatement, 1 thread) on the same workload."""
+    from threadpoolctl import threadpool_limits
+
+    import oracle.simulation as osim
+    with threadpool_limits(1):
+        compute, timestep, nc, sn, h, nn, gd, Ud = osim.setup(tg_config(osim, n))
+        U, P = tg_initial(nc)
+        Fp, F = compute(Ud, None, 0, 0)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            U, P, _, _ = timestep(U, P, 1e-3, 1.0, 0.01, Ud, Fp, F)
+        el = time.perf_counter() - t0
+    return {"value": steps / el, "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} full NS steps of the same 256x256 Q2 workload, numpy oracle, 1 thread"}
+
+
+def run_reference(args):
+    """--impl reference: the oracle port of the reference's CPU path, all host
+    threads, same workload and metric."""
+    import oracle.simulation as osim
+    n = args.size
+    compute, timestep, nc, sn, h, nn, gd, Ud = osim.setup(tg_config(osim, n))
+    U, P = tg_initial(nc)
+    Fp, F = compute(Ud, None, 0, 0)
+    for _ in range(min(args.warmup, 1)):
+        U, P, _, _ = timestep(U, P, 1e-3, 1.0, 0.01, Ud, Fp, F)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        U, P, _, _ = timestep(U, P, 1e-3, 1.0, 0.01, Ud, Fp, F)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    line = {"metric": "NS steps/s", "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic TG initial field)",
+            "impl": "reference",
+            "config": {k: v_ for k, v_ in WORKLOAD.items() if k not in ("nex", "ney")} | {"parallelism": "none (CPU)"},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{args.steps} full NS steps, numpy oracle, all host threads"},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    r = run_ours(args, rank, world, local_rank)
+    extra = {}
+    if not args.no_extra and rank == 0:
+        extra = poisson_and_matvec(args)
+    hbm, src = measured_peaks()
+    K = args.steps
+    ms_step = r["total_ms"] / K
+    value = world * 1000.0 / ms_step
+    stage = dict(zip(STAGES, r["stage_ms"]))
+    stage_tot = sum(r["stage_ms"])
+    share = {k: v / stage_tot for k, v in stage.items()} if stage_tot > 0 else {}
+    p_iters = [pi for _, pi in r["iters"]]
+    u_iters = [ui for ui, _ in r["iters"]]
+    cg_bytes = np.mean([cg_algorithmic_bytes(r["level_nn"], it, None) for it in p_iters])
+    cg_ms = stage["pressure_pcg"]
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "k_cg_tg256_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    ctx = r["ctx"]
+    bi_bytes = np.mean([bicgstab_algorithmic_bytes(ctx.nn, ctx.ne, ctx.nen, 2, it) for it in u_iters])
+    line = {
+        "metric": "NS steps/s", "value": value, "unit": "steps/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial field)",
+        "config": {**{k: v for k, v in WORKLOAD.items() if k not in ("nex", "ney")},
+                   "unique_nodes": r["nn"], "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "e2e": {"value": world * 1000.0 * K / r["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": int(r["launches"]),
+        "roofline": {"kernel": "k_cg (persistent MG-PCG pressure solve)", "bound": "hbm",
+                     "achieved": cg_bytes / (cg_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": cg_bytes / (cg_ms * 1e-3) / 1e9 / hbm, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": cg_bytes, "avg_launch_ms": cg_ms,
+                     "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"},
+        "roofline_momentum": {"kernel": "k_bicgstab<2>", "achieved": bi_bytes / (stage["momentum_bicgstab"] * 1e-3) / 1e9,
+                              "peak": hbm, "unit": "GB/s",
+                              "frac": bi_bytes / (stage["momentum_bicgstab"] * 1e-3) / 1e9 / hbm},
+        "stage_ms": stage, "stage_share": share,
+        "iterations": {"momentum_mean": float(np.mean(u_iters)), "pressure_mean": float(np.mean(p_iters))},
+        "clocks": r["clocks"],
+        **extra,
+    }
+    if rank == 0 and world == 1 and args.cpu_steps > 0:
+        line["cpu_baseline"] = cpu_baseline(args.size, args.cpu_steps)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -237,6 +237,14 @@ int fem_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cudaStream_
 int fem_dot(fem_ctx* ctx, const double* x, const double* y, int n, double* out, cudaStream_t stream);
 int fem_axpby(fem_ctx* ctx, double a, const double* x, double b, double* y, int n, cudaStream_t stream);
 
+/* Stage timing of fem_step4 / fem_transport_phi. When enabled, the context
+ * records a CUDA event on the call's stream before each stage (Ce build,
+ * momentum rhs, momentum BiCGSTAB, U*, PPE rhs, pressure PCG, projection) and
+ * after the last. fem_ctx_stage_times synchronizes on the last event and writes
+ * up to max_n stage durations in ms; it returns the number written (or < 0). */
+int fem_ctx_enable_timing(fem_ctx* ctx, int enable);
+int fem_ctx_stage_times(fem_ctx* ctx, float* ms, int max_n);
+
 /* Number of this library's kernel launches issued so far in this process. */
 long long fem_launch_count(void);
 

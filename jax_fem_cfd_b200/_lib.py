@@ -56,6 +56,8 @@ SIGNATURES = {
     "fem_make_mask": (c_int, [P, c_int, c_int, P, P]),
     "fem_dot": (c_int, [P, P, P, c_int, P, P]),
     "fem_axpby": (c_int, [P, c_double, P, c_double, P, c_int, P]),
+    "fem_ctx_enable_timing": (c_int, [P, c_int]),
+    "fem_ctx_stage_times": (c_int, [P, P, c_int]),
     "fem_launch_count": (c_longlong, []),
     "fem_last_error": (ctypes.c_char_p, []),
 }

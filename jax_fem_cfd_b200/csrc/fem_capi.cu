@@ -119,7 +119,14 @@ struct fem_ctx {
   double *dotpart = nullptr, *Fe = nullptr;
   int Fe_cap = 0;
   int* flags = nullptr;  // device scratch ints
+  // optional stage timing
+  int timing = 0, nev = 0;
+  cudaEvent_t ev[16] = {};
 };
+
+static inline void stage_mark(fem_ctx* c, cudaStream_t s) {
+  if (c->timing && c->nev < 16) cudaEventRecord(c->ev[c->nev++], s);
+}
 
 template <class T>
 static int dalloc(T** p, size_t n) {
@@ -226,6 +233,8 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
+  for (int i = 0; i < 16; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
@@ -705,8 +714,11 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   const FemGrid& g = c->g;
   const int nd = c->ndim, nen = g.nen;
   const double theta = 0.5;
+  c->nev = 0;
+  stage_mark(c, s);
   // 1. Ce(U_n), beta = 1/2 (solvers/standard.py:152)
   FEM_TRY(fem_launch_convection(g, quad_of(c), Un, 0.5, 0, c->Ce, s));
+  stage_mark(c, s);
   // 2. momentum rhs, x0 and G P_n (solvers/standard.py:31-37)
   StepArgs S;
   S.g = g;
@@ -726,16 +738,23 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   FEM_TRY(fem_launch_mom_rhs(S, Un, Pn, Ud, F, c->rhsU, c->Uhat, c->gPn, s));
   // 3. BiCGSTAB on (rho/dt) Me + theta (rho Ce + mu Le), identity rows on gamma_d (:20-28, :41)
   FEM_TRY(fem_launch_lincomb(nen * nen, rho / dt, c->Me, theta * mu, c->Le, c->Kd, s));
+  stage_mark(c, s);
   const MatCombo op{c->Kd, 1.0, c->Ce, theta * rho, 0, nullptr, 0.0};
   FEM_TRY(run_bicgstab(c, nd, op, S.dmask, c->rhsU, c->Uhat, tol, 0.0, 0, iters, status, s));
+  stage_mark(c, s);
   // 4. U* = U_hat + (dt/rho) G P_n / M (:156)
   FEM_TRY(fem_launch_ustar(nd * g.nn, dt / rho, c->Uhat, c->gPn, c->M, c->Ustar, s));
+  stage_mark(c, s);
   // 5. PPE rhs and x0 (:97-107)
   FEM_TRY(fem_launch_p_rhs(S, c->Ustar, Fp, Pn, c->rhsP, Po, s));
+  stage_mark(c, s);
   // 6. pressure (P)CG, maxiter 1000 (:115-123)
   FEM_TRY(run_cg(c, c->rhsP, Po, tol, 0.0, 1000, precond, c->set_zeroP ? 0 : 1, 1, iters + 1, status + 1, s));
+  stage_mark(c, s);
   // 7. projection and Dirichlet values (:160-163)
-  return fem_launch_ufinal(S, c->Ustar, Po, Ud, Uo, s);
+  FEM_TRY(fem_launch_ufinal(S, c->Ustar, Po, Ud, Uo, s));
+  stage_mark(c, s);
+  return FEM_OK;
 }
 
 extern "C" int fem_transport_phi(fem_ctx* c, const double* Un, const double* U, const double* phin, double dt,
@@ -810,6 +829,24 @@ extern "C" int fem_dot(fem_ctx* c, const double* x, const double* y, int n, doub
 extern "C" int fem_axpby(fem_ctx* c, double a, const double* x, double b, double* y, int n, cudaStream_t s) {
   if (!c || !x || !y || n < 0) return FEM_E_ARG;
   return fem_launch_axpby(a, x, b, y, n, s);
+}
+
+extern "C" int fem_ctx_enable_timing(fem_ctx* c, int enable) {
+  if (!c) return FEM_E_ARG;
+  if (enable && !c->ev[0])
+    for (int i = 0; i < 16; ++i) FEM_CHECK(cudaEventCreate(&c->ev[i]));
+  c->timing = enable ? 1 : 0;
+  c->nev = 0;
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_stage_times(fem_ctx* c, float* ms, int max_n) {
+  if (!c || !ms || max_n < 0) return FEM_E_ARG;
+  if (!c->timing || c->nev < 2) return 0;
+  FEM_CHECK(cudaEventSynchronize(c->ev[c->nev - 1]));
+  int n = 0;
+  for (int i = 0; i + 1 < c->nev && n < max_n; ++i, ++n) FEM_CHECK(cudaEventElapsedTime(&ms[n], c->ev[i], c->ev[i + 1]));
+  return n;
 }
 
 extern "C" long long fem_launch_count(void) { return g_launches.load(); }
