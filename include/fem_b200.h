@@ -245,6 +245,12 @@ int fem_axpby(fem_ctx* ctx, double a, const double* x, double b, double* y, int 
 int fem_ctx_enable_timing(fem_ctx* ctx, int enable);
 int fem_ctx_stage_times(fem_ctx* ctx, float* ms, int max_n);
 
+/* Barrier trace of the persistent solver kernels (diagnostics): when set,
+ * CTA 0 appends the %globaltimer value (ns) at every grid-barrier exit to
+ * buf[1..cap-1] and keeps the count in buf[0] (the caller zeroes buf[0]).
+ * cap = 0 disables tracing. */
+int fem_ctx_set_trace(fem_ctx* ctx, unsigned long long* buf, int cap);
+
 /* Number of this library's kernel launches issued so far in this process. */
 long long fem_launch_count(void);
 

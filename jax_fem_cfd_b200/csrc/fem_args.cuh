@@ -5,6 +5,10 @@
 
 #define FEM_THREADS 512
 #define FEM_OP_THREADS 256
+// dynamic shared memory available to the CTA-0 multigrid levels of k_cg / k_vcycle
+#define FEM_BLOCK_SMEM_MAX (150 * 1024)
+// whole dynamic smem of k_cg / k_vcycle: reduction scratch + tile staging + CTA-0 levels
+#define FEM_DYN_SMEM_MAX ((128 + FEM_TILE_SMEM) * 8 + FEM_BLOCK_SMEM_MAX)
 
 struct BiArgs {
   FemSync sync;
@@ -44,6 +48,9 @@ int fem_launch_element_matrices(int nq, int nen, int dim, const double* wq, cons
                                 double* Me, double* Le, double* Leoff, double* Ge, cudaStream_t s);
 int fem_launch_assemble_diag(const FemGrid& g, int ndim, const double* Me, const double* Le, double* M, double* Ldiag,
                              cudaStream_t s);
+int fem_launch_stencil_build(const FemGrid& g, const double* A, int transpose, int skip_diag, double* out,
+                             cudaStream_t s);
+int fem_launch_invdiag(int n, const double* D, const uint8_t* pin, double* invD, double* winvD, cudaStream_t s);
 int fem_launch_level_sums(const FemGrid& g, const FemLattice& lat, const double* diag, double* out, cudaStream_t s);
 
 int fem_launch_ebe(int ncomp, const FemGrid& g, const MatCombo& m, const double* x, double* y, cudaStream_t s);

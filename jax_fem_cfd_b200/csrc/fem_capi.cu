@@ -81,11 +81,14 @@ static FemLattice lattice_of(const FemGrid& g) {
   return L;
 }
 
+#define FEM_TAB_MAX (64 * 27)
+
 struct CtxLevel {
   FemGrid g;
   double *Le = nullptr, *Leoff = nullptr, *diag = nullptr, *x = nullptr, *r = nullptr, *t = nullptr;
+  double *tab = nullptr, *tab_off = nullptr, *invD = nullptr, *winvD = nullptr;
   uint8_t* pin = nullptr;
-  double sum_invD = 0.0, sum_colw = 0.0;
+  double sum_invD = 0.0, sum_colw = 0.0, sum_rc = 0.0, sum_rcD = 0.0;
 };
 
 struct fem_ctx {
@@ -101,7 +104,7 @@ struct fem_ctx {
   uint8_t *dmask = nullptr, *pmask = nullptr, *aipin = nullptr;
   int has_dmask = 0, set_zeroP = 1;
   // multigrid
-  int nlev = 0, block_from = 0;
+  int nlev = 0, block_from = 0, block_smem = 0;
   double coarse_tol = 1e-8;
   CtxLevel lv[FEM_MAX_LEVELS];
   double *cr = nullptr, *cp = nullptr, *cq = nullptr;  // coarse CG scratch
@@ -122,6 +125,8 @@ struct fem_ctx {
   // optional stage timing
   int timing = 0, nev = 0;
   cudaEvent_t ev[16] = {};
+  unsigned long long* trace = nullptr;
+  int trace_cap = 0;
 };
 
 static inline void stage_mark(fem_ctx* c, cudaStream_t s) {
@@ -244,7 +249,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
     if (p) cudaFree(p);
   for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
     CtxLevel& L = c->lv[l];
-    void* lp[] = {L.Le, L.Leoff, L.diag, L.x, L.t, L.pin, (l > 0) ? L.r : nullptr};
+    void* lp[] = {L.Le, L.Leoff, L.diag, L.x, L.t, L.pin, (l > 0) ? L.r : nullptr, L.tab, L.tab_off, L.invD, L.winvD};
     for (void* p : lp)
       if (p) cudaFree(p);
   }
@@ -320,7 +325,14 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   L0.Le = nullptr;  // level 0 aliases the context matrices
   FEM_ALLOC(L0.x, nn);
   FEM_ALLOC(L0.t, nn);
+  FEM_ALLOC(L0.tab, FEM_TAB_MAX);
+  FEM_ALLOC(L0.tab_off, FEM_TAB_MAX);
+  FEM_ALLOC(L0.invD, nn);
+  FEM_ALLOC(L0.winvD, nn);
   L0.r = c->pr;
+  FEM_TRY(fem_launch_stencil_build(g, c->Le, 0, 0, L0.tab, s));
+  FEM_TRY(fem_launch_stencil_build(g, c->Le, 0, 1, L0.tab_off, s));
+  FEM_TRY(fem_launch_invdiag(g.nn, c->Ldiag, c->pmask, L0.invD, L0.winvD, s));
   c->nlev = 1;
   FEM_CHECK(cudaDeviceSynchronize());
   return FEM_OK;
@@ -387,6 +399,7 @@ extern "C" int fem_ctx_set_bc(fem_ctx* c, const uint8_t* dmask, const uint8_t* p
     FEM_CHECK(cudaMemcpyAsync(c->aipin, pmask, nn, cudaMemcpyDeviceToDevice, s));
   }
   c->set_zeroP = set_zeroP ? 1 : 0;
+  FEM_TRY(fem_launch_invdiag(c->g.nn, c->Ldiag, c->pmask, c->lv[0].invD, c->lv[0].winvD, s));
   return FEM_OK;
 }
 
@@ -401,7 +414,7 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
   // release previous levels
   for (int l = 1; l < FEM_MAX_LEVELS; ++l) {
     CtxLevel& L = c->lv[l];
-    void* lp[] = {L.Le, L.Leoff, L.diag, L.x, L.t, L.pin, L.r};
+    void* lp[] = {L.Le, L.Leoff, L.diag, L.x, L.t, L.pin, L.r, L.tab, L.tab_off, L.invD, L.winvD};
     for (void* p : lp)
       if (p) cudaFree(p);
     L = CtxLevel();
@@ -421,7 +434,7 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
   size_t off = 0;
   int rc = FEM_OK;
   double* sums;
-  FEM_ALLOC(sums, 2 * FEM_MAX_LEVELS);
+  FEM_ALLOC(sums, 4 * FEM_MAX_LEVELS);
   for (int l = 0; l < nlev && rc == FEM_OK; ++l) {
     CtxLevel& L = c->lv[l];
     if (l == 0) {
@@ -456,11 +469,21 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
     }
     off += nn;
     const double* diag = (l == 0) ? c->Ldiag : L.diag;
-    FEM_TRY(fem_launch_level_sums(L.g, lattice_of(L.g), diag, sums + 2 * l, s));
+    if (l > 0) {
+      rc |= dalloc(&L.tab, FEM_TAB_MAX);
+      rc |= dalloc(&L.tab_off, FEM_TAB_MAX);
+      rc |= dalloc(&L.invD, nn);
+      rc |= dalloc(&L.winvD, nn);
+      if (rc) break;
+      FEM_TRY(fem_launch_stencil_build(L.g, L.Le, 0, 0, L.tab, s));
+      FEM_TRY(fem_launch_stencil_build(L.g, L.Le, 0, 1, L.tab_off, s));
+    }
+    FEM_TRY(fem_launch_invdiag(L.g.nn, diag, L.pin, L.invD, L.winvD, s));
+    FEM_TRY(fem_launch_level_sums(L.g, lattice_of(L.g), diag, sums + 4 * l, s));
   }
-  double hs[2 * FEM_MAX_LEVELS];
+  double hs[4 * FEM_MAX_LEVELS];
   if (rc == FEM_OK) {
-    FEM_CHECK(cudaMemcpyAsync(hs, sums, sizeof(double) * 2 * nlev, cudaMemcpyDeviceToHost, s));
+    FEM_CHECK(cudaMemcpyAsync(hs, sums, sizeof(double) * 4 * nlev, cudaMemcpyDeviceToHost, s));
     FEM_CHECK(cudaStreamSynchronize(s));
   }
   cudaFree(tmp);
@@ -472,8 +495,10 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
   cudaFree(sums);
   if (rc) return rc;
   for (int l = 0; l < nlev; ++l) {
-    c->lv[l].sum_invD = hs[2 * l];
-    c->lv[l].sum_colw = hs[2 * l + 1];
+    c->lv[l].sum_invD = hs[4 * l];
+    c->lv[l].sum_colw = hs[4 * l + 1];
+    c->lv[l].sum_rc = hs[4 * l + 2];
+    c->lv[l].sum_rcD = hs[4 * l + 3];
   }
   c->nlev = nlev;
   c->coarse_tol = coarse_tol;
@@ -482,16 +507,22 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
   FEM_ALLOC(c->cr, ncn);
   FEM_ALLOC(c->cp, ncn);
   FEM_ALLOC(c->cq, ncn);
-  // first level handled by CTA 0 alone
-  int small = 4096;
+  // First level handled by CTA 0 alone: the coarsest levels whose vectors
+  // (x, r, t per level + 3 coarse-CG vectors) fit the dynamic smem budget and
+  // whose sizes are small enough for one SM (<= FEM_MG_BLOCK_NN nodes).
+  int small = 8192;
   const char* ev = getenv("FEM_MG_BLOCK_NN");
   if (ev) small = atoi(ev);
+  const long long budget = FEM_BLOCK_SMEM_MAX / sizeof(double);
   int bf = nlev - 1;
-  for (int l = 0; l < nlev; ++l)
-    if (c->lv[l].g.nn <= small) {
-      bf = l;
-      break;
-    }
+  long long need = 3LL * c->lv[nlev - 1].g.nn + 3LL * c->lv[nlev - 1].g.nn;
+  for (int l = nlev - 2; l >= 0; --l) {
+    const long long nd = need + 3LL * c->lv[l].g.nn;
+    if (c->lv[l].g.nn > small || nd > budget) break;
+    need = nd;
+    bf = l;
+  }
+  c->block_smem = (need <= budget && getenv("FEM_MG_BLOCK_GLOBAL") == nullptr) ? (int)need : 0;
   c->block_from = bf;
   return FEM_OK;
 }
@@ -591,9 +622,10 @@ extern "C" int fem_lattice_restrict(int nhx, int nhy, int nHx, int nHy, int peri
 
 static void fill_cg_args(fem_ctx* c, CgArgs& A) {
   memset(&A, 0, sizeof(A));
-  A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS};
+  A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS, c->trace, c->trace_cap};
   A.nlev = c->nlev;
   A.block_from = c->block_from;
+  A.block_smem = c->block_smem;
   A.pinned = c->set_zeroP;
   A.coarse_maxiter = 1000;
   A.coarse_tol = c->coarse_tol;
@@ -609,12 +641,16 @@ static void fill_cg_args(fem_ctx* c, CgArgs& A) {
     MgLevel& M = A.lv[l];
     M.g = L.g;
     M.lat = lattice_of(L.g);
-    M.Le = (l == 0) ? c->Le : L.Le;
-    M.Le_off = (l == 0) ? c->Leoff : L.Leoff;
+    M.tab = L.tab;
+    M.tab_off = L.tab_off;
+    M.invD = L.invD;
+    M.winvD = L.winvD;
     M.diag = (l == 0) ? c->Ldiag : L.diag;
     M.pin = (l == 0) ? (L.pin ? L.pin : c->pmask) : L.pin;
     M.sum_invD = L.sum_invD;
     M.sum_colw = L.sum_colw;
+    M.sum_rc = L.sum_rc;
+    M.sum_rcD = L.sum_rcD;
     M.x = L.x;
     M.r = (l == 0) ? c->pr : L.r;
     M.t = L.t;
@@ -673,7 +709,7 @@ static int run_bicgstab(fem_ctx* c, int ncomp, const MatCombo& op, const uint8_t
   if (ncomp < 1 || ncomp > c->ndim) return FEM_E_ARG;  // workspace holds ndim*nn per vector
   BiArgs A;
   memset(&A, 0, sizeof(A));
-  A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS};
+  A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS, c->trace, c->trace_cap};
   A.g = c->g;
   A.op = op;
   A.mask = mask;
@@ -847,6 +883,13 @@ extern "C" int fem_ctx_stage_times(fem_ctx* c, float* ms, int max_n) {
   int n = 0;
   for (int i = 0; i + 1 < c->nev && n < max_n; ++i, ++n) FEM_CHECK(cudaEventElapsedTime(&ms[n], c->ev[i], c->ev[i + 1]));
   return n;
+}
+
+extern "C" int fem_ctx_set_trace(fem_ctx* c, unsigned long long* buf, int cap) {
+  if (!c || cap < 0 || (cap > 0 && !buf)) return FEM_E_ARG;
+  c->trace = cap > 0 ? buf : nullptr;
+  c->trace_cap = cap;
+  return FEM_OK;
 }
 
 extern "C" long long fem_launch_count(void) { return g_launches.load(); }

@@ -176,6 +176,8 @@ struct FemSync {
   int* err;               // sticky error flags (FEM_ERR_*)
   double* partials;       // [slot][cta] partial sums
   int nslots;
+  unsigned long long* trace;  // optional: globaltimer at each barrier exit (CTA 0), trace[0] = count
+  int trace_cap;
 };
 
 __device__ __forceinline__ unsigned int fem_ld_acquire(const unsigned int* p) {
@@ -196,28 +198,41 @@ __device__ __forceinline__ unsigned long long fem_globaltimer() {
 // every CTA leaves the kernel at its next barrier instead of hanging the GPU.
 #define FEM_BARRIER_TIMEOUT_NS 2000000000ull
 
+// Diagnostic trace mark (CTA 0, thread 0): appends %globaltimer | (tag << 56).
+__device__ __forceinline__ void fem_trace_mark(const FemSync& s, unsigned long long tag) {
+  if (s.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long n = s.trace[0] + 1;
+    if ((int)n < s.trace_cap) {
+      s.trace[n] = (fem_globaltimer() & 0x00FFFFFFFFFFFFFFull) | (tag << 56);
+      s.trace[0] = n;
+    }
+  }
+}
+
+// Grid barrier on a monotonic arrival counter (reset to 0 before each launch):
+// barrier number k of the launch completes when the counter reaches
+// k * gridDim.x. One fire-and-forget release-add per CTA, then acquire polling.
 struct GridTeam {
   FemSync s;
+  unsigned int* round;  // per-CTA count of completed barriers (shared memory, thread 0, starts at 0)
   __device__ __forceinline__ int rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
   __device__ __forceinline__ int size() const { return gridDim.x * blockDim.x; }
-  __device__ __forceinline__ bool leader_block() const { return blockIdx.x == 0; }
+  __device__ __forceinline__ int cta() const { return blockIdx.x; }
+  __device__ __forceinline__ int ncta() const { return gridDim.x; }
   // Returns false if the kernel must stop (timeout or error raised elsewhere).
   __device__ bool sync() const {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
       int ok = 1;
-      const unsigned int g0 = fem_ld_acquire(s.gen);
+      const unsigned int target = (*round + 1u) * gridDim.x;
+      *round = *round + 1u;
       __threadfence();
-      const unsigned int arrived = atomicAdd(s.count, 1u);
-      if (arrived == gridDim.x - 1) {
-        atomicExch(s.count, 0u);
-        __threadfence();
-        fem_st_release(s.gen, g0 + 1u);
-      } else {
+      asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(s.count), "r"(1u) : "memory");
+      if (gridDim.x > 1) {
         const unsigned long long t0 = fem_globaltimer();
         unsigned int polls = 0;
-        while (fem_ld_acquire(s.gen) == g0) {
+        while (fem_ld_acquire(s.count) < target) {
           if (((++polls) & 63u) == 0u) {
             if (*(volatile int*)s.err & FEM_ERR_BARRIER_TIMEOUT) { ok = 0; break; }
             if (fem_globaltimer() - t0 > FEM_BARRIER_TIMEOUT_NS) {
@@ -231,6 +246,13 @@ struct GridTeam {
       __threadfence();
       if (*(volatile int*)s.err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
       s_ok = ok;
+      if (s.trace && blockIdx.x == 0) {
+        const unsigned long long n = s.trace[0] + 1;
+        if ((int)n < s.trace_cap) {
+          s.trace[n] = fem_globaltimer();
+          s.trace[0] = n;
+        }
+      }
     }
     __syncthreads();
     return s_ok != 0;
@@ -240,6 +262,8 @@ struct GridTeam {
 struct BlockTeam {
   __device__ __forceinline__ int rank() const { return threadIdx.x; }
   __device__ __forceinline__ int size() const { return blockDim.x; }
+  __device__ __forceinline__ int cta() const { return 0; }
+  __device__ __forceinline__ int ncta() const { return 1; }
   __device__ __forceinline__ bool sync() const {
     __syncthreads();
     return true;
@@ -279,16 +303,32 @@ struct GridReducer {
 #pragma unroll
       for (int q = 0; q < K; ++q) s.partials[(size_t)(slot + q) * gridDim.x + blockIdx.x] = v[q];
   }
-  // Sum of per-CTA partials in CTA order (identical in every CTA).
+  // Totals of K slots (any slot numbers), every partial load in flight at once;
+  // CTA partials are combined in a fixed order (identical in every CTA).
   template <int K>
-  __device__ __forceinline__ void result(double (&out)[K], int slot, double* smem) const {
+  __device__ __forceinline__ void result_slots(double (&out)[K], const int (&slots)[K], double* smem) const {
     __syncthreads();
     if (threadIdx.x < 32) {
+      const int G = gridDim.x;
+      double acc[K];
+#pragma unroll
+      for (int q = 0; q < K; ++q) acc[q] = 0.0;
+      for (int base = 0; base < G; base += 256) {
+        double v[K][8];
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int c = base + threadIdx.x + 32 * k;
+            v[q][k] = (c < G) ? __ldcg(&s.partials[(size_t)slots[q] * G + c]) : 0.0;
+          }
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+          acc[q] += ((v[q][0] + v[q][1]) + (v[q][2] + v[q][3])) + ((v[q][4] + v[q][5]) + (v[q][6] + v[q][7]));
+      }
 #pragma unroll
       for (int q = 0; q < K; ++q) {
-        double t = 0.0;
-        for (int c = threadIdx.x; c < (int)gridDim.x; c += 32)
-          t += __ldcg(&s.partials[(size_t)(slot + q) * gridDim.x + c]);
+        double t = acc[q];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
         if (threadIdx.x == 0) smem[q] = t;
@@ -298,6 +338,13 @@ struct GridReducer {
 #pragma unroll
     for (int q = 0; q < K; ++q) out[q] = smem[q];
     __syncthreads();
+  }
+  template <int K>
+  __device__ __forceinline__ void result(double (&out)[K], int slot, double* smem) const {
+    int sl[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) sl[q] = slot + q;
+    result_slots<K>(out, sl, smem);
   }
 };
 
@@ -311,6 +358,12 @@ struct BlockReducer {
       for (int q = 0; q < K; ++q) store[slot + q] = v[q];
   }
   template <int K>
+  __device__ __forceinline__ void result_slots(double (&out)[K], const int (&slots)[K], double*) const {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = store[slots[q]];
+  }
+  template <int K>
   __device__ __forceinline__ void result(double (&out)[K], int slot, double*) const {
     __syncthreads();
 #pragma unroll
@@ -319,3 +372,19 @@ struct BlockReducer {
 };
 
 __device__ __forceinline__ bool fem_isfinite(double x) { return isfinite(x); }
+
+// Node iteration in 2D tiles of 32 x (blockDim/32) lattice nodes, one tile per
+// CTA at a time, so stencil neighbours in adjacent rows are read by the same
+// CTA (L1 hits). f(n, x, y, z) with n the node index of lattice (x, y, z).
+template <class Team, class F>
+__device__ __forceinline__ void fem_tile_loop(const Team& tm, int nx, int ny, int nz, F&& f) {
+  const int TY = blockDim.x >> 5;
+  const int ntx = (nx + 31) >> 5, nty = (ny + TY - 1) / TY;
+  const int nt2 = ntx * nty, ntile = nt2 * nz;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int t = tm.cta(); t < ntile; t += tm.ncta()) {
+    const int z = t / nt2, r = t - z * nt2, by = r / ntx, bx = r - by * ntx;
+    const int x = bx * 32 + tx, y = by * TY + ty;
+    if (x < nx && y < ny) f((z * ny + y) * nx + x, x, y, z);
+  }
+}

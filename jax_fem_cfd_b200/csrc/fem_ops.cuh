@@ -251,6 +251,14 @@ __device__ __forceinline__ double fem_restrict_at(const FemLattice& h, int R, in
   return xh(h.idx(r0, c0)) + 0.5 * e + 0.25 * d;
 }
 
+// Row sum of the restriction at coarse unique node (R, C): (R 1)_I on the full
+// fine lattice (neighbours outside it are skipped, periodic too).
+__device__ __forceinline__ double fem_restrict_rowsum(const FemLattice& H, int R, int C) {
+  const double wr = 1.0 + (R > 0 ? 0.5 : 0.0) + (R < H.ny - 1 ? 0.5 : 0.0);
+  const double wc = 1.0 + (C > 0 ? 0.5 : 0.0) + (C < H.nx - 1 ? 0.5 : 0.0);
+  return wr * wc;
+}
+
 // Column sum of the prolongation at coarse unique node (R, C): sum_i P_iI.
 __device__ __forceinline__ double fem_interp_colsum(const FemLattice& H, int R, int C) {
   if (H.periodic) return 4.0;

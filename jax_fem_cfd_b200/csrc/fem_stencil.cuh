@@ -1,0 +1,480 @@
+// Element-kind specialised lattice machinery.
+//
+// 1. fem_incident_k<KIND>: the node-centric incidence loop with the element
+//    kind known at compile time (unrolled candidates, compile-time local-node
+//    offsets) for operators with per-element matrices (Ce, SUPG terms).
+//
+// 2. Assembled stencils: for a SHARED element matrix A on the uniform lattice,
+//    the node-centric sum y_n = sum_{(e,a) ~ n} sum_b A[a][b] x[node(e,b)] only
+//    depends on which incident elements exist, i.e. on the node's class along
+//    each axis (boundary position and, for quad9, parity). A table holds, per
+//    class, the coefficient of every lattice offset (3^d or 5^2 offsets), built
+//    on the device from A with the same incidence rules; applying it is an
+//    unrolled constant-offset stencil. Values equal the element-by-element sum
+//    up to summation order.
+#pragma once
+#include "fem_common.cuh"
+
+template <int KIND>
+struct KI;
+template <>
+struct KI<FEM_Q1_2D> {
+  static constexpr int R = 1, W = 3, NOFF = 9, S = 1, NEN = 4, DIM = 2;
+};
+template <>
+struct KI<FEM_Q2_2D> {
+  static constexpr int R = 2, W = 5, NOFF = 25, S = 2, NEN = 9, DIM = 2;
+};
+template <>
+struct KI<FEM_HEX8> {
+  static constexpr int R = 1, W = 3, NOFF = 27, S = 1, NEN = 8, DIM = 3;
+};
+
+template <int KIND>
+__device__ __forceinline__ constexpr int kdi(int b) {
+  return KIND == FEM_Q2_2D ? (int)((FEM_Q2_DI >> (2 * b)) & 3u) : (int)((FEM_Q1_DI >> (2 * (b & 3))) & 3u);
+}
+template <int KIND>
+__device__ __forceinline__ constexpr int kdj(int b) {
+  return KIND == FEM_Q2_2D ? (int)((FEM_Q2_DJ >> (2 * b)) & 3u) : (int)((FEM_Q1_DJ >> (2 * (b & 3))) & 3u);
+}
+template <int KIND>
+__device__ __forceinline__ constexpr int kdk(int b) {
+  return KIND == FEM_HEX8 ? (b >> 2) : 0;
+}
+
+// Candidates along one axis: (e0, d0) valid if v0, (e1, d1) valid if v1.
+template <int KIND>
+__device__ __forceinline__ void fem_axis_pair(int periodic, int c, int nel, int& e0, int& d0, bool& v0, int& e1,
+                                              int& d1, bool& v1) {
+  if (KIND == FEM_Q2_2D && (c & 1)) {
+    e0 = (c - 1) >> 1;
+    d0 = 1;
+    v0 = true;
+    e1 = 0;
+    d1 = 0;
+    v1 = false;
+    return;
+  }
+  const int h = (KIND == FEM_Q2_2D) ? (c >> 1) : c;
+  v0 = (h >= 1) || periodic;
+  e0 = (h >= 1) ? h - 1 : nel - 1;
+  d0 = (KIND == FEM_Q2_2D) ? 2 : 1;
+  v1 = h < nel;
+  e1 = h;
+  d1 = 0;
+}
+
+// f(ie, je, ke, e, a) for every element incident to lattice node (i, j, k).
+template <int KIND, class F>
+__device__ __forceinline__ void fem_incident_k(const FemGrid& g, int i, int j, int k, F&& f) {
+  int ei0, di0, ei1, di1, ej0, dj0, ej1, dj1, ek0 = 0, dk0 = 0, ek1 = 0, dk1 = 0;
+  bool vi0, vi1, vj0, vj1, vk0 = true, vk1 = false;
+  fem_axis_pair<KIND>(g.periodic, i, g.nex, ei0, di0, vi0, ei1, di1, vi1);
+  fem_axis_pair<KIND>(g.periodic, j, g.ney, ej0, dj0, vj0, ej1, dj1, vj1);
+  if (KIND == FEM_HEX8) fem_axis_pair<FEM_HEX8>(0, k, g.nez, ek0, dk0, vk0, ek1, dk1, vk1);
+#pragma unroll
+  for (int zk = 0; zk < (KIND == FEM_HEX8 ? 2 : 1); ++zk) {
+    if (!(zk ? vk1 : vk0)) continue;
+    const int ek = zk ? ek1 : ek0, dk = zk ? dk1 : dk0;
+#pragma unroll
+    for (int zj = 0; zj < 2; ++zj) {
+      if (!(zj ? vj1 : vj0)) continue;
+      const int ej = zj ? ej1 : ej0, dj = zj ? dj1 : dj0;
+#pragma unroll
+      for (int zi = 0; zi < 2; ++zi) {
+        if (!(zi ? vi1 : vi0)) continue;
+        const int ei = zi ? ei1 : ei0, di = zi ? di1 : di0;
+        const int e = (ek * g.ney + ej) * g.nex + ei;
+        f(ei, ej, ek, e, fem_local_index(KIND, di, dj, dk));
+      }
+    }
+  }
+}
+
+// Node index of local node B (compile-time) of element (ie, je, ke).
+template <int KIND, int B>
+__device__ __forceinline__ int fem_enode(const FemGrid& g, int ie, int je, int ke) {
+  constexpr int S = KI<KIND>::S;
+  int c = S * ie + kdi<KIND>(B), r = S * je + kdj<KIND>(B);
+  if (g.periodic) {
+    if (c >= g.nnx) c -= g.nnx;
+    if (r >= g.nny) r -= g.nny;
+  }
+  return ((ke + kdk<KIND>(B)) * g.nny + r) * g.nnx + c;
+}
+
+template <int KIND, int B = 0>
+struct ElemNodes {
+  template <class F>
+  __device__ __forceinline__ static void run(const FemGrid& g, int ie, int je, int ke, F&& f) {
+    if constexpr (B < KI<KIND>::NEN) {
+      f(B, fem_enode<KIND, B>(g, ie, je, ke));
+      ElemNodes<KIND, B + 1>::run(g, ie, je, ke, f);
+    }
+  }
+};
+
+// Gather with a per-element coefficient functor m(e, a, b) and NC sources src(j, c).
+template <int KIND, int NC, class Mat, class Src>
+__device__ __forceinline__ void fem_gather_k(const FemGrid& g, int i, int j, int k, const Mat& m, const Src& src,
+                                             double (&y)[NC]) {
+#pragma unroll
+  for (int c = 0; c < NC; ++c) y[c] = 0.0;
+  fem_incident_k<KIND>(g, i, j, k, [&](int ie, int je, int ke, int e, int a) {
+    double part[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) part[c] = 0.0;
+    ElemNodes<KIND>::run(g, ie, je, ke, [&](int b, int jn) {
+      const double coef = m(e, a, b, KI<KIND>::NEN);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) part[c] += coef * src(jn, c);
+    });
+#pragma unroll
+    for (int c = 0; c < NC; ++c) y[c] += part[c];
+  });
+}
+
+// ---------------------------------------------------------------- stencils --
+
+__host__ __device__ __forceinline__ int fem_axis_ncls(int kind, int periodic) {
+  if (kind == FEM_Q2_2D) return periodic ? 2 : 4;
+  return periodic ? 1 : 3;
+}
+__device__ __forceinline__ int fem_axis_cls(int kind, int periodic, int c, int nel) {
+  if (kind == FEM_Q2_2D) {
+    if (periodic) return c & 1;
+    if (c & 1) return 3;
+    return c == 0 ? 0 : (c == 2 * nel ? 2 : 1);
+  }
+  if (periodic) return 0;
+  return c == 0 ? 0 : (c == nel ? 2 : 1);
+}
+// representative lattice coordinate of a class, -1 if the lattice has none
+__device__ __forceinline__ int fem_axis_rep(int kind, int periodic, int cls, int nel) {
+  if (kind == FEM_Q2_2D) {
+    if (periodic) return cls;
+    if (cls == 0) return 0;
+    if (cls == 1) return nel >= 2 ? 2 : -1;
+    if (cls == 2) return 2 * nel;
+    return 1;
+  }
+  if (periodic) return 0;
+  if (cls == 0) return 0;
+  if (cls == 1) return nel >= 2 ? 1 : -1;
+  return nel;
+}
+
+__host__ __device__ __forceinline__ int fem_stencil_ncls(const FemGrid& g) {
+  const int n = fem_axis_ncls(g.kind, g.periodic);
+  return g.kind == FEM_HEX8 ? n * n * n : n * n;
+}
+__host__ __device__ __forceinline__ int fem_stencil_noff(int kind) {
+  return kind == FEM_Q2_2D ? 25 : (kind == FEM_HEX8 ? 27 : 9);
+}
+
+// offset of lattice coordinate v relative to c, periodic-aware, in [-R, R]
+__device__ __forceinline__ int fem_rel(int v, int c, int n, int periodic) {
+  int d = v - c;
+  if (periodic) {
+    d %= n;
+    if (d < 0) d += n;
+    if (2 * d > n) d -= n;
+  }
+  return d;
+}
+
+// Table of the assembled form of shared matrix A (nen x nen): out[cls][off].
+// transpose: use A^T; skip_diag: omit the b == a terms (A with a zero diagonal).
+template <int KIND>
+__global__ void k_stencil_build(FemGrid g, const double* __restrict__ A, int transpose, int skip_diag,
+                                double* __restrict__ out) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF, NEN = KI<KIND>::NEN, S = KI<KIND>::S;
+  const int nc = fem_axis_ncls(KIND, g.periodic);
+  const int ncls = fem_stencil_ncls(g);
+  for (int cls = blockIdx.x * blockDim.x + threadIdx.x; cls < ncls; cls += gridDim.x * blockDim.x) {
+    double acc[NOFF];
+#pragma unroll
+    for (int o = 0; o < NOFF; ++o) acc[o] = 0.0;
+    const int cx = cls % nc, cy = (cls / nc) % nc, cz = cls / (nc * nc);
+    const int i = fem_axis_rep(KIND, g.periodic, cx, g.nex), j = fem_axis_rep(KIND, g.periodic, cy, g.ney);
+    const int k = (KIND == FEM_HEX8) ? fem_axis_rep(KIND, 0, cz, g.nez) : 0;
+    if (i >= 0 && j >= 0 && k >= 0) {
+      fem_incident_k<KIND>(g, i, j, k, [&](int ie, int je, int ke, int e, int a) {
+        for (int b = 0; b < NEN; ++b) {
+          if (skip_diag && b == a) continue;
+          const int bi = S * ie + kdi<KIND>(b), bj = S * je + kdj<KIND>(b), bk = ke + kdk<KIND>(b);
+          const int dx = fem_rel(bi, i, g.nnx, g.periodic) + R, dy = fem_rel(bj, j, g.nny, g.periodic) + R;
+          const int dz = (KIND == FEM_HEX8) ? (bk - k + R) : 0;
+          const double v = transpose ? A[b * NEN + a] : A[a * NEN + b];
+          const int off = (dz * W + dy) * W + dx;
+#pragma unroll
+          for (int o = 0; o < NOFF; ++o)
+            if (o == off) acc[o] += v;
+        }
+      });
+    }
+#pragma unroll
+    for (int o = 0; o < NOFF; ++o) out[(size_t)cls * NOFF + o] = acc[o];
+  }
+}
+
+// y = sum_off coef[cls(i,j,k)][off] * src(node(i,j,k) + off)
+template <int KIND, class Src>
+__device__ __forceinline__ double fem_stencil_apply(const FemGrid& g, const double* __restrict__ tab, int i, int j,
+                                                    int k, const Src& src) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  const int nc = fem_axis_ncls(KIND, g.periodic);
+  const int cx = fem_axis_cls(KIND, g.periodic, i, g.nex), cy = fem_axis_cls(KIND, g.periodic, j, g.ney);
+  const int cz = (KIND == FEM_HEX8) ? fem_axis_cls(KIND, 0, k, g.nez) : 0;
+  const double* __restrict__ c = tab + (size_t)((cz * nc + cy) * nc + cx) * NOFF;
+  int col[W], row[W], pl[KIND == FEM_HEX8 ? W : 1];
+#pragma unroll
+  for (int d = 0; d < W; ++d) {
+    int v = i + d - R, w = j + d - R;
+    if (g.periodic) {
+      v = v < 0 ? v + g.nnx : (v >= g.nnx ? v - g.nnx : v);
+      w = w < 0 ? w + g.nny : (w >= g.nny ? w - g.nny : w);
+    } else {
+      v = v < 0 ? 0 : (v >= g.nnx ? g.nnx - 1 : v);
+      w = w < 0 ? 0 : (w >= g.nny ? g.nny - 1 : w);
+    }
+    col[d] = v;
+    row[d] = w * g.nnx;
+  }
+  if (KIND == FEM_HEX8) {
+#pragma unroll
+    for (int d = 0; d < W; ++d) {
+      int z = k + d - R;
+      z = z < 0 ? 0 : (z >= g.nnz ? g.nnz - 1 : z);
+      pl[d] = z * g.nnx * g.nny;
+    }
+  } else {
+    pl[0] = 0;
+  }
+  double y = 0.0;
+#pragma unroll
+  for (int dz = 0; dz < (KIND == FEM_HEX8 ? W : 1); ++dz)
+#pragma unroll
+    for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < W; ++dx) {
+        const int o = (dz * W + dy) * W + dx;
+        y += __ldg(c + o) * src(pl[dz] + row[dy] + col[dx]);
+      }
+  return y;
+}
+
+// Gradient: y_d = sum Ge_d rows * P (ND outputs from one input).
+template <int KIND, int ND, class Src>
+__device__ __forceinline__ void fem_gather_grad_k(const FemGrid& g, int i, int j, int k, const double* Ge,
+                                                  const Src& P, double (&y)[ND]) {
+  constexpr int NEN = KI<KIND>::NEN, NEN2 = NEN * NEN;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) y[d] = 0.0;
+  fem_incident_k<KIND>(g, i, j, k, [&](int ie, int je, int ke, int e, int a) {
+    double part[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) part[d] = 0.0;
+    ElemNodes<KIND>::run(g, ie, je, ke, [&](int b, int jn) {
+      const double pj = P(jn);
+#pragma unroll
+      for (int d = 0; d < ND; ++d) part[d] += Ge[d * NEN2 + a * NEN + b] * pj;
+    });
+#pragma unroll
+    for (int d = 0; d < ND; ++d) y[d] += part[d];
+  });
+}
+
+// Divergence: sum_d sum Ge_d^T rows * U_d (per-component sums added at the end,
+// as the reference adds the assembled component vectors).
+template <int KIND, int ND>
+__device__ __forceinline__ double fem_gather_div_k(const FemGrid& g, int i, int j, int k, const double* Ge,
+                                                   const double* __restrict__ U) {
+  constexpr int NEN = KI<KIND>::NEN, NEN2 = NEN * NEN;
+  double acc[ND];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) acc[d] = 0.0;
+  const size_t nn = g.nn;
+  fem_incident_k<KIND>(g, i, j, k, [&](int ie, int je, int ke, int e, int a) {
+    double part[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) part[d] = 0.0;
+    ElemNodes<KIND>::run(g, ie, je, ke, [&](int b, int jn) {
+#pragma unroll
+      for (int d = 0; d < ND; ++d) part[d] += Ge[d * NEN2 + b * NEN + a] * U[jn + d * nn];
+    });
+#pragma unroll
+    for (int d = 0; d < ND; ++d) acc[d] += part[d];
+  });
+  double y = acc[0];
+#pragma unroll
+  for (int d = 1; d < ND; ++d) y += acc[d];
+  return y;
+}
+
+// Kernel dispatch on the element kind (the grid's kind must match KIND).
+#define FEM_KIND_DISPATCH(kind, KIND_NAME, ...)        \
+  do {                                                 \
+    if ((kind) == FEM_Q1_2D) {                         \
+      constexpr int KIND_NAME = FEM_Q1_2D;             \
+      __VA_ARGS__;                                     \
+    } else if ((kind) == FEM_Q2_2D) {                  \
+      constexpr int KIND_NAME = FEM_Q2_2D;             \
+      __VA_ARGS__;                                     \
+    } else {                                           \
+      constexpr int KIND_NAME = FEM_HEX8;              \
+      __VA_ARGS__;                                     \
+    }                                                  \
+  } while (0)
+
+// Tiled stencil with shared-memory staging. For each 32 x (blockDim/32) tile of
+// the lattice owned by this CTA, the source values of the tile plus an R-wide
+// halo (3 planes in 3D) are produced by load(node) and staged in smem with all
+// loads in flight at once; then every thread applies the assembled stencil of
+// its node from smem and calls body(n, x, y, z, value, center_source).
+// The smem buffer needs (32+2R) * (blockDim/32+2R) * (3 in 3D) doubles.
+#define FEM_TILE_SMEM 6144
+
+// Tile height (lattice rows) so that one round of tiles covers the level with
+// at most ncta tiles (one tile per CTA), capped by the smem staging buffer.
+__device__ __forceinline__ int fem_tile_rows(int nx, int ny, int nplanes, int halo, int ncta, int cap_doubles,
+                                             int planes_staged) {
+  const int ntx = (nx + 31) >> 5;
+  int th = (ny * ntx * nplanes + ncta - 1) / ncta;
+  const int rows_per_tile_cap = cap_doubles / ((32 + 2 * halo) * planes_staged) - 2 * halo;
+  const int minr = blockDim.x >> 5;
+  if (th < minr) th = minr;
+  if (th > rows_per_tile_cap) th = rows_per_tile_cap;
+  if (th > ny) th = ny < minr ? minr : ny;
+  return th;
+}
+
+template <int KIND, class Team, class Load, class Body>
+__device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid& g, const double* __restrict__ tab,
+                                                  double* __restrict__ sm, const Load& load, const Body& body) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  constexpr bool D3 = (KIND == FEM_HEX8);
+  const int WR = blockDim.x >> 5;  // warps = rows per pass
+  const int TY = fem_tile_rows(g.nnx, g.nny, g.nnz, R, tm.ncta(), FEM_TILE_SMEM, D3 ? 3 : 1);
+  const int SX = 32 + 2 * R, SY = TY + 2 * R, SXY = SX * SY, NS = SXY * (D3 ? 3 : 1);
+  const int ntx = (g.nnx + 31) >> 5, nty = (g.nny + TY - 1) / TY, nt2 = ntx * nty, ntile = nt2 * g.nnz;
+  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
+  const int nc = fem_axis_ncls(KIND, g.periodic);
+  for (int t = tm.cta(); t < ntile; t += tm.ncta()) {
+    const int z = t / nt2, rr = t - z * nt2, by = rr / ntx, bx = rr - by * ntx;
+    const int x0 = bx * 32 - R, y0 = by * TY - R;
+    // all staged loads of a batch in flight before the first smem store
+    constexpr int NB = 8;
+    for (int q0 = 0; q0 < NS; q0 += NB * (int)blockDim.x) {
+      double v[NB];
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {
+        const int s = q0 + k * blockDim.x + threadIdx.x;
+        if (s < NS) {
+          const int lz = D3 ? s / SXY : 0, r2 = s - lz * SXY, ly = r2 / SX, lx = r2 - ly * SX;
+          int gx = x0 + lx, gy = y0 + ly, gz = D3 ? z + lz - 1 : 0;
+          if (g.periodic) {
+            gx = gx < 0 ? gx + g.nnx : (gx >= g.nnx ? gx - g.nnx : gx);
+            gy = gy < 0 ? gy + g.nny : (gy >= g.nny ? gy - g.nny : gy);
+          } else {
+            gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
+            gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);
+          }
+          if (D3) gz = gz < 0 ? 0 : (gz >= g.nnz ? g.nnz - 1 : gz);
+          v[k] = load((gz * g.nny + gy) * g.nnx + gx);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {
+        const int s = q0 + k * blockDim.x + threadIdx.x;
+        if (s < NS) sm[s] = v[k];
+      }
+    }
+    __syncthreads();
+    for (int ty = ty0; ty < TY; ty += WR) {
+      const int x = bx * 32 + tx, y = by * TY + ty;
+      if (x < g.nnx && y < g.nny) {
+        const int cx = fem_axis_cls(KIND, g.periodic, x, g.nex), cy = fem_axis_cls(KIND, g.periodic, y, g.ney);
+        const int cz = D3 ? fem_axis_cls(KIND, 0, z, g.nez) : 0;
+        const double* __restrict__ c = tab + (size_t)((cz * nc + cy) * nc + cx) * NOFF;
+        double acc = 0.0;
+#pragma unroll
+        for (int dz = 0; dz < (D3 ? W : 1); ++dz)
+#pragma unroll
+          for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx)
+              acc += __ldg(c + (dz * W + dy) * W + dx) * sm[dz * SXY + (ty + dy) * SX + tx + dx];
+        const int n = (z * g.nny + y) * g.nnx + x;
+        body(n, x, y, z, acc, sm[(D3 ? SXY : 0) + (ty + R) * SX + tx + R]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Tiled element-by-element product with per-element coefficients m(e, a, b, nen)
+// and NC source components staged in smem (layout sm[c * NS + s]). For each
+// owned node: y_c = sum_{(e,a)} sum_b m(e,a,b) * src_c(node(e,b)); then
+// body(n, y[NC], center[NC]). Needs NC * (32+2R)(blockDim/32+2R)(3 in 3D) doubles.
+template <int KIND, int NC, class Team, class Load, class Mat, class Body>
+__device__ __forceinline__ void fem_tiled_ebe(const Team& tm, const FemGrid& g, double* __restrict__ sm,
+                                              const Load& load, const Mat& m, const Body& body) {
+  constexpr int R = KI<KIND>::R, NEN = KI<KIND>::NEN;
+  constexpr bool D3 = (KIND == FEM_HEX8);
+  const int TY = blockDim.x >> 5;
+  const int SX = 32 + 2 * R, SY = TY + 2 * R, SXY = SX * SY, NS = SXY * (D3 ? 3 : 1);
+  const int ntx = (g.nnx + 31) >> 5, nty = (g.nny + TY - 1) / TY, nt2 = ntx * nty, ntile = nt2 * g.nnz;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int t = tm.cta(); t < ntile; t += tm.ncta()) {
+    const int z = t / nt2, rr = t - z * nt2, by = rr / ntx, bx = rr - by * ntx;
+    const int x0 = bx * 32 - R, y0 = by * TY - R;
+#pragma unroll 2
+    for (int s = threadIdx.x; s < NS; s += blockDim.x) {
+      const int lz = D3 ? s / SXY : 0, r2 = s - lz * SXY, ly = r2 / SX, lx = r2 - ly * SX;
+      int gx = x0 + lx, gy = y0 + ly, gz = D3 ? z + lz - 1 : 0;
+      if (g.periodic) {
+        gx = gx < 0 ? gx + g.nnx : (gx >= g.nnx ? gx - g.nnx : gx);
+        gy = gy < 0 ? gy + g.nny : (gy >= g.nny ? gy - g.nny : gy);
+      } else {
+        gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
+        gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);
+      }
+      if (D3) gz = gz < 0 ? 0 : (gz >= g.nnz ? g.nnz - 1 : gz);
+      const int j = (gz * g.nny + gy) * g.nnx + gx;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sm[c * NS + s] = load(j, c);
+    }
+    __syncthreads();
+    const int x = bx * 32 + tx, y = by * TY + ty;
+    if (x < g.nnx && y < g.nny) {
+      const int cen = (D3 ? SXY : 0) + (ty + R) * SX + tx + R;
+      double v[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[c] = 0.0;
+      fem_incident_k<KIND>(g, x, y, z, [&](int, int, int, int e, int a) {
+        int dia, dja, dka;
+        fem_local_offset(KIND, a, dia, dja, dka);
+        const int base = cen - dia - dja * SX - dka * SXY;
+        double part[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) part[c] = 0.0;
+#pragma unroll
+        for (int b = 0; b < NEN; ++b) {
+          const int sidx = base + kdi<KIND>(b) + kdj<KIND>(b) * SX + kdk<KIND>(b) * SXY;
+          const double coef = m(e, a, b, NEN);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) part[c] += coef * sm[c * NS + sidx];
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) v[c] += part[c];
+      });
+      double ctr[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) ctr[c] = sm[c * NS + cen];
+      body((z * g.nny + y) * g.nnx + x, v, ctr);
+    }
+    __syncthreads();
+  }
+}

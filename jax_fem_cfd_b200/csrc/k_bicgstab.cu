@@ -2,36 +2,31 @@
 #include "fem_args.cuh"
 
 
-template <int NC, class Src>
-__device__ __forceinline__ void bi_apply(const BiArgs& A, int i, const Src& src, double (&y)[NC]) {
-  const FemGrid& g = A.g;
-  const int nen = g.nen;
-#pragma unroll
-  for (int c = 0; c < NC; ++c) y[c] = 0.0;
-  fem_for_incident(g, i, [&](int ie, int je, int ke, int e, int a) {
-    double part[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) part[c] = 0.0;
-    for (int b = 0; b < nen; ++b) {
-      const double coef = A.op(e, a, b, nen);
-      const int j = fem_elem_node(g, ie, je, ke, b);
-#pragma unroll
-      for (int c = 0; c < NC; ++c) part[c] += coef * src(j, c);
-    }
-#pragma unroll
-    for (int c = 0; c < NC; ++c) y[c] += part[c];
-  });
+template <int KIND, int NC, class Src>
+__device__ __forceinline__ void bi_apply(const BiArgs& A, const MatCombo& op, int i, const Src& src, double (&y)[NC]) {
+  int ix, iy, iz;
+  fem_ij(A.g, i, ix, iy, iz);
+  fem_gather_k<KIND, NC>(A.g, ix, iy, iz, op, src, y);
   if (A.mask) {
 #pragma unroll
     for (int c = 0; c < NC; ++c)
-      if (A.mask[i + (size_t)c * g.nn]) y[c] = src(i, c);
+      if (A.mask[i + (size_t)c * A.g.nn]) y[c] = src(i, c);
   }
 }
 
-template <int NC>
+template <int KIND, int NC>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
   __shared__ double smem[128];
-  const GridTeam gt{A.sync};
+  __shared__ double sAsh[81];
+  __shared__ double tsm[3 * 1836];
+  MatCombo op = A.op;
+  if (op.A) {
+    for (int t = threadIdx.x; t < KI<KIND>::NEN * KI<KIND>::NEN; t += blockDim.x) sAsh[t] = op.A[t];
+    op.A = sAsh;
+  }
+  __shared__ unsigned int s_round;
+  if (threadIdx.x == 0) s_round = 0u;
+  const GridTeam gt{A.sync, &s_round};
   const GridReducer gr{A.sync};
   const int nn = A.g.nn;
   const size_t N = nn;
@@ -42,20 +37,21 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
   {
     {
       double a[2] = {0.0, 0.0};
-      for (int i = gt.rank(); i < nn; i += gt.size()) {
-        double Ax[NC];
-        bi_apply<NC>(A, i, [&](int j, int c) { return A.x[j + c * N]; }, Ax);
+      fem_tiled_ebe<KIND, NC>(gt, A.g, tsm, [&](int j, int c) { return A.x[j + c * N]; }, op,
+                              [&](int i, const double(&Ax)[NC], const double(&xc)[NC]) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          const double bi = A.b[i + c * N], ri = bi - Ax[c];
-          A.r[i + c * N] = ri;
-          A.rhat[i + c * N] = ri;
-          A.p0[i + c * N] = ri;
-          A.q0[i + c * N] = ri;
+          const size_t o = i + c * N;
+          const double ax = (A.mask && A.mask[o]) ? xc[c] : Ax[c];
+          const double bi = A.b[o], ri = bi - ax;
+          A.r[o] = ri;
+          A.rhat[o] = ri;
+          A.p0[o] = ri;
+          A.q0[o] = ri;
           a[0] += bi * bi;
           a[1] += ri * ri;
         }
-      }
+      });
       gr.reduce<2>(a, SL_BB, smem);
       if (!gt.sync()) goto done;
     }
@@ -82,16 +78,16 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
           return r[o] + beta * (pold[o] - omega * qold[o]);
         };
         double a[1] = {0.0};
-        for (int i = gt.rank(); i < nn; i += gt.size()) {
-          double q[NC];
-          bi_apply<NC>(A, i, pn, q);
+        fem_tiled_ebe<KIND, NC>(gt, A.g, tsm, pn, op, [&](int i, const double(&qv)[NC], const double(&pc)[NC]) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
-            pnew[i + c * N] = pn(i, c);
-            qnew[i + c * N] = q[c];
-            a[0] += A.rhat[i + c * N] * q[c];
+            const size_t o = i + c * N;
+            const double q = (A.mask && A.mask[o]) ? pc[c] : qv[c];
+            pnew[o] = pc[c];
+            qnew[o] = q;
+            a[0] += A.rhat[o] * q;
           }
-        }
+        });
         gr.reduce<1>(a, SL_BI + 1, smem);
         if (!gt.sync()) goto done;
       }
@@ -104,18 +100,18 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
       };
       {
         double a[3] = {0.0, 0.0, 0.0};
-        for (int i = gt.rank(); i < nn; i += gt.size()) {
-          double tv[NC];
-          bi_apply<NC>(A, i, sv, tv);
+        fem_tiled_ebe<KIND, NC>(gt, A.g, tsm, sv, op, [&](int i, const double(&tvv)[NC], const double(&sc)[NC]) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
-            const double s = sv(i, c);
-            A.t[i + c * N] = tv[c];
+            const size_t o = i + c * N;
+            const double tvc = (A.mask && A.mask[o]) ? sc[c] : tvv[c];
+            const double s = sc[c];
+            A.t[o] = tvc;
             a[0] += s * s;
-            a[1] += tv[c] * s;
-            a[2] += tv[c] * tv[c];
+            a[1] += tvc * s;
+            a[2] += tvc * tvc;
           }
-        }
+        });
         gr.reduce<3>(a, SL_BI + 2, smem);
         if (!gt.sync()) goto done;
       }
@@ -174,11 +170,15 @@ done:
 
 
 
+static const void* bi_fn(int kind, int ncomp) {
+  if (kind == FEM_Q1_2D) return ncomp == 1 ? (const void*)k_bicgstab<FEM_Q1_2D, 1> : (const void*)k_bicgstab<FEM_Q1_2D, 2>;
+  if (kind == FEM_Q2_2D) return ncomp == 1 ? (const void*)k_bicgstab<FEM_Q2_2D, 1> : (const void*)k_bicgstab<FEM_Q2_2D, 2>;
+  return ncomp == 1 ? (const void*)k_bicgstab<FEM_HEX8, 1> : (const void*)k_bicgstab<FEM_HEX8, 3>;
+}
+
 int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s) {
   BiArgs a = A;
   void* args[] = {&a};
-  const void* fn = ncomp == 1 ? (const void*)k_bicgstab<1>
-                              : (ncomp == 2 ? (const void*)k_bicgstab<2> : (const void*)k_bicgstab<3>);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(FEM_THREADS);
@@ -188,15 +188,17 @@ int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s) {
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  cudaLaunchKernelExC(&cfg, fn, args);
+  cudaLaunchKernelExC(&cfg, bi_fn(A.g.kind, ncomp), args);
   return fem_after_launch("k_bicgstab");
 }
 int fem_coop_occupancy_bi(int* occ) {
-  int a = 0, b = 0, c = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_bicgstab<1>, FEM_THREADS, 0) != cudaSuccess) return -1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_bicgstab<2>, FEM_THREADS, 0) != cudaSuccess) return -1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_bicgstab<3>, FEM_THREADS, 0) != cudaSuccess) return -1;
-  int m = a < b ? a : b;
-  *occ = m < c ? m : c;
+  int m = 1 << 30;
+  for (int kind = 0; kind < 3; ++kind)
+    for (int nc = 1; nc <= 2; ++nc) {
+      int a = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, bi_fn(kind, nc), FEM_THREADS, 0) != cudaSuccess) return -1;
+      m = a < m ? a : m;
+    }
+  *occ = m;
   return 0;
 }

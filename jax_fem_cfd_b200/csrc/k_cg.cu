@@ -3,6 +3,7 @@
 
 
 // Preconditioner application z = M r; returns gamma = r . z.
+template <int KIND>
 __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer& gr, const CgArgs& A, double* smem,
                               double* bstore, double* cg_r, double* cg_p, double* cg_q, double rr, double r2d,
                               double& gamma, double& mz) {
@@ -18,7 +19,7 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
     return true;
   }
   if (A.prec == FEM_PREC_MG) {
-    if (!mg_vcycle(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return false;
+    if (!mg_vcycle<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return false;
     double s[2];
     gr.result<2>(s, SL_X(0), smem);
     if (A.pinned) {
@@ -37,20 +38,22 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
   const double* __restrict__ D = L0.diag;
   const uint8_t* __restrict__ ap = A.ai_pin;
   double* __restrict__ T = L0.t;
-  for (int i = gt.rank(); i < nn; i += gt.size()) {
-    double d1l = fem_gather_fn(L0.g, i, MatShared{L0.Le, 1.0}, [&](int j) { return r[j] / D[j]; }) / D[i];
-    if (ap && ap[i]) d1l = pt ? r[i] / D[i] : 0.0;
-    T[i] = d1l;
-  }
+  const double* __restrict__ iD = L0.invD;
+  fem_tiled_stencil<KIND>(gt, L0.g, L0.tab, smem + 128, [&](int j) { return r[j] * iD[j]; },
+                          [&](int i, int, int, int, double v, double) {
+                            double d1l = v / D[i];
+                            if (ap && ap[i]) d1l = pt ? r[i] / D[i] : 0.0;
+                            T[i] = d1l;
+                          });
   if (!gt.sync()) return false;
   double acc[1] = {0.0};
-  for (int i = gt.rank(); i < nn; i += gt.size()) {
-    double t = fem_gather_fn(L0.g, i, MatShared{L0.Le, 1.0}, [&](int j) { return T[j]; });
+  fem_tiled_stencil<KIND>(gt, L0.g, L0.tab, smem + 128, [&](int j) { return T[j]; }, [&](int i, int, int, int,
+                                                                                         double t, double) {
     if (ap && ap[i]) t = pt ? T[i] : 0.0;
     const double zi = 3 * (r[i] / D[i]) - 3 * T[i] + t / D[i];
     A.z[i] = zi;
     acc[0] += r[i] * zi;
-  }
+  });
   gr.reduce<1>(acc, SL_RZ, smem);
   if (!gt.sync()) return false;
   double s[1];
@@ -59,13 +62,16 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
   return true;
 }
 
+template <int KIND>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q) {
-  __shared__ double smem[128];
+  extern __shared__ double smem[];  // [0,128) reductions, [128, 128+FEM_TILE_SMEM) tiles, then CTA-0 levels
   __shared__ double bstore[FEM_NSLOTS];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
   const CgArgs& A = sA;
-  const GridTeam gt{A.sync};
+  __shared__ unsigned int s_round;
+  if (threadIdx.x == 0) s_round = 0u;
+  const GridTeam gt{A.sync, &s_round};
   const GridReducer gr{A.sync};
   const MgLevel& L0 = A.lv[0];
   const FemGrid& g = L0.g;
@@ -92,17 +98,17 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
     // r0 = b - A x0
     {
       double a2[2] = {0.0, 0.0}, a3[2] = {0.0, 0.0}, a1[1] = {0.0};
-      for (int i = gt.rank(); i < nn; i += gt.size()) {
-        double Ax = fem_gather_fn(g, i, MatShared{L0.Le, 1.0}, [&](int j) { return A.x[j]; });
+      fem_tiled_stencil<KIND>(gt, g, L0.tab, smem + 128, [&](int j) { return A.x[j]; }, [&](int i, int, int, int,
+                                                                                             double Ax, double) {
         if (pin0 && pin0[i]) Ax = 0.0;
         const double bi = b[i], ri = bi - Ax;
         A.r[i] = ri;
         a2[0] += bi * bi;
         a2[1] += ri * ri;
         a3[0] += ri;
-        a3[1] += ri / D[i];
+        a3[1] += ri * L0.invD[i];
         a1[0] += ri * ri / D[i];
-      }
+      });
       gr.reduce<2>(a2, SL_BB, smem);
       gr.reduce<2>(a3, SL_R(0), smem);
       gr.reduce<1>(a1, SL_RZ, smem);
@@ -114,7 +120,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
     rr = bb_rr[1];
     const double atol2 = fmax(A.tol * A.tol * bb_rr[0], A.atol * A.atol);
     double gamma, mz;
-    if (!cg_apply_prec(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, r2d[0], gamma, mz)) goto done;
+    if (!cg_apply_prec<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, r2d[0], gamma, mz)) goto done;
     double beta = 0.0;
     bool have_p = false;
     int cur = 0;
@@ -126,7 +132,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
       double* __restrict__ pnew = cur ? A.p0 : A.p1;
       const int prec = A.prec;
       const double* __restrict__ r = A.r;
-      const double* __restrict__ zs = (prec == FEM_PREC_MG) ? L0.x : A.z;
+      const double* __restrict__ zs = (prec == FEM_PREC_MG) ? L0.t : A.z;
       auto zval = [&](int j) -> double {
         if (prec == FEM_PREC_NONE) return r[j];
         if (prec == FEM_PREC_JACOBI) return r[j] / D[j];
@@ -136,14 +142,12 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
       auto pz = [&](int j) -> double { return have_p ? zval(j) + beta * pold[j] : zval(j); };
       {
         double a[1] = {0.0};
-        for (int i = gt.rank(); i < nn; i += gt.size()) {
-          const double pn = pz(i);
+        fem_tiled_stencil<KIND>(gt, g, L0.tab, smem + 128, pz, [&](int i, int, int, int, double q, double pn) {
           pnew[i] = pn;
-          double q = fem_gather_fn(g, i, MatShared{L0.Le, 1.0}, pz);
           if (pin0 && pin0[i]) q = 0.0;
           A.Ap[i] = q;
           a[0] += pn * q;
-        }
+        });
         gr.reduce<1>(a, SL_PAP, smem);
         if (!gt.sync()) goto done;
       }
@@ -158,7 +162,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
           A.r[i] = ri;
           a2[1] += ri * ri;
           a3[0] += ri;
-          a3[1] += ri / D[i];
+          a3[1] += ri * L0.invD[i];
           a1[0] += ri * ri / D[i];
         }
         gr.reduce<2>(a2, SL_BB, smem);
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
         gamma_ = t1[0];
       } else {
         if (!(rr > atol2 && k < A.maxiter)) break;  // z of a final iteration is never used
-        if (!cg_apply_prec(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, t1[0], gamma_, mz)) goto done;
+        if (!cg_apply_prec<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, t1[0], gamma_, mz)) goto done;
       }
       beta = gamma_ / gamma;
       gamma = gamma_;
@@ -218,14 +222,17 @@ done:
 
 
 
+template <int KIND>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q,
                                                             double* z) {
-  __shared__ double smem[128];
+  extern __shared__ double smem[];  // [0,128) reductions, [128, 128+FEM_TILE_SMEM) tiles, then CTA-0 levels
   __shared__ double bstore[FEM_NSLOTS];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
   const CgArgs& A = sA;
-  const GridTeam gt{A.sync};
+  __shared__ unsigned int s_round;
+  if (threadIdx.x == 0) s_round = 0u;
+  const GridTeam gt{A.sync, &s_round};
   const GridReducer gr{A.sync};
   const MgLevel& L0 = A.lv[0];
   const int nn = L0.g.nn;
@@ -234,22 +241,23 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double
   double a[2] = {0.0, 0.0};
   for (int i = gt.rank(); i < nn; i += gt.size()) {
     a[0] += L0.r[i];
-    a[1] += L0.r[i] / L0.diag[i];
+    a[1] += L0.r[i] * L0.invD[i];
   }
   gr.reduce<2>(a, SL_R(0), smem);
   if (!gt.sync()) return;
-  if (!mg_vcycle(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return;
+  if (!mg_vcycle<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return;
   double sx[2];
   gr.result<2>(sx, SL_X(0), smem);
   const double mz = A.pinned ? 0.0 : sx[0] / nn;
-  for (int i = gt.rank(); i < nn; i += gt.size()) z[i] = L0.x[i] - mz;
+  for (int i = gt.rank(); i < nn; i += gt.size()) z[i] = L0.t[i] - mz;
 }
 
-static int coop_launch(const void* fn, int grid, void** args, cudaStream_t s, const char* what) {
+static int coop_launch(const void* fn, int grid, void** args, cudaStream_t s, const char* what, size_t dyn = 0) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(FEM_THREADS);
   cfg.stream = s;
+  cfg.dynamicSmemBytes = dyn;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeCooperative;
   at[0].val.cooperative = 1;
@@ -259,20 +267,45 @@ static int coop_launch(const void* fn, int grid, void** args, cudaStream_t s, co
   return fem_after_launch(what);
 }
 
+static const void* cg_fn(int kind) {
+  return kind == FEM_Q1_2D ? (const void*)k_cg<FEM_Q1_2D>
+                           : (kind == FEM_Q2_2D ? (const void*)k_cg<FEM_Q2_2D> : (const void*)k_cg<FEM_HEX8>);
+}
+static const void* vc_fn(int kind) {
+  return kind == FEM_Q1_2D ? (const void*)k_vcycle<FEM_Q1_2D>
+                           : (kind == FEM_Q2_2D ? (const void*)k_vcycle<FEM_Q2_2D> : (const void*)k_vcycle<FEM_HEX8>);
+}
 int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq};
-  return coop_launch((const void*)k_cg, grid, args, s, "k_cg");
+  return coop_launch(cg_fn(A.lv[0].g.kind), grid, args, s, "k_cg",
+                     (size_t)(128 + FEM_TILE_SMEM + A.block_smem) * sizeof(double));
 }
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq, &z};
-  return coop_launch((const void*)k_vcycle, grid, args, s, "k_vcycle");
+  return coop_launch(vc_fn(A.lv[0].g.kind), grid, args, s, "k_vcycle",
+                     (size_t)(128 + FEM_TILE_SMEM + A.block_smem) * sizeof(double));
 }
 int fem_coop_occupancy_cg(int* occ) {
-  int a = 0, b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg, FEM_THREADS, 0) != cudaSuccess) return -1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_vcycle, FEM_THREADS, 0) != cudaSuccess) return -1;
-  *occ = a < b ? a : b;
+  int m = 1 << 30;
+  for (int kind = 0; kind < 3; ++kind) {
+    // allow the CTA-0 multigrid levels up to FEM_BLOCK_SMEM_MAX bytes of dynamic smem
+    if (cudaFuncSetAttribute(cg_fn(kind), cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_DYN_SMEM_MAX) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(vc_fn(kind), cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_DYN_SMEM_MAX) !=
+            cudaSuccess)
+      return -1;
+    int a = 0, b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, cg_fn(kind), FEM_THREADS, FEM_DYN_SMEM_MAX) !=
+        cudaSuccess)
+      return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, vc_fn(kind), FEM_THREADS, FEM_DYN_SMEM_MAX) !=
+        cudaSuccess)
+      return -1;
+    m = a < m ? a : m;
+    m = b < m ? b : m;
+  }
+  *occ = m;
   return 0;
 }

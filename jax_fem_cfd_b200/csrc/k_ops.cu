@@ -2,33 +2,44 @@
 #include "fem_args.cuh"
 
 
-template <int NC>
+template <int KIND, int NC>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_ebe_apply(FemGrid g, MatCombo m, const double* __restrict__ x,
                                                               double* __restrict__ y) {
+  const size_t N = g.nn;
+  auto src = [&](int j, int c) { return x[j + c * N]; };
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
     double v[NC];
-    fem_gather<NC>(g, n, m, x, g.nn, v);
+    fem_gather_k<KIND, NC>(g, ix, iy, iz, m, src, v);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) y[n + (size_t)c * g.nn] = v[c];
+    for (int c = 0; c < NC; ++c) y[n + c * N] = v[c];
   }
 }
 
-template <int ND>
+template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_grad(FemGrid g, const double* __restrict__ Ge,
                                                          const double* __restrict__ P, double* __restrict__ y) {
+  constexpr int ND = KI<KIND>::DIM;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
     double v[ND];
-    fem_gather_grad<ND>(g, n, Ge, P, v);
+    fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, Ge, [&](int j) { return P[j]; }, v);
 #pragma unroll
     for (int d = 0; d < ND; ++d) y[n + (size_t)d * g.nn] = v[d];
   }
 }
 
-template <int ND>
+template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_div(FemGrid g, const double* __restrict__ Ge,
                                                         const double* __restrict__ U, double* __restrict__ y) {
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x)
-    y[n] = fem_gather_div<ND>(g, n, Ge, U, g.nn);
+  constexpr int ND = KI<KIND>::DIM;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
+    y[n] = fem_gather_div_k<KIND, ND>(g, ix, iy, iz, Ge, U);
+  }
 }
 
 // Ce / Ctau_tilde build, FEM_CE_EPB elements per CTA.
@@ -226,21 +237,21 @@ __global__ void k_elem_combine(size_t n, double s_m, const double* __restrict__ 
 
 int fem_launch_ebe(int ncomp, const FemGrid& g, const MatCombo& m, const double* x, double* y, cudaStream_t s) {
   const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
-  if (ncomp == 1) k_ebe_apply<1><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
-  else if (ncomp == 2) k_ebe_apply<2><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
-  else k_ebe_apply<3><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
+  FEM_KIND_DISPATCH(g.kind, K, {
+    if (ncomp == 1) k_ebe_apply<K, 1><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
+    else if (ncomp == 2) k_ebe_apply<K, 2><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
+    else k_ebe_apply<K, 3><<<nb, FEM_OP_THREADS, 0, s>>>(g, m, x, y);
+  });
   return fem_after_launch("k_ebe_apply");
 }
 int fem_launch_grad(int ndim, const FemGrid& g, const double* Ge, const double* P, double* y, cudaStream_t s) {
   const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
-  if (ndim == 2) k_grad<2><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, P, y);
-  else k_grad<3><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, P, y);
+  FEM_KIND_DISPATCH(g.kind, K, (k_grad<K><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, P, y)));
   return fem_after_launch("k_grad");
 }
 int fem_launch_div(int ndim, const FemGrid& g, const double* Ge, const double* U, double* y, cudaStream_t s) {
   const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
-  if (ndim == 2) k_div<2><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, U, y);
-  else k_div<3><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, U, y);
+  FEM_KIND_DISPATCH(g.kind, K, (k_div<K><<<nb, FEM_OP_THREADS, 0, s>>>(g, Ge, U, y)));
   return fem_after_launch("k_div");
 }
 int fem_launch_convection(const FemGrid& g, const FemQuad& Q, const double* U, double beta, int mode, double* out,

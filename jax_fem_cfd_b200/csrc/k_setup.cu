@@ -218,18 +218,21 @@ __global__ void k_assemble_diag(FemGrid g, int ndim, const double* __restrict__ 
 
 
 __global__ void k_level_sums(FemGrid g, FemLattice lat, const double* __restrict__ diag, double* out) {
-  __shared__ double smem[96];
-  double a[2] = {0.0, 0.0};
+  __shared__ double smem[128];
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
   const int ux = lat.ux();
   for (int i = threadIdx.x; i < g.nn; i += blockDim.x) {
-    a[0] += 1.0 / diag[i];
-    a[1] += fem_interp_colsum(lat, i / ux, i % ux);
+    const double iv = 1.0 / diag[i];
+    const int R = i / ux, C = i % ux;
+    const double rc = fem_restrict_rowsum(lat, R, C);
+    a[0] += iv;
+    a[1] += fem_interp_colsum(lat, R, C);
+    a[2] += rc;
+    a[3] += rc * iv;
   }
-  fem_block_sum<2>(a, smem);
-  if (threadIdx.x == 0) {
-    out[0] = a[0];
-    out[1] = a[1];
-  }
+  fem_block_sum<4>(a, smem);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 4; ++q) out[q] = a[q];
 }
 
 int fem_launch_mesh_generate(const FemGrid& g, double dx, double dy, double dz, double* coords, int64_t* nconn,
@@ -254,4 +257,26 @@ int fem_launch_assemble_diag(const FemGrid& g, int ndim, const double* Me, const
 int fem_launch_level_sums(const FemGrid& g, const FemLattice& lat, const double* diag, double* out, cudaStream_t s) {
   k_level_sums<<<1, 512, 0, s>>>(g, lat, diag, out);
   return fem_after_launch("k_level_sums");
+}
+
+__global__ void k_invdiag(int n, const double* __restrict__ D, const uint8_t* __restrict__ pin, double* __restrict__ invD,
+                          double* __restrict__ winvD) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = 1.0 / D[i];
+    invD[i] = v;
+    winvD[i] = (pin && pin[i]) ? 0.0 : v;
+  }
+}
+
+int fem_launch_stencil_build(const FemGrid& g, const double* A, int transpose, int skip_diag, double* out,
+                             cudaStream_t s) {
+  const int ncls = fem_stencil_ncls(g);
+  FEM_KIND_DISPATCH(g.kind, K, (k_stencil_build<K><<<1, 64, 0, s>>>(g, A, transpose, skip_diag, out)));
+  (void)ncls;
+  return fem_after_launch("k_stencil_build");
+}
+
+int fem_launch_invdiag(int n, const double* D, const uint8_t* pin, double* invD, double* winvD, cudaStream_t s) {
+  k_invdiag<<<fem_nblocks(n, 256), 256, 0, s>>>(n, D, pin, invD, winvD);
+  return fem_after_launch("k_invdiag");
 }

@@ -3,7 +3,7 @@
 
 
 // rhs of solvers/standard.py:31-37 and the initial guess x0; also keeps G P_n.
-template <int ND>
+template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_mom_rhs(StepArgs S, const double* __restrict__ Un,
                                                             const double* __restrict__ Pn,
                                                             const double* __restrict__ Ud,
@@ -11,12 +11,17 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_mom_rhs(StepArgs S, const do
                                                             double* __restrict__ x0, double* __restrict__ gPn) {
   const FemGrid& g = S.g;
   const size_t N = g.nn;
+  constexpr int ND = KI<KIND>::DIM;
   const MatCombo vc{S.Le, S.mu, S.Ce, S.rho, 0, nullptr, 0.0};
+  const MatShared ms_m{S.Me, 1.0};
+  auto src = [&](int j, int c) { return Un[j + c * N]; };
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
     double ms[ND], v[ND], gp[ND];
-    fem_gather<ND>(g, n, MatShared{S.Me, 1.0}, Un, g.nn, ms);
-    fem_gather<ND>(g, n, vc, Un, g.nn, v);
-    fem_gather_grad<ND>(g, n, S.Ge, Pn, gp);
+    fem_gather_k<KIND, ND>(g, ix, iy, iz, ms_m, src, ms);
+    fem_gather_k<KIND, ND>(g, ix, iy, iz, vc, src, v);
+    fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return Pn[j]; }, gp);
 #pragma unroll
     for (int c = 0; c < ND; ++c) {
       const size_t o = n + c * N;
@@ -38,14 +43,17 @@ __global__ void k_ustar(int n, double c, const double* __restrict__ Uh, const do
 }
 
 // PPE rhs (rho/dt)(D U* - F_p) with pinned rows zeroed, and x0 (solvers/standard.py:97-107).
-template <int ND>
+template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_p_rhs(StepArgs S, const double* __restrict__ Us,
                                                           const double* __restrict__ Fp,
                                                           const double* __restrict__ Pn, double* __restrict__ rhs,
                                                           double* __restrict__ x0) {
   const FemGrid& g = S.g;
+  constexpr int ND = KI<KIND>::DIM;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
-    const double du = fem_gather_div<ND>(g, n, S.Ge, Us, g.nn);
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
+    const double du = fem_gather_div_k<KIND, ND>(g, ix, iy, iz, S.Ge, Us);
     double r = (S.rho / S.dt) * (Fp ? du - Fp[n] : du);
     double x = Pn[n];
     if (S.pinned && S.pmask && S.pmask[n]) {
@@ -58,16 +66,19 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_p_rhs(StepArgs S, const doub
 }
 
 // U = U* - (dt/rho) G P / M ; U[gamma_d] = U_d   (solvers/standard.py:160-163)
-template <int ND>
+template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_ufinal(StepArgs S, const double* __restrict__ Us,
                                                            const double* __restrict__ P,
                                                            const double* __restrict__ Ud, double* __restrict__ U) {
   const FemGrid& g = S.g;
   const size_t N = g.nn;
   const double c = S.dt / S.rho;
+  constexpr int ND = KI<KIND>::DIM;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
     double gp[ND];
-    fem_gather_grad<ND>(g, n, S.Ge, P, gp);
+    fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return P[j]; }, gp);
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       const size_t o = n + d * N;
@@ -80,14 +91,20 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_ufinal(StepArgs S, const dou
 // Scalar transport rhs (passive_transport.py:294-301 / 318-325):
 // rhs = (1/dt)(Me + Mtau_e) phi_n - 0.5 (Ce_n + D Le + Ctau_e) phi_n, with the
 // per-element parts pre-combined into Erhs_e; Dirichlet rows -> phi_d.
+template <int KIND>
 __global__ void k_phi_rhs(FemGrid g, const double* __restrict__ Me, const double* __restrict__ Le, double dt, double D,
                           const double* __restrict__ Mt, const double* __restrict__ Cn, const double* __restrict__ Ct,
                           const double* __restrict__ phin, const uint8_t* __restrict__ mask,
                           const double* __restrict__ phid, double* __restrict__ rhs, double* __restrict__ x0) {
+  const MatCombo mm{Me, 1.0, Mt, 1.0, 0, nullptr, 0.0};
+  const MatCombo vm{Le, D, Cn, 1.0, 0, Ct, 1.0};
+  auto src = [&](int j, int) { return phin[j]; };
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
     double ms[1], vc[1];
-    fem_gather<1>(g, n, MatCombo{Me, 1.0, Mt, 1.0, 0, nullptr, 0.0}, phin, g.nn, ms);
-    fem_gather<1>(g, n, MatCombo{Le, D, Cn, 1.0, 0, Ct, 1.0}, phin, g.nn, vc);
+    fem_gather_k<KIND, 1>(g, ix, iy, iz, mm, src, ms);
+    fem_gather_k<KIND, 1>(g, ix, iy, iz, vm, src, vc);
     const double r = (1 / dt) * ms[0] - 0.5 * vc[0];
     const bool m = mask && mask[n];
     rhs[n] = m ? phid[n] : r;
@@ -95,13 +112,10 @@ __global__ void k_phi_rhs(FemGrid g, const double* __restrict__ Me, const double
   }
 }
 
-
-
 int fem_launch_mom_rhs(const StepArgs& S, const double* Un, const double* Pn, const double* Ud, const double* F,
                        double* rhs, double* x0, double* gPn, cudaStream_t s) {
   const int nb = fem_nblocks(S.g.nn, FEM_OP_THREADS);
-  if (S.ndim == 2) k_mom_rhs<2><<<nb, FEM_OP_THREADS, 0, s>>>(S, Un, Pn, Ud, F, rhs, x0, gPn);
-  else k_mom_rhs<3><<<nb, FEM_OP_THREADS, 0, s>>>(S, Un, Pn, Ud, F, rhs, x0, gPn);
+  FEM_KIND_DISPATCH(S.g.kind, K, (k_mom_rhs<K><<<nb, FEM_OP_THREADS, 0, s>>>(S, Un, Pn, Ud, F, rhs, x0, gPn)));
   return fem_after_launch("k_mom_rhs");
 }
 int fem_launch_ustar(int n, double c, const double* Uh, const double* gPn, const double* M, double* Us,
@@ -112,21 +126,21 @@ int fem_launch_ustar(int n, double c, const double* Uh, const double* gPn, const
 int fem_launch_p_rhs(const StepArgs& S, const double* Us, const double* Fp, const double* Pn, double* rhs, double* x0,
                      cudaStream_t s) {
   const int nb = fem_nblocks(S.g.nn, FEM_OP_THREADS);
-  if (S.ndim == 2) k_p_rhs<2><<<nb, FEM_OP_THREADS, 0, s>>>(S, Us, Fp, Pn, rhs, x0);
-  else k_p_rhs<3><<<nb, FEM_OP_THREADS, 0, s>>>(S, Us, Fp, Pn, rhs, x0);
+  FEM_KIND_DISPATCH(S.g.kind, K, (k_p_rhs<K><<<nb, FEM_OP_THREADS, 0, s>>>(S, Us, Fp, Pn, rhs, x0)));
   return fem_after_launch("k_p_rhs");
 }
 int fem_launch_ufinal(const StepArgs& S, const double* Us, const double* P, const double* Ud, double* U,
                       cudaStream_t s) {
   const int nb = fem_nblocks(S.g.nn, FEM_OP_THREADS);
-  if (S.ndim == 2) k_ufinal<2><<<nb, FEM_OP_THREADS, 0, s>>>(S, Us, P, Ud, U);
-  else k_ufinal<3><<<nb, FEM_OP_THREADS, 0, s>>>(S, Us, P, Ud, U);
+  FEM_KIND_DISPATCH(S.g.kind, K, (k_ufinal<K><<<nb, FEM_OP_THREADS, 0, s>>>(S, Us, P, Ud, U)));
   return fem_after_launch("k_ufinal");
 }
 int fem_launch_phi_rhs(const FemGrid& g, const double* Me, const double* Le, double dt, double D, const double* Mt,
                        const double* Cn, const double* Ct, const double* phin, const uint8_t* mask,
                        const double* phid, double* rhs, double* x0, cudaStream_t s) {
-  k_phi_rhs<<<fem_nblocks(g.nn, FEM_OP_THREADS), FEM_OP_THREADS, 0, s>>>(g, Me, Le, dt, D, Mt, Cn, Ct, phin, mask,
-                                                                         phid, rhs, x0);
+  const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
+  FEM_KIND_DISPATCH(g.kind, K,
+                    (k_phi_rhs<K><<<nb, FEM_OP_THREADS, 0, s>>>(g, Me, Le, dt, D, Mt, Cn, Ct, phin, mask, phid, rhs,
+                                                               x0)));
   return fem_after_launch("k_phi_rhs");
 }
