@@ -509,8 +509,9 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
   FEM_ALLOC(c->cq, ncn);
   // First level handled by CTA 0 alone: the coarsest levels whose vectors
   // (x, r, t per level + 3 coarse-CG vectors) fit the dynamic smem budget and
-  // whose sizes are small enough for one SM (<= FEM_MG_BLOCK_NN nodes).
-  int small = 8192;
+  // whose sizes are small enough for one SM (<= FEM_MG_BLOCK_NN nodes; 1024
+  // measured best on the 512^2-node Q2 Taylor-Green pressure solve).
+  int small = 1024;
   const char* ev = getenv("FEM_MG_BLOCK_NN");
   if (ev) small = atoi(ev);
   const long long budget = FEM_BLOCK_SMEM_MAX / sizeof(double);

@@ -177,7 +177,12 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
   // level (<= one tile per CTA) within the smem staging buffer
   const int CTX = 16;
   const int ntx = (cux + CTX - 1) / CTX;
-  int CTY = (cuy * ntx + tm.ncta() - 1) / tm.ncta();
+  int CTY;
+  {
+    int nty_t = tm.ncta() / ntx;
+    if (nty_t < 1) nty_t = 1;
+    CTY = (cuy + nty_t - 1) / nty_t;
+  }
   {
     const int cap = (FEM_TILE_SMEM - (2 * CTX + 1 + 2 * R) * (1 + 2 * R) - (2 * CTX + 1)) /
                     (2 * (2 * CTX + 1 + 2 * R) + 2 * (2 * CTX + 1));

@@ -341,7 +341,9 @@ __device__ __forceinline__ double fem_gather_div_k(const FemGrid& g, int i, int 
 __device__ __forceinline__ int fem_tile_rows(int nx, int ny, int nplanes, int halo, int ncta, int cap_doubles,
                                              int planes_staged) {
   const int ntx = (nx + 31) >> 5;
-  int th = (ny * ntx * nplanes + ncta - 1) / ncta;
+  int nty = ncta / (ntx * nplanes);
+  if (nty < 1) nty = 1;
+  int th = (ny + nty - 1) / nty;
   const int rows_per_tile_cap = cap_doubles / ((32 + 2 * halo) * planes_staged) - 2 * halo;
   const int minr = blockDim.x >> 5;
   if (th < minr) th = minr;
