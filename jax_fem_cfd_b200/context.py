@@ -33,8 +33,17 @@ def ptr(t):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 
 
+def _from_dlpack(x):
+    """Zero-copy torch view of a foreign DLPack producer (e.g. a JAX array)."""
+    if not isinstance(x, (torch.Tensor, np.ndarray)) and hasattr(x, "__dlpack__"):
+        return torch.from_dlpack(x)
+    return x
+
+
 def f64(x):
-    """Contiguous float64 CUDA tensor view/copy of x (numpy, list, scalar or tensor)."""
+    """Contiguous float64 CUDA tensor view/copy of x (numpy, list, scalar, tensor
+    or DLPack producer)."""
+    x = _from_dlpack(x)
     if isinstance(x, torch.Tensor):
         if x.device.type != "cuda":
             x = x.to(device(), non_blocking=True)
@@ -45,6 +54,7 @@ def f64(x):
 
 
 def i64(x):
+    x = _from_dlpack(x)
     if isinstance(x, torch.Tensor):
         if x.device.type != "cuda":
             x = x.to(device())
