@@ -226,6 +226,36 @@ int fem_transport_phi(fem_ctx* ctx, const double* U_n, const double* U, const do
 int fem_boundary_flux(fem_ctx* ctx, const int32_t* bconn, const double* nvec, int nb, int nodes_per_face,
                       const double* U_full, double* F_p, cudaStream_t stream);
 
+/* Same result as fem_boundary_flux, but the call never allocates or frees
+ * device memory. No counterpart in the reference: the reference has one
+ * boundary integral and leaves device memory to XLA.
+ *
+ * fem_boundary_flux keeps its per-face scratch (nb * nodes_per_face doubles) in
+ * the context. When a larger boundary arrives, it grows that scratch with a
+ * stream synchronize, cudaFree and cudaMalloc, and cudaFree synchronizes the
+ * whole device. Some callers cannot do that: a host framework whose handlers
+ * must take every device byte from the framework's own allocator, or a
+ * time-stepping loop that must not stall the device when its set of boundary
+ * faces changes. This entry point is for them. Its scratch is one fixed array
+ * of FEM_NOALLOC_FACE_VALUES doubles inside this library, one copy per device,
+ * held by every GPU that loads the library until the process exits.
+ *  - nb * nodes_per_face must be <= FEM_NOALLOC_FACE_VALUES (for example 32768
+ *    lin2 edges or 16384 quad4 faces). Larger requests return FEM_E_ARG with
+ *    the limit in fem_last_error(), and nothing is launched.
+ *  - The calling thread's current device must be ctx's device (else
+ *    FEM_E_STATE). The first call on each device looks up that device's copy
+ *    of the array (cudaGetSymbolAddress, which may load the library's device
+ *    code). Make that first call before any stream capture begins.
+ *  - Nothing has to start at zero: each call writes every scratch value it
+ *    reads, on `stream`, before reading it.
+ *  - All calls on one device share the one array, and it keeps the last
+ *    call's contents. Two calls that can overlap on the GPU (different streams
+ *    with no event between them, or different host threads) race on it and
+ *    may return wrong fluxes: order them on one stream. */
+#define FEM_NOALLOC_FACE_VALUES 65536
+int fem_boundary_flux_noalloc(fem_ctx* ctx, const int32_t* bconn, const double* nvec, int nb,
+                              int nodes_per_face, const double* U_full, double* F_p, cudaStream_t stream);
+
 /* out[idx[k]] = vals[k] for k < n (idx int64; vals NULL writes `value`),
  * the functional x.at[idx].set(v) of the reference. */
 int fem_scatter(const int64_t* idx, const double* vals, double value, int n, double* out, cudaStream_t stream);

@@ -52,6 +52,7 @@ SIGNATURES = {
     "fem_step4": (c_int, [P, P, P, c_double, c_double, c_double, P, P, P, c_double, c_int, P, P, P, P, P]),
     "fem_transport_phi": (c_int, [P, P, P, P, c_double, c_double, c_int, P, P, c_double, P, P, P, P]),
     "fem_boundary_flux": (c_int, [P, P, P, c_int, c_int, P, P, P]),
+    "fem_boundary_flux_noalloc": (c_int, [P, P, P, c_int, c_int, P, P, P]),
     "fem_scatter": (c_int, [P, P, c_double, c_int, P, P]),
     "fem_make_mask": (c_int, [P, c_int, c_int, P, P]),
     "fem_dot": (c_int, [P, P, P, c_int, P, P]),

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "fem_b200.h"
@@ -842,6 +843,59 @@ extern "C" int fem_boundary_flux(fem_ctx* c, const int32_t* bconn, const double*
     c->Fe_cap = nb * npf;
   }
   return fem_launch_boundary(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, c->Fe, Fp, s);
+}
+
+// Fixed per-face scratch of fem_boundary_flux_noalloc: one copy per device in
+// this library's device image, shared by every call on that device. Each call
+// writes all nb * npf values it later reads (k_boundary_fe before
+// k_boundary_scatter, same stream), so no value has to start at zero.
+static __device__ __align__(256) double g_noalloc_fe[FEM_NOALLOC_FACE_VALUES];
+
+#define FEM_NOALLOC_MAX_DEVICES 64
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_fe_ptr[FEM_NOALLOC_MAX_DEVICES] = {};
+
+// Device address of `device`'s copy of g_noalloc_fe (host code cannot use the
+// symbol itself). Looked up once per device on its first call, with that
+// device current; later calls read the cached value.
+static int noalloc_fe_scratch(int device, double** out) {
+  if (device < 0 || device >= FEM_NOALLOC_MAX_DEVICES) {
+    snprintf(g_err, sizeof(g_err), "fem_boundary_flux_noalloc: device %d beyond the %d supported", device,
+             FEM_NOALLOC_MAX_DEVICES);
+    return FEM_E_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_fe_ptr[device]) {
+    double* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_fe);
+    if (e != cudaSuccess) return set_err("cudaGetSymbolAddress(g_noalloc_fe)", e);
+    g_noalloc_fe_ptr[device] = p;
+  }
+  *out = g_noalloc_fe_ptr[device];
+  return FEM_OK;
+}
+
+extern "C" int fem_boundary_flux_noalloc(fem_ctx* c, const int32_t* bconn, const double* nvec, int nb, int npf,
+                                         const double* U, double* Fp, cudaStream_t s) {
+  if (!c || !bconn || !nvec || !U || !Fp || nb < 0 || npf < 2 || npf > 4) return FEM_E_ARG;
+  const long long need = (long long)nb * npf;
+  if (need > FEM_NOALLOC_FACE_VALUES) {
+    snprintf(g_err, sizeof(g_err),
+             "fem_boundary_flux_noalloc: nb * nodes_per_face = %lld exceeds the fixed scratch of %d values "
+             "(use fem_boundary_flux)",
+             need, FEM_NOALLOC_FACE_VALUES);
+    return FEM_E_ARG;
+  }
+  int cur = -1;
+  FEM_CHECK(cudaGetDevice(&cur));
+  if (cur != c->device) {
+    snprintf(g_err, sizeof(g_err), "fem_boundary_flux_noalloc: current device %d is not the context's device %d",
+             cur, c->device);
+    return FEM_E_STATE;
+  }
+  double* fe = nullptr;
+  FEM_TRY(noalloc_fe_scratch(cur, &fe));
+  return fem_launch_boundary(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, fe, Fp, s);
 }
 
 extern "C" int fem_scatter(const int64_t* idx, const double* vals, double value, int n, double* out,
