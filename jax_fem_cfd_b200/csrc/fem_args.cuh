@@ -6,9 +6,10 @@
 #define FEM_THREADS 512
 #define FEM_OP_THREADS 256
 // dynamic shared memory available to the CTA-0 multigrid levels of k_cg / k_vcycle
-#define FEM_BLOCK_SMEM_MAX (150 * 1024)
-// whole dynamic smem of k_cg / k_vcycle: reduction scratch + tile staging + CTA-0 levels
-#define FEM_DYN_SMEM_MAX ((128 + FEM_TILE_SMEM) * 8 + FEM_BLOCK_SMEM_MAX)
+#define FEM_BLOCK_SMEM_MAX (120 * 1024)
+// whole dynamic smem of k_cg / k_vcycle: reduction scratch + tile staging +
+// stencil tables + CTA-0 levels
+#define FEM_DYN_SMEM_MAX ((128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * 8 + FEM_BLOCK_SMEM_MAX)
 
 struct BiArgs {
   FemSync sync;

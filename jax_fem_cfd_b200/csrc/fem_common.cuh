@@ -209,17 +209,53 @@ __device__ __forceinline__ void fem_trace_mark(const FemSync& s, unsigned long l
   }
 }
 
+// Shared-memory staging. fem_stage issues dst[q] = src[idx(q)] for q < n: by
+// 8-byte cp.async (no register round trip, every copy of the thread in flight)
+// when src is global memory, by plain copies when src is itself in shared
+// memory (the CTA-0 coarse levels). fem_stage_wait completes all of them and
+// makes them visible to the whole CTA.
+template <class Idx>
+__device__ __forceinline__ void fem_stage(double* dst, const double* src, int n, const Idx& idx) {
+  if (src == nullptr) return;  // unused source slot
+  if (__isGlobal(src)) {
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + q);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src + idx(q)) : "memory");
+    }
+  } else {
+    for (int q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[idx(q)];
+  }
+}
+__device__ __forceinline__ void fem_stage_wait() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+}
+__device__ __forceinline__ int fem_floordiv2(int v) { return v >> 1; }  // arithmetic shift: floor for v < 0
+// v mod n in [0, n) for any int v (periodic lattice coordinates of staged halos,
+// which can lie more than one period away when a tile is wider than the level)
+__device__ __forceinline__ int fem_wrap(int v, int n) {
+  if ((unsigned)v < (unsigned)n) return v;
+  if (v < 0 && v >= -n) return v + n;
+  if (v >= n && v < 2 * n) return v - n;
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+
 // Grid barrier on a monotonic arrival counter (reset to 0 before each launch):
 // barrier number k of the launch completes when the counter reaches
 // k * gridDim.x. One fire-and-forget release-add per CTA, then acquire polling.
 struct GridTeam {
-  FemSync s;
+  const FemSync* s;     // the launch's barrier state (shared-memory copy of the kernel arguments)
   unsigned int* round;  // per-CTA count of completed barriers (shared memory, thread 0, starts at 0)
   __device__ __forceinline__ int rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
   __device__ __forceinline__ int size() const { return gridDim.x * blockDim.x; }
   __device__ __forceinline__ int cta() const { return blockIdx.x; }
   __device__ __forceinline__ int ncta() const { return gridDim.x; }
   // Returns false if the kernel must stop (timeout or error raised elsewhere).
+  // Ordering: the CTA's writes reach thread 0 through __syncthreads, its
+  // release-add publishes them at gpu scope, the pollers' acquire-load of the
+  // final count orders every later read after them, and the closing
+  // __syncthreads passes that on to the CTA's other threads.
   __device__ bool sync() const {
     __shared__ int s_ok;
     __syncthreads();
@@ -227,30 +263,31 @@ struct GridTeam {
       int ok = 1;
       const unsigned int target = (*round + 1u) * gridDim.x;
       *round = *round + 1u;
-      __threadfence();
-      asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(s.count), "r"(1u) : "memory");
+      unsigned int* cnt = s->count;
+      int* err = s->err;
+      asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(cnt), "r"(1u) : "memory");
       if (gridDim.x > 1) {
         const unsigned long long t0 = fem_globaltimer();
         unsigned int polls = 0;
-        while (fem_ld_acquire(s.count) < target) {
+        while (fem_ld_acquire(cnt) < target) {
           if (((++polls) & 63u) == 0u) {
-            if (*(volatile int*)s.err & FEM_ERR_BARRIER_TIMEOUT) { ok = 0; break; }
+            if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) { ok = 0; break; }
             if (fem_globaltimer() - t0 > FEM_BARRIER_TIMEOUT_NS) {
-              atomicOr(s.err, FEM_ERR_BARRIER_TIMEOUT);
+              atomicOr(err, FEM_ERR_BARRIER_TIMEOUT);
               ok = 0;
               break;
             }
           }
         }
       }
-      __threadfence();
-      if (*(volatile int*)s.err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
+      if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
       s_ok = ok;
-      if (s.trace && blockIdx.x == 0) {
-        const unsigned long long n = s.trace[0] + 1;
-        if ((int)n < s.trace_cap) {
-          s.trace[n] = fem_globaltimer();
-          s.trace[0] = n;
+      unsigned long long* tr = s->trace;
+      if (tr && blockIdx.x == 0) {
+        const unsigned long long n = tr[0] + 1;
+        if ((int)n < s->trace_cap) {
+          tr[n] = (fem_globaltimer() & 0x00FFFFFFFFFFFFFFull) | (31ull << 56);
+          tr[0] = n;
         }
       }
     }
@@ -272,8 +309,9 @@ struct BlockTeam {
 
 // Deterministic block-wide sum of K values (fixed shuffle tree + fixed warp order).
 template <int K>
-__device__ __forceinline__ void fem_block_sum(double (&v)[K], double* smem /* >= 32*K */) {
+__device__ __forceinline__ void fem_block_sum(double (&v)[K], double* smem /* >= 16*K (32*K above 512 threads) */) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const int S = nw > 16 ? 32 : 16;
 #pragma unroll
   for (int q = 0; q < K; ++q)
 #pragma unroll
@@ -281,11 +319,11 @@ __device__ __forceinline__ void fem_block_sum(double (&v)[K], double* smem /* >=
   __syncthreads();
   if (lane == 0)
 #pragma unroll
-    for (int q = 0; q < K; ++q) smem[q * 32 + warp] = v[q];
+    for (int q = 0; q < K; ++q) smem[q * S + warp] = v[q];
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < K; ++q) {
-    double t = (lane < nw) ? smem[q * 32 + lane] : 0.0;
+    double t = (lane < nw) ? smem[q * S + lane] : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     v[q] = t;
@@ -295,48 +333,67 @@ __device__ __forceinline__ void fem_block_sum(double (&v)[K], double* smem /* >=
 // Reduction handles. reduce() is called by every thread of the team inside a
 // phase; totals are read by result() after the team's next sync().
 struct GridReducer {
-  FemSync s;
+  const FemSync* s;
   template <int K>
   __device__ __forceinline__ void reduce(double (&v)[K], int slot, double* smem) const {
     fem_block_sum<K>(v, smem);
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
+      double* part = s->partials;
 #pragma unroll
-      for (int q = 0; q < K; ++q) s.partials[(size_t)(slot + q) * gridDim.x + blockIdx.x] = v[q];
+      for (int q = 0; q < K; ++q) part[(size_t)(slot + q) * gridDim.x + blockIdx.x] = v[q];
+    }
   }
-  // Totals of K slots (any slot numbers), every partial load in flight at once;
-  // CTA partials are combined in a fixed order (identical in every CTA).
+  // One block sum for K values bound for any K slots.
+  template <int K>
+  __device__ __forceinline__ void reduce_slots(double (&v)[K], const int (&slots)[K], double* smem) const {
+    fem_block_sum<K>(v, smem);
+    if (threadIdx.x == 0) {
+      double* part = s->partials;
+#pragma unroll
+      for (int q = 0; q < K; ++q) part[(size_t)slots[q] * gridDim.x + blockIdx.x] = v[q];
+    }
+  }
+  // Totals of K <= 8 slots (any slot numbers). Thread c loads CTA c's partial of
+  // every slot (all loads of a thread in flight at once), warps combine theirs
+  // by a fixed shuffle tree, and every thread adds the warp sums in warp order:
+  // the same order, hence the same bits, in every CTA. Uses smem[0, 16*K).
   template <int K>
   __device__ __forceinline__ void result_slots(double (&out)[K], const int (&slots)[K], double* smem) const {
+    static_assert(K <= 8, "result_slots: at most 8 slots");
+    const int G = gridDim.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int nwd = (G + 31) >> 5;
+    if (nwd > 16) nwd = 16;
+    if (nwd > (int)(blockDim.x >> 5)) nwd = blockDim.x >> 5;
+    const double* __restrict__ part = s->partials;
     __syncthreads();
-    if (threadIdx.x < 32) {
-      const int G = gridDim.x;
+    if (warp < nwd) {
       double acc[K];
 #pragma unroll
       for (int q = 0; q < K; ++q) acc[q] = 0.0;
-      for (int base = 0; base < G; base += 256) {
-        double v[K][8];
+      for (int c = threadIdx.x; c < G; c += nwd * 32) {
+        double v[K];
 #pragma unroll
-        for (int q = 0; q < K; ++q)
+        for (int q = 0; q < K; ++q) v[q] = __ldcg(&part[(size_t)slots[q] * G + c]);
 #pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int c = base + threadIdx.x + 32 * k;
-            v[q][k] = (c < G) ? __ldcg(&s.partials[(size_t)slots[q] * G + c]) : 0.0;
-          }
-#pragma unroll
-        for (int q = 0; q < K; ++q)
-          acc[q] += ((v[q][0] + v[q][1]) + (v[q][2] + v[q][3])) + ((v[q][4] + v[q][5]) + (v[q][6] + v[q][7]));
+        for (int q = 0; q < K; ++q) acc[q] += v[q];
       }
 #pragma unroll
       for (int q = 0; q < K; ++q) {
-        double t = acc[q];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (threadIdx.x == 0) smem[q] = t;
+        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
       }
+      if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < K; ++q) smem[q * 16 + warp] = acc[q];
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < K; ++q) out[q] = smem[q];
+    for (int q = 0; q < K; ++q) {
+      double t = 0.0;
+      for (int w = 0; w < nwd; ++w) t += smem[q * 16 + w];
+      out[q] = t;
+    }
     __syncthreads();
   }
   template <int K>
@@ -356,6 +413,13 @@ struct BlockReducer {
     if (threadIdx.x == 0)
 #pragma unroll
       for (int q = 0; q < K; ++q) store[slot + q] = v[q];
+  }
+  template <int K>
+  __device__ __forceinline__ void reduce_slots(double (&v)[K], const int (&slots)[K], double* smem) const {
+    fem_block_sum<K>(v, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < K; ++q) store[slots[q]] = v[q];
   }
   template <int K>
   __device__ __forceinline__ void result_slots(double (&out)[K], const int (&slots)[K], double*) const {

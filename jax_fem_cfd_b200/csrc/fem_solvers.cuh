@@ -91,6 +91,42 @@ __device__ __forceinline__ void fem_stage_args(const T& src, T* dst) {
   __syncthreads();
 }
 
+// Stencil tables of the solver levels in shared memory (FEM_TAB_SMEM doubles
+// after the tile buffer): copied once per launch, in level order while they
+// fit, and the shared argument copy is pointed at them. Tables that do not fit
+// stay in global memory; every reader uses plain loads, so both work.
+#define FEM_TAB_SMEM 2048
+template <int KIND>
+__device__ void fem_tables_to_smem(CgArgs& sA, double* stab) {
+  constexpr int NOFF = KI<KIND>::NOFF;
+  int off = 0;
+  for (int l = 0; l < sA.nlev; ++l) {
+    const MgLevel& L = sA.lv[l];
+    if (!L.tab || !L.tab_off) break;
+    const int m = fem_stencil_ncls(L.g) * NOFF;
+    if (off + 2 * m > FEM_TAB_SMEM) break;
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+      stab[off + q] = L.tab[q];
+      stab[off + m + q] = L.tab_off[q];
+    }
+    off += 2 * m;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    off = 0;
+    for (int l = 0; l < sA.nlev; ++l) {
+      MgLevel& L = sA.lv[l];
+      if (!L.tab || !L.tab_off) break;
+      const int m = fem_stencil_ncls(L.g) * NOFF;
+      if (off + 2 * m > FEM_TAB_SMEM) break;
+      L.tab = stab + off;
+      L.tab_off = stab + off + m;
+      off += 2 * m;
+    }
+  }
+  __syncthreads();
+}
+
 // lattice coordinates of a node
 __device__ __forceinline__ void fem_ij(const FemGrid& g, int n, int& i, int& j, int& k) {
   if (g.kind == FEM_HEX8) {
@@ -118,6 +154,12 @@ __device__ __forceinline__ void fem_ij(const FemGrid& g, int n, int& i, int& j, 
 struct LevelAffine {
   double alpha, beta, sum_rhD;
 };
+// Per-CTA cache of each level's (alpha, beta), written by the down-sweep and
+// read back by the up-sweep of the same level (same slots, same formula).
+__device__ __forceinline__ double* fem_affine_cache() {
+  __shared__ double c[2 * FEM_MAX_LEVELS];
+  return c;
+}
 template <class Red>
 __device__ __forceinline__ LevelAffine fem_level_affine(const Red& red, const CgArgs& A, int m, double* smem) {
   const MgLevel& L = A.lv[m];
@@ -142,13 +184,15 @@ __device__ __forceinline__ LevelAffine fem_level_affine(const Red& red, const Cg
 // Down-sweep step n -> n+1 in one phase: pre-smooth from zero
 // (xh = (2/3) rh / D, 0 on gamma_p or minus its mean), fine residual
 // t = rh - L xh, restriction u_{n+1} = R t. Tiled over the coarse unique lattice
-// (16 x blockDim/64 coarse nodes per tile): xh is staged for the tile's fine
-// region plus the stencil halo, t is formed in smem on that region plus one node,
-// and the tile's coarse nodes are restricted from smem. Each CTA writes x_n and
-// sums t only on the fine nodes its tile owns.
+// (16 coarse columns x CTY rows, CTY chosen for one round of tiles): u and 1/D
+// of the tile's fine region plus the stencil halo, and 1/D of its coarse nodes,
+// are staged in one batch; xh, t (on the region plus one node) and the
+// restriction are then formed from smem only. Each CTA writes x_n and sums t
+// only on the fine nodes its tile owns.
 template <int KIND, class Team, class Red>
 __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArgs& A, int n, double* smem) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  fem_trace_mark(A.sync, 15);
   const MgLevel& L = A.lv[n];
   const MgLevel& C = A.lv[n + 1];
   const FemGrid& g = L.g;
@@ -159,101 +203,111 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
   if (!pinned) {
     f = fem_level_affine(red, A, n, smem);
     mx = (2.0 / 3.0) * f.sum_rhD / nn;
+    if (threadIdx.x == 0) {
+      fem_affine_cache()[2 * n] = f.alpha;
+      fem_affine_cache()[2 * n + 1] = f.beta;
+    }
   }
   fem_trace_mark(A.sync, 1);
-  const double* __restrict__ u = L.r;
-  const double* __restrict__ iD = pinned ? L.winvD : L.invD;
-  const uint8_t* __restrict__ pin = L.pin;
+  const double* u = L.r;
+  const double* iDv = pinned ? L.winvD : L.invD;
+  const double* tab = L.tab;
   const int ux = g.nnx, uy = g.nny;
-  auto rhf = [&](int j) -> double {
-    if (pinned || n == 0) return u[j] - f.beta;
-    const int r = j / ux, c = j - r * ux;
-    return u[j] - f.alpha * fem_restrict_rowsum(L.lat, r, c) - f.beta;
-  };
-  auto xs = [&](int j) -> double { return pinned ? (2.0 / 3.0) * u[j] * iD[j] : (2.0 / 3.0) * rhf(j) * iD[j] - mx; };
   const int nc = fem_axis_ncls(KIND, g.periodic);
   const int cux = C.lat.ux(), cuy = C.lat.uy();
-  // 16 coarse columns per tile; rows chosen so one round of tiles covers the
-  // level (<= one tile per CTA) within the smem staging buffer
-  const int CTX = 16;
-  const int ntx = (cux + CTX - 1) / CTX;
+  const int CTX = 16, ntx = (cux + CTX - 1) / CTX;
+  const int FW = 2 * CTX + 1, SW = FW + 2 * R;
+  // smem per tile: u and xh on SW x SH, t on FW x FH, coarse 1/D on CTX x CTY,
+  // gamma_p flags (bytes) on SW x SH
+  auto need = [&](int cty) {
+    const int fh = 2 * cty + 1, sh = fh + 2 * R;
+    return 2 * SW * sh + FW * fh + CTX * cty + (SW * sh + 7) / 8 + 1;
+  };
   int CTY;
   {
     int nty_t = tm.ncta() / ntx;
     if (nty_t < 1) nty_t = 1;
     CTY = (cuy + nty_t - 1) / nty_t;
-  }
-  {
-    const int cap = (FEM_TILE_SMEM - (2 * CTX + 1 + 2 * R) * (1 + 2 * R) - (2 * CTX + 1)) /
-                    (2 * (2 * CTX + 1 + 2 * R) + 2 * (2 * CTX + 1));
-    if (CTY > cap) CTY = cap;
-    if (CTY < 1) CTY = 1;
     if (CTY > cuy) CTY = cuy;
+    while (CTY > 1 && need(CTY) > FEM_TILE_SMEM) --CTY;
   }
-  const int FW = 2 * CTX + 1, FH = 2 * CTY + 1;  // fine region of t
-  const int SW = FW + 2 * R, SH = FH + 2 * R;    // staged xh
-  double* __restrict__ sx = smem + 128;
-  double* __restrict__ st = sx + SW * SH;
+  const int FH = 2 * CTY + 1, SH = FH + 2 * R, NS = SW * SH;
+  double* su = smem + 128;
+  double* sx = su + NS;
+  double* st = sx + NS;
+  double* sci = st + FW * FH;
+  unsigned char* spin = reinterpret_cast<unsigned char*>(sci + CTX * CTY);
   const int nty = (cuy + CTY - 1) / CTY, ntile = ntx * nty;
-  double acc_t[1] = {0.0}, acc_u[2] = {0.0, 0.0};
+  double acc[3] = {0.0, 0.0, 0.0};  // sum t (owned fine nodes), sum u_{n+1}, sum u_{n+1} / D_{n+1}
   for (int tl = tm.cta(); tl < ntile; tl += tm.ncta()) {
     const int by = tl / ntx, bx = tl - by * ntx;
     const int C0 = bx * CTX, R0 = by * CTY;
     const int fx0 = 2 * C0 - 1, fy0 = 2 * R0 - 1;  // fine coordinates of the t-region origin
-    // all staged loads of a batch in flight before the first smem store
-    constexpr int NB = 8;
-    for (int q0 = 0; q0 < SW * SH; q0 += NB * (int)blockDim.x) {
-      double v[NB];
-#pragma unroll
-      for (int k = 0; k < NB; ++k) {
-        const int q = q0 + k * blockDim.x + threadIdx.x;
-        if (q < SW * SH) {
-          const int ly = q / SW, lx = q - ly * SW;
-          int gx = fx0 - R + lx, gy = fy0 - R + ly;
-          if (g.periodic) {
-            gx = gx < 0 ? gx + ux : (gx >= ux ? gx - ux : gx);
-            gy = gy < 0 ? gy + uy : (gy >= uy ? gy - uy : gy);
-          } else {
-            gx = gx < 0 ? 0 : (gx >= ux ? ux - 1 : gx);
-            gy = gy < 0 ? 0 : (gy >= uy ? uy - 1 : gy);
-          }
-          v[k] = xs(gy * ux + gx);
+    auto fidx = [&](int q) -> int {
+      const int ly = q / SW, lx = q - ly * SW;
+      int gx = fx0 - R + lx, gy = fy0 - R + ly;
+      if (g.periodic) {
+        gx = fem_wrap(gx, ux);
+        gy = fem_wrap(gy, uy);
+      } else {
+        gx = gx < 0 ? 0 : (gx >= ux ? ux - 1 : gx);
+        gy = gy < 0 ? 0 : (gy >= uy ? uy - 1 : gy);
+      }
+      return gy * ux + gx;
+    };
+    fem_stage(su, u, NS, fidx);
+    fem_stage(sx, iDv, NS, fidx);
+    fem_stage(sci, C.invD, CTX * CTY, [&](int q) -> int {
+      const int ky = q / CTX, kx = q - ky * CTX;
+      const int Rr = min(R0 + ky, cuy - 1), Cc = min(C0 + kx, cux - 1);
+      return Rr * cux + Cc;
+    });
+    fem_stage_wait();
+    fem_trace_mark(A.sync, 2);
+    // xh on the staged region (pinned: winvD is 0 on gamma_p, which also marks it)
+    for (int q = threadIdx.x; q < NS; q += blockDim.x) {
+      const double d = sx[q];
+      double v;
+      if (pinned) {
+        spin[q] = (d == 0.0);
+        v = (2.0 / 3.0) * su[q] * d;
+      } else {
+        double rh = su[q] - f.beta;
+        if (n > 0) {
+          const int j = fidx(q), r = j / ux, c = j - r * ux;
+          rh = su[q] - f.alpha * fem_restrict_rowsum(L.lat, r, c) - f.beta;
         }
+        v = (2.0 / 3.0) * rh * d - mx;
       }
-#pragma unroll
-      for (int k = 0; k < NB; ++k) {
-        const int q = q0 + k * blockDim.x + threadIdx.x;
-        if (q < SW * SH) sx[q] = v[k];
-      }
+      sx[q] = v;
     }
     __syncthreads();
-    fem_trace_mark(A.sync, 2);
     for (int q = threadIdx.x; q < FW * FH; q += blockDim.x) {
       const int py = q / FW, px = q - py * FW;
       const int x = fx0 + px, y = fy0 + py;
       double tv = 0.0;
       if (x >= 0 && x < ux && y >= 0 && y < uy) {
         const int cx = fem_axis_cls(KIND, g.periodic, x, g.nex), cy = fem_axis_cls(KIND, g.periodic, y, g.ney);
-        const double* __restrict__ cf = L.tab + (size_t)(cy * nc + cx) * NOFF;
+        const double* cf = tab + (size_t)(cy * nc + cx) * NOFF;
         double Lx = 0.0;
 #pragma unroll
         for (int dy = 0; dy < W; ++dy)
 #pragma unroll
-          for (int dx = 0; dx < W; ++dx) Lx += __ldg(cf + dy * W + dx) * sx[(py + dy) * SW + px + dx];
-        const int j = y * ux + x;
+          for (int dx = 0; dx < W; ++dx) Lx += cf[dy * W + dx] * sx[(py + dy) * SW + px + dx];
+        const int qc = (py + R) * SW + px + R;
         double rz;
         if (pinned) {
-          const bool p = pin && pin[j];
-          rz = p ? 0.0 : u[j];
+          const bool p = spin[qc] != 0;
+          rz = p ? 0.0 : su[qc];
           if (p) Lx = 0.0;
         } else {
-          rz = rhf(j);
+          rz = (n == 0) ? su[qc] - f.beta : su[qc] - f.alpha * fem_restrict_rowsum(L.lat, y, x) - f.beta;
         }
         tv = rz - Lx;
         // fine nodes owned by this tile: [2 C0, 2 C0 + 2 CTX) x [2 R0, 2 R0 + 2 CTY)
         if (px >= 1 && px <= 2 * CTX && py >= 1 && py <= 2 * CTY) {
-          L.x[j] = sx[(py + R) * SW + px + R];
-          acc_t[0] += tv;
+          L.x[y * ux + x] = sx[qc];
+          acc[0] += tv;
         }
       }
       st[q] = tv;
@@ -278,18 +332,17 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
         if (dn && rt) d += st[(cy0 - 1) * FW + cx0 + 1];
         if (dn && lf) d += st[(cy0 - 1) * FW + cx0 - 1];
         const double v = st[cy0 * FW + cx0] + 0.5 * e + 0.25 * d;
-        const int I = Rr * cux + Cc;
-        C.r[I] = v;
-        acc_u[0] += v;
-        acc_u[1] += v * C.invD[I];
+        C.r[Rr * cux + Cc] = v;
+        acc[1] += v;
+        acc[2] += v * sci[kk];
       }
     }
     __syncthreads();
   }
   fem_trace_mark(A.sync, 4);
   if (!pinned) {
-    red.template reduce<1>(acc_t, SL_T(n), smem);
-    red.template reduce<2>(acc_u, SL_R(n + 1), smem);
+    const int sl[3] = {SL_T(n), SL_R(n + 1), SL_R(n + 1) + 1};
+    red.template reduce_slots<3>(acc, sl, smem);
   }
   fem_trace_mark(A.sync, 5);
   return tm.sync();
@@ -337,8 +390,9 @@ __device__ __noinline__ void mg_coarse(const Red& red, const CgArgs& A, double* 
   __syncthreads();
   while (gamma > atol2 && k < A.coarse_maxiter) {
     double pq[1] = {0.0};
-    fem_tiled_stencil<KIND>(tm, g, L.tab, smem + 128, [&](int j) { return cg_p[j]; },
-                            [&](int i, int, int, int, double q, double pi) {
+    const double* srcp[1] = {cg_p};
+    fem_tiled_stencil<KIND, 1>(tm, g, L.tab, smem + 128, srcp, [](int, const double(&v)[1]) { return v[0]; },
+                               [&](int i, int, int, int, double q, double pi) {
                               if (pin && pin[i]) q = 0.0;
                               cg_q[i] = q;
                               pq[0] += pi * q;
@@ -371,12 +425,17 @@ __device__ __forceinline__ void mg_xsums(const MgLevel& L, int i, double xi, dou
   a[1] += fem_interp_colsum(L.lat, i / ux, i % ux) * xi;
 }
 
-// Up-sweep at level n: prolongate X_{n+1}, add to X_n, one weighted Jacobi sweep.
-// The prolongated iterate y = X_n + P X_{n+1} (- mean, or 0 on gamma_p) is
-// evaluated while staging the Jacobi stencil's tile, so the sweep is a single
-// phase. For n == 0 the result is z = M r; the phase also accumulates r.z pieces.
+// Up-sweep at level n: prolongate X_{n+1}, add to X_n, one weighted Jacobi sweep,
+// in one phase per 32 x TY tile. Staged in one batch: X_n on the tile plus the
+// stencil halo (and ω/D there in pinned mode, whose zeros mark gamma_p), the
+// coarse X_{n+1} under that region, and rhs and diag of the tile's own nodes.
+// The prolongated iterate y = X_n + P X_{n+1} (- means, or 0 on gamma_p) is
+// formed in smem; the sweep then reads smem only. For n == 0 the result is
+// z = M r and the phase also accumulates the r.z pieces.
 template <int KIND, class Team, class Red>
 __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs& A, int n, double* smem) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  fem_trace_mark(A.sync, 14);
   const MgLevel& L = A.lv[n];
   const MgLevel& C = A.lv[n + 1];
   const FemGrid& g = L.g;
@@ -385,52 +444,143 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
   double mX = 0.0, mP = 0.0;
   LevelAffine f{0.0, 0.0, 0.0};
   if (!pinned) {
+    double v[2];
+    red.template result<2>(v, SL_X(n + 1), smem);  // its __syncthreads also publishes the cache
+    mX = v[0] / C.g.nn;
+    mP = (v[1] - mX * C.sum_colw) / nn;
     if (n > 0) {
-      double v[5];
-      const int sl[5] = {SL_X(n + 1), SL_X(n + 1) + 1, SL_R(n), SL_R(n) + 1, SL_T(n - 1)};
-      red.template result_slots<5>(v, sl, smem);
-      mX = v[0] / C.g.nn;
-      mP = (v[1] - mX * C.sum_colw) / nn;
-      f.alpha = v[4] / A.lv[n - 1].g.nn;
-      f.beta = (v[2] - f.alpha * L.sum_rc) / nn;
-    } else {
-      double v[2];
-      red.template result<2>(v, SL_X(n + 1), smem);
-      mX = v[0] / C.g.nn;
-      mP = (v[1] - mX * C.sum_colw) / nn;
+      f.alpha = fem_affine_cache()[2 * n];
+      f.beta = fem_affine_cache()[2 * n + 1];
     }
   }
-  const double* __restrict__ Xc = C.t;  // corrected coarse iterate (after its own up-sweep / coarse solve)
-  const double* __restrict__ Xf = L.x;  // pre-smoothed iterate of the down-sweep
-  const uint8_t* __restrict__ pin = L.pin;
-  const int ux = g.nnx;
-  auto yfun = [&](int j) -> double {
-    if (pinned && pin && pin[j]) return 0.0;
-    const int r = j / ux, c = j - r * ux;
-    const double xH = fem_interp_at(C.lat, r, c, [&](int I) { return pinned ? Xc[I] : Xc[I] - mX; });
-    return Xf[j] + (pinned ? xH : xH - mP);
-  };
-  // Jacobi: x = w (rh - Loff y)/D + (1-w) y
-  const double* __restrict__ rh = L.r;
+  fem_trace_mark(A.sync, 11);
+  const int ux = g.nnx, uy = g.nny, cux = C.lat.ux(), cuy = C.lat.uy();
+  const bool per = g.periodic;
+  const int nc = fem_axis_ncls(KIND, per);
+  const int WR = blockDim.x >> 5, tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
+  const int SX = 32 + 2 * R, CXB = SX / 2 + 3;
+  const int nf = pinned ? 2 : 1;
+  auto need = [&](int ty) { return nf * SX * (ty + 2 * R) + CXB * ((ty + 2 * R) / 2 + 3) + 64 * ty; };
+  const int ntx = (ux + 31) >> 5;
+  int TY;
+  {
+    int nty_t = tm.ncta() / ntx;
+    if (nty_t < 1) nty_t = 1;
+    TY = (uy + nty_t - 1) / nty_t;
+    const int minr = WR < uy ? WR : uy;
+    if (TY < minr) TY = minr;
+    if (TY > uy) TY = uy;
+    while (TY > 1 && need(TY) > FEM_TILE_SMEM) --TY;
+  }
+  const int SY = TY + 2 * R, NS = SX * SY, CYB = SY / 2 + 3;
+  double* sy = smem + 128;
+  double* sw = sy + NS;                     // pinned only
+  double* sc = sy + nf * NS;                // coarse X_{n+1}, CXB x CYB
+  double* sr = sc + CXB * CYB;              // rhs of owned nodes, 32 x TY
+  double* sd = sr + 32 * TY;                // diag of owned nodes
+  const int nty = (uy + TY - 1) / TY, ntile = ntx * nty;
+  const double* tabo = L.tab_off;
   const double w = 2.0 / 3.0;
   double a[2] = {0.0, 0.0};
-  // the staged tile reads Xf at neighbours: all threads of the team must have
-  // read X_n before any writes it, so the new x goes to L.t and is swapped in below
-  fem_tiled_stencil<KIND>(tm, g, L.tab_off, smem + 128, yfun, [&](int i, int, int, int, double off, double yi) {
-    const double rv = (!pinned && n > 0)
-                          ? rh[i] - f.alpha * fem_restrict_rowsum(L.lat, i / ux, i - (i / ux) * ux) - f.beta
-                          : rh[i];
-    double xn = w * (rv - off) / L.diag[i] + (1.0 - w) * yi;
-    if (pinned && pin && pin[i]) xn = 0.0;
-    L.t[i] = xn;
-    if (n == 0) {
-      a[0] += xn;
-      a[1] += rh[i] * xn;
-    } else {
-      mg_xsums(L, i, xn, a);
+  for (int tl = tm.cta(); tl < ntile; tl += tm.ncta()) {
+    const int by = tl / ntx, bx = tl - by * ntx;
+    const int x0 = bx * 32, y0 = by * TY, gx0 = x0 - R, gy0 = y0 - R;
+    const int cr0 = fem_floordiv2(gy0), cc0 = fem_floordiv2(gx0);
+    // fine coordinates of a staged point: unwrapped (periodic) or clamped
+    auto fcoord = [&](int q, int& fr, int& fc) {
+      const int ly = q / SX, lx = q - ly * SX;
+      fr = gy0 + ly;
+      fc = gx0 + lx;
+      if (!per) {
+        fr = fr < 0 ? 0 : (fr >= uy ? uy - 1 : fr);
+        fc = fc < 0 ? 0 : (fc >= ux ? ux - 1 : fc);
+      }
+    };
+    auto fidx = [&](int q) -> int {
+      int fr, fc;
+      fcoord(q, fr, fc);
+      if (per) {
+        fr = fem_wrap(fr, uy);
+        fc = fem_wrap(fc, ux);
+      }
+      return fr * ux + fc;
+    };
+    auto oidx = [&](int q) -> int {  // owned node q = ty * 32 + tx, clamped into the lattice
+      const int ty = q >> 5, x = min(x0 + (q & 31), ux - 1), y = min(y0 + ty, uy - 1);
+      return y * ux + x;
+    };
+    fem_stage(sy, L.x, NS, fidx);
+    if (pinned) fem_stage(sw, L.winvD, NS, fidx);
+    fem_stage(sc, C.t, CXB * CYB, [&](int q) -> int {
+      const int i = q / CXB, j = q - i * CXB;
+      int cr = cr0 + i, cc = cc0 + j;
+      if (per) {
+        cr = fem_wrap(cr, cuy);
+        cc = fem_wrap(cc, cux);
+      } else {
+        cr = cr < 0 ? 0 : (cr >= cuy ? cuy - 1 : cr);
+        cc = cc < 0 ? 0 : (cc >= cux ? cux - 1 : cc);
+      }
+      return cr * cux + cc;
+    });
+    fem_stage(sr, L.r, 32 * TY, oidx);
+    fem_stage(sd, L.diag, 32 * TY, oidx);
+    fem_stage_wait();
+    // y = X_n + P X_{n+1} in place (the arithmetic of fem_interp_at)
+    for (int q = threadIdx.x; q < NS; q += blockDim.x) {
+      int fr, fc;
+      fcoord(q, fr, fc);
+      double y;
+      if (pinned && sw[q] == 0.0) {
+        y = 0.0;
+      } else {
+        const int Rr = fem_floordiv2(fr) - cr0, Cc = fem_floordiv2(fc) - cc0;
+        auto xH = [&](int dr, int dc) -> double {
+          const double v = sc[(Rr + dr) * CXB + Cc + dc];
+          return pinned ? v : v - mX;
+        };
+        double xh;
+        if (!(fr & 1) && !(fc & 1)) xh = xH(0, 0);
+        else if (!(fr & 1)) xh = 0.5 * xH(0, 0) + 0.5 * xH(0, 1);
+        else if (!(fc & 1)) xh = 0.5 * xH(0, 0) + 0.5 * xH(1, 0);
+        else xh = 0.25 * xH(0, 0) + 0.25 * xH(0, 1) + 0.25 * xH(1, 0) + 0.25 * xH(1, 1);
+        y = sy[q] + (pinned ? xh : xh - mP);
+      }
+      sy[q] = y;
     }
-  });
+    __syncthreads();
+    // Jacobi: x = w (rh - Loff y)/D + (1-w) y on the owned nodes
+    for (int ty = ty0; ty < TY; ty += WR) {
+      const int x = x0 + tx, yy = y0 + ty;
+      if (x < ux && yy < uy) {
+        const int cx = fem_axis_cls(KIND, per, x, g.nex), cy = fem_axis_cls(KIND, per, yy, g.ney);
+        const double* cf = tabo + (size_t)(cy * nc + cx) * NOFF;
+        double off = 0.0;
+#pragma unroll
+        for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+          for (int dx = 0; dx < W; ++dx) off += cf[dy * W + dx] * sy[(ty + dy) * SX + tx + dx];
+        const int qc = (ty + R) * SX + tx + R;
+        const double yi = sy[qc];
+        const double rhv = sr[ty * 32 + tx];
+        const double rv = (!pinned && n > 0) ? rhv - f.alpha * fem_restrict_rowsum(L.lat, yy, x) - f.beta : rhv;
+        double xn = w * (rv - off) / sd[ty * 32 + tx] + (1.0 - w) * yi;
+        if (pinned && sw[qc] == 0.0) xn = 0.0;
+        L.t[yy * ux + x] = xn;
+        if (n == 0) {
+          a[0] += xn;
+          a[1] += rhv * xn;
+        } else {
+          a[0] += xn;
+          a[1] += fem_interp_colsum(L.lat, yy, x) * xn;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  fem_trace_mark(A.sync, 12);
   if (n == 0 || !pinned) red.template reduce<2>(a, SL_X(n), smem);
+  fem_trace_mark(A.sync, 13);
   if (!tm.sync()) return false;
   return true;
 }
@@ -461,7 +611,7 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
       }
       __syncthreads();
       if (threadIdx.x == 0) {
-        double* p = dyn + 128 + FEM_TILE_SMEM;
+        double* p = dyn + 128 + FEM_TILE_SMEM + FEM_TAB_SMEM;
         for (int n = s; n < N; ++n) {
           const int m = A.lv[n].g.nn;
           sAb.lv[n].x = p;
@@ -475,7 +625,7 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
       double* __restrict__ rdst = sAb.lv[s].r;
       for (int i = threadIdx.x; i < A.lv[s].g.nn; i += blockDim.x) rdst[i] = rsrc[i];
       const int mc = A.lv[N - 1].g.nn;
-      double* p = dyn + 128 + FEM_TILE_SMEM;
+      double* p = dyn + 128 + FEM_TILE_SMEM + FEM_TAB_SMEM;
       for (int n = s; n < N; ++n) p += 3 * A.lv[n].g.nn;
       cg_r = p;
       cg_p = p + mc;
@@ -494,8 +644,11 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
       }
       __syncthreads();
     }
+    fem_trace_mark(A.sync, 6);
     for (int n = s; n < N - 1; ++n) mg_down<KIND>(bt, br, B, n, smem);
+    fem_trace_mark(A.sync, 7);
     mg_coarse<KIND>(br, B, smem, cg_r, cg_p, cg_q);
+    fem_trace_mark(A.sync, 8);
     const MgLevel& Lc = B.lv[N - 1];
     if (N == 1) {
       // single level: the coarse solve is the whole preconditioner; r.z pieces
@@ -512,7 +665,9 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
       br.reduce<2>(a, SL_X(N - 1), smem);
       __syncthreads();
     }
+    fem_trace_mark(A.sync, 9);
     for (int n = N - 2; n >= s; --n) mg_up<KIND>(bt, br, B, n, smem);
+    fem_trace_mark(A.sync, 10);
     if (in_smem) {
       const double* __restrict__ xs = sAb.lv[s].t;
       double* __restrict__ xd = A.lv[s].t;

@@ -328,13 +328,16 @@ __device__ __forceinline__ double fem_gather_div_k(const FemGrid& g, int i, int 
     }                                                  \
   } while (0)
 
-// Tiled stencil with shared-memory staging. For each 32 x (blockDim/32) tile of
-// the lattice owned by this CTA, the source values of the tile plus an R-wide
-// halo (3 planes in 3D) are produced by load(node) and staged in smem with all
-// loads in flight at once; then every thread applies the assembled stencil of
-// its node from smem and calls body(n, x, y, z, value, center_source).
-// The smem buffer needs (32+2R) * (blockDim/32+2R) * (3 in 3D) doubles.
-#define FEM_TILE_SMEM 6144
+// Tiled stencil with shared-memory staging. For each 32 x TY tile of the
+// lattice owned by this CTA (TY from fem_tile_rows), the NSRC source vectors
+// over the tile plus an R-wide halo (3 planes in 3D) are staged into smem in
+// one batch (fem_stage), combined in place into the stencil's input
+// v = comb(q, s_0[q], .., s_{NSRC-1}[q]) (q = staged index), and every thread
+// applies the assembled stencil of its nodes from smem and calls
+// body(n, x, y, z, value, v_center). The tables `tab` may live in shared or
+// global memory (plain loads). Needs NSRC * (32+2R) * (TY+2R) * (3 in 3D)
+// doubles of smem at sm.
+#define FEM_TILE_SMEM 8192
 
 // Tile height (lattice rows) so that one round of tiles covers the level with
 // at most ncta tiles (one tile per CTA), capped by the smem staging buffer.
@@ -352,13 +355,14 @@ __device__ __forceinline__ int fem_tile_rows(int nx, int ny, int nplanes, int ha
   return th;
 }
 
-template <int KIND, class Team, class Load, class Body>
-__device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid& g, const double* __restrict__ tab,
-                                                  double* __restrict__ sm, const Load& load, const Body& body) {
+template <int KIND, int NSRC, class Team, class Comb, class Body>
+__device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid& g, const double* tab,
+                                                  double* __restrict__ sm, const double* const (&src)[NSRC],
+                                                  const Comb& comb, const Body& body) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
   constexpr bool D3 = (KIND == FEM_HEX8);
   const int WR = blockDim.x >> 5;  // warps = rows per pass
-  const int TY = fem_tile_rows(g.nnx, g.nny, g.nnz, R, tm.ncta(), FEM_TILE_SMEM, D3 ? 3 : 1);
+  const int TY = fem_tile_rows(g.nnx, g.nny, g.nnz, R, tm.ncta(), FEM_TILE_SMEM, (D3 ? 3 : 1) * NSRC);
   const int SX = 32 + 2 * R, SY = TY + 2 * R, SXY = SX * SY, NS = SXY * (D3 ? 3 : 1);
   const int ntx = (g.nnx + 31) >> 5, nty = (g.nny + TY - 1) / TY, nt2 = ntx * nty, ntile = nt2 * g.nnz;
   const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
@@ -366,32 +370,27 @@ __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid&
   for (int t = tm.cta(); t < ntile; t += tm.ncta()) {
     const int z = t / nt2, rr = t - z * nt2, by = rr / ntx, bx = rr - by * ntx;
     const int x0 = bx * 32 - R, y0 = by * TY - R;
-    // all staged loads of a batch in flight before the first smem store
-    constexpr int NB = 8;
-    for (int q0 = 0; q0 < NS; q0 += NB * (int)blockDim.x) {
-      double v[NB];
-#pragma unroll
-      for (int k = 0; k < NB; ++k) {
-        const int s = q0 + k * blockDim.x + threadIdx.x;
-        if (s < NS) {
-          const int lz = D3 ? s / SXY : 0, r2 = s - lz * SXY, ly = r2 / SX, lx = r2 - ly * SX;
-          int gx = x0 + lx, gy = y0 + ly, gz = D3 ? z + lz - 1 : 0;
-          if (g.periodic) {
-            gx = gx < 0 ? gx + g.nnx : (gx >= g.nnx ? gx - g.nnx : gx);
-            gy = gy < 0 ? gy + g.nny : (gy >= g.nny ? gy - g.nny : gy);
-          } else {
-            gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
-            gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);
-          }
-          if (D3) gz = gz < 0 ? 0 : (gz >= g.nnz ? g.nnz - 1 : gz);
-          v[k] = load((gz * g.nny + gy) * g.nnx + gx);
-        }
+    auto gidx = [&](int s) -> int {
+      const int lz = D3 ? s / SXY : 0, r2 = s - lz * SXY, ly = r2 / SX, lx = r2 - ly * SX;
+      int gx = x0 + lx, gy = y0 + ly, gz = D3 ? z + lz - 1 : 0;
+      if (g.periodic) {
+        gx = fem_wrap(gx, g.nnx);
+        gy = fem_wrap(gy, g.nny);
+      } else {
+        gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
+        gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);
       }
+      if (D3) gz = gz < 0 ? 0 : (gz >= g.nnz ? g.nnz - 1 : gz);
+      return (gz * g.nny + gy) * g.nnx + gx;
+    };
 #pragma unroll
-      for (int k = 0; k < NB; ++k) {
-        const int s = q0 + k * blockDim.x + threadIdx.x;
-        if (s < NS) sm[s] = v[k];
-      }
+    for (int k = 0; k < NSRC; ++k) fem_stage(sm + k * NS, src[k], NS, gidx);
+    fem_stage_wait();
+    for (int s = threadIdx.x; s < NS; s += blockDim.x) {
+      double v[NSRC];
+#pragma unroll
+      for (int k = 0; k < NSRC; ++k) v[k] = sm[k * NS + s];
+      sm[s] = comb(s, v);
     }
     __syncthreads();
     for (int ty = ty0; ty < TY; ty += WR) {
@@ -399,7 +398,7 @@ __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid&
       if (x < g.nnx && y < g.nny) {
         const int cx = fem_axis_cls(KIND, g.periodic, x, g.nex), cy = fem_axis_cls(KIND, g.periodic, y, g.ney);
         const int cz = D3 ? fem_axis_cls(KIND, 0, z, g.nez) : 0;
-        const double* __restrict__ c = tab + (size_t)((cz * nc + cy) * nc + cx) * NOFF;
+        const double* c = tab + (size_t)((cz * nc + cy) * nc + cx) * NOFF;
         double acc = 0.0;
 #pragma unroll
         for (int dz = 0; dz < (D3 ? W : 1); ++dz)
@@ -407,7 +406,7 @@ __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid&
           for (int dy = 0; dy < W; ++dy)
 #pragma unroll
             for (int dx = 0; dx < W; ++dx)
-              acc += __ldg(c + (dz * W + dy) * W + dx) * sm[dz * SXY + (ty + dy) * SX + tx + dx];
+              acc += c[(dz * W + dy) * W + dx] * sm[dz * SXY + (ty + dy) * SX + tx + dx];
         const int n = (z * g.nny + y) * g.nnx + x;
         body(n, x, y, z, acc, sm[(D3 ? SXY : 0) + (ty + R) * SX + tx + R]);
       }
@@ -437,8 +436,8 @@ __device__ __forceinline__ void fem_tiled_ebe(const Team& tm, const FemGrid& g, 
       const int lz = D3 ? s / SXY : 0, r2 = s - lz * SXY, ly = r2 / SX, lx = r2 - ly * SX;
       int gx = x0 + lx, gy = y0 + ly, gz = D3 ? z + lz - 1 : 0;
       if (g.periodic) {
-        gx = gx < 0 ? gx + g.nnx : (gx >= g.nnx ? gx - g.nnx : gx);
-        gy = gy < 0 ? gy + g.nny : (gy >= g.nny ? gy - g.nny : gy);
+        gx = fem_wrap(gx, g.nnx);
+        gy = fem_wrap(gy, g.nny);
       } else {
         gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
         gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);

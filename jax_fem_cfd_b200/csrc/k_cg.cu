@@ -20,15 +20,16 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
   }
   if (A.prec == FEM_PREC_MG) {
     if (!mg_vcycle<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return false;
-    double s[2];
-    gr.result<2>(s, SL_X(0), smem);
     if (A.pinned) {
+      double s[2];
+      gr.result<2>(s, SL_X(0), smem);
       gamma = s[1];
     } else {
-      double rs[2];
-      gr.result<2>(rs, SL_R(0), smem);
+      double s[3];
+      const int sl[3] = {SL_X(0), SL_X(0) + 1, SL_R(0)};
+      gr.result_slots<3>(s, sl, smem);
       mz = s[0] / nn;
-      gamma = s[1] - mz * rs[0];
+      gamma = s[1] - mz * s[2];
     }
     return true;
   }
@@ -39,16 +40,19 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
   const uint8_t* __restrict__ ap = A.ai_pin;
   double* __restrict__ T = L0.t;
   const double* __restrict__ iD = L0.invD;
-  fem_tiled_stencil<KIND>(gt, L0.g, L0.tab, smem + 128, [&](int j) { return r[j] * iD[j]; },
-                          [&](int i, int, int, int, double v, double) {
+  const double* src1[2] = {r, iD};
+  fem_tiled_stencil<KIND, 2>(gt, L0.g, L0.tab, smem + 128, src1,
+                             [](int, const double(&v)[2]) { return v[0] * v[1]; },
+                             [&](int i, int, int, int, double v, double) {
                             double d1l = v / D[i];
                             if (ap && ap[i]) d1l = pt ? r[i] / D[i] : 0.0;
                             T[i] = d1l;
                           });
   if (!gt.sync()) return false;
   double acc[1] = {0.0};
-  fem_tiled_stencil<KIND>(gt, L0.g, L0.tab, smem + 128, [&](int j) { return T[j]; }, [&](int i, int, int, int,
-                                                                                         double t, double) {
+  const double* src2[1] = {T};
+  fem_tiled_stencil<KIND, 1>(gt, L0.g, L0.tab, smem + 128, src2, [](int, const double(&v)[1]) { return v[0]; },
+                             [&](int i, int, int, int, double t, double) {
     if (ap && ap[i]) t = pt ? T[i] : 0.0;
     const double zi = 3 * (r[i] / D[i]) - 3 * T[i] + t / D[i];
     A.z[i] = zi;
@@ -64,15 +68,17 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
 
 template <int KIND>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q) {
-  extern __shared__ double smem[];  // [0,128) reductions, [128, 128+FEM_TILE_SMEM) tiles, then CTA-0 levels
+  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables, then CTA-0 levels
+  extern __shared__ double smem[];
   __shared__ double bstore[FEM_NSLOTS];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
+  fem_tables_to_smem<KIND>(sA, smem + 128 + FEM_TILE_SMEM);
   const CgArgs& A = sA;
   __shared__ unsigned int s_round;
   if (threadIdx.x == 0) s_round = 0u;
-  const GridTeam gt{A.sync, &s_round};
-  const GridReducer gr{A.sync};
+  const GridTeam gt{&A.sync, &s_round};
+  const GridReducer gr{&A.sync};
   const MgLevel& L0 = A.lv[0];
   const FemGrid& g = L0.g;
   const int nn = g.nn;
@@ -98,8 +104,9 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
     // r0 = b - A x0
     {
       double a2[2] = {0.0, 0.0}, a3[2] = {0.0, 0.0}, a1[1] = {0.0};
-      fem_tiled_stencil<KIND>(gt, g, L0.tab, smem + 128, [&](int j) { return A.x[j]; }, [&](int i, int, int, int,
-                                                                                             double Ax, double) {
+      const double* srcx[1] = {A.x};
+      fem_tiled_stencil<KIND, 1>(gt, g, L0.tab, smem + 128, srcx, [](int, const double(&v)[1]) { return v[0]; },
+                                 [&](int i, int, int, int, double Ax, double) {
         if (pin0 && pin0[i]) Ax = 0.0;
         const double bi = b[i], ri = bi - Ax;
         A.r[i] = ri;
@@ -133,21 +140,25 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
       const int prec = A.prec;
       const double* __restrict__ r = A.r;
       const double* __restrict__ zs = (prec == FEM_PREC_MG) ? L0.t : A.z;
-      auto zval = [&](int j) -> double {
-        if (prec == FEM_PREC_NONE) return r[j];
-        if (prec == FEM_PREC_JACOBI) return r[j] / D[j];
-        if (prec == FEM_PREC_MG) return zs[j] - mz;
-        return zs[j];
-      };
-      auto pz = [&](int j) -> double { return have_p ? zval(j) + beta * pold[j] : zval(j); };
       {
+        // p = z + beta p_old staged and combined in smem; Ap on the owned nodes
+        const double* srcA[3] = {(prec == FEM_PREC_NONE || prec == FEM_PREC_JACOBI) ? r : zs,
+                                 have_p ? pold : nullptr, prec == FEM_PREC_JACOBI ? D : nullptr};
+        auto comb = [&](int, const double(&v)[3]) -> double {
+          double zv;
+          if (prec == FEM_PREC_JACOBI) zv = v[0] / v[2];
+          else if (prec == FEM_PREC_MG) zv = v[0] - mz;
+          else zv = v[0];
+          return have_p ? zv + beta * v[1] : zv;
+        };
         double a[1] = {0.0};
-        fem_tiled_stencil<KIND>(gt, g, L0.tab, smem + 128, pz, [&](int i, int, int, int, double q, double pn) {
-          pnew[i] = pn;
-          if (pin0 && pin0[i]) q = 0.0;
-          A.Ap[i] = q;
-          a[0] += pn * q;
-        });
+        fem_tiled_stencil<KIND, 3>(gt, g, L0.tab, smem + 128, srcA, comb,
+                                   [&](int i, int, int, int, double q, double pn) {
+                                     pnew[i] = pn;
+                                     if (pin0 && pin0[i]) q = 0.0;
+                                     A.Ap[i] = q;
+                                     a[0] += pn * q;
+                                   });
         gr.reduce<1>(a, SL_PAP, smem);
         if (!gt.sync()) goto done;
       }
@@ -155,27 +166,50 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
       gr.result<1>(pap, SL_PAP, smem);
       const double alpha = gamma / pap[0];
       {
-        double a2[2] = {0.0, 0.0}, a3[2] = {0.0, 0.0}, a1[1] = {0.0};
-        for (int i = gt.rank(); i < nn; i += gt.size()) {
-          A.x[i] = A.x[i] + alpha * pnew[i];
-          const double ri = A.r[i] - alpha * A.Ap[i];
-          A.r[i] = ri;
-          a2[1] += ri * ri;
-          a3[0] += ri;
-          a3[1] += ri * L0.invD[i];
-          a1[0] += ri * ri / D[i];
+        // x += alpha p, r -= alpha Ap; loads of a batch of nodes first
+        double a4[4] = {0.0, 0.0, 0.0, 0.0};  // r.r, sum r, sum r / D (via 1/D), sum r^2 / D
+        constexpr int U = 2;
+        const int stride = gt.size();
+        const double* __restrict__ iD0 = L0.invD;
+        for (int i0 = gt.rank(); i0 < nn; i0 += U * stride) {
+          double xv[U], pv[U], rv[U], av[U], iv[U], dv[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * stride;
+            if (i < nn) {
+              xv[u] = A.x[i];
+              pv[u] = pnew[i];
+              rv[u] = A.r[i];
+              av[u] = A.Ap[i];
+              iv[u] = iD0[i];
+              dv[u] = D[i];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * stride;
+            if (i < nn) {
+              A.x[i] = xv[u] + alpha * pv[u];
+              const double ri = rv[u] - alpha * av[u];
+              A.r[i] = ri;
+              a4[0] += ri * ri;
+              a4[1] += ri;
+              a4[2] += ri * iv[u];
+              a4[3] += ri * ri / dv[u];
+            }
+          }
         }
-        gr.reduce<2>(a2, SL_BB, smem);
-        gr.reduce<2>(a3, SL_R(0), smem);
-        gr.reduce<1>(a1, SL_RZ, smem);
+        const int sl4[4] = {SL_RR, SL_R(0), SL_R(0) + 1, SL_RZ};
+        gr.reduce_slots<4>(a4, sl4, smem);
         fem_watchdog_arm(A.sync.err, t_start);
         if (!gt.sync()) goto done;
       }
       ++k;
-      double t2[2], t1[1];
-      gr.result<2>(t2, SL_BB, smem);
-      gr.result<1>(t1, SL_RZ, smem);
-      rr = t2[1];
+      double t2[2];
+      const int slrz[2] = {SL_RR, SL_RZ};
+      gr.result_slots<2>(t2, slrz, smem);
+      rr = t2[0];
+      double t1[1] = {t2[1]};
       double gamma_;
       if (prec == FEM_PREC_NONE) {
         gamma_ = rr;
@@ -225,15 +259,17 @@ done:
 template <int KIND>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q,
                                                             double* z) {
-  extern __shared__ double smem[];  // [0,128) reductions, [128, 128+FEM_TILE_SMEM) tiles, then CTA-0 levels
+  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables, then CTA-0 levels
+  extern __shared__ double smem[];
   __shared__ double bstore[FEM_NSLOTS];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
+  fem_tables_to_smem<KIND>(sA, smem + 128 + FEM_TILE_SMEM);
   const CgArgs& A = sA;
   __shared__ unsigned int s_round;
   if (threadIdx.x == 0) s_round = 0u;
-  const GridTeam gt{A.sync, &s_round};
-  const GridReducer gr{A.sync};
+  const GridTeam gt{&A.sync, &s_round};
+  const GridReducer gr{&A.sync};
   const MgLevel& L0 = A.lv[0];
   const int nn = L0.g.nn;
   fem_zero_partials(A.sync);
@@ -279,13 +315,13 @@ int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq,
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq};
   return coop_launch(cg_fn(A.lv[0].g.kind), grid, args, s, "k_cg",
-                     (size_t)(128 + FEM_TILE_SMEM + A.block_smem) * sizeof(double));
+                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM + A.block_smem) * sizeof(double));
 }
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq, &z};
   return coop_launch(vc_fn(A.lv[0].g.kind), grid, args, s, "k_vcycle",
-                     (size_t)(128 + FEM_TILE_SMEM + A.block_smem) * sizeof(double));
+                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM + A.block_smem) * sizeof(double));
 }
 int fem_coop_occupancy_cg(int* occ) {
   int m = 1 << 30;
