@@ -5,11 +5,13 @@
 
 #define FEM_THREADS 512
 #define FEM_OP_THREADS 256
-// dynamic shared memory available to the CTA-0 multigrid levels of k_cg / k_vcycle
-#define FEM_BLOCK_SMEM_MAX (120 * 1024)
-// whole dynamic smem of k_cg / k_vcycle: reduction scratch + tile staging +
-// stencil tables + CTA-0 levels
-#define FEM_DYN_SMEM_MAX ((128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * 8 + FEM_BLOCK_SMEM_MAX)
+// whole dynamic smem of k_cg / k_vcycle: reduction scratch + tile staging + stencil tables
+#define FEM_DYN_SMEM_MAX ((128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * 8)
+// coarse multigrid levels: at most FEM_MG_TEAM CTAs, levels of at most
+// FEM_MG_TEAM_NN nodes (both can be overridden by the environment variables of
+// the same names)
+#define FEM_MG_TEAM 16
+#define FEM_MG_TEAM_NN 4096
 
 struct BiArgs {
   FemSync sync;

@@ -105,7 +105,7 @@ struct fem_ctx {
   uint8_t *dmask = nullptr, *pmask = nullptr, *aipin = nullptr;
   int has_dmask = 0, set_zeroP = 1;
   // multigrid
-  int nlev = 0, block_from = 0, block_smem = 0;
+  int nlev = 0, block_from = 0;
   double coarse_tol = 1e-8;
   CtxLevel lv[FEM_MAX_LEVELS];
   double *cr = nullptr, *cp = nullptr, *cq = nullptr;  // coarse CG scratch
@@ -508,23 +508,12 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
   FEM_ALLOC(c->cr, ncn);
   FEM_ALLOC(c->cp, ncn);
   FEM_ALLOC(c->cq, ncn);
-  // First level handled by CTA 0 alone: the coarsest levels whose vectors
-  // (x, r, t per level + 3 coarse-CG vectors) fit the dynamic smem budget and
-  // whose sizes are small enough for one SM (<= FEM_MG_BLOCK_NN nodes; 1024
-  // measured best on the 512^2-node Q2 Taylor-Green pressure solve).
-  int small = 1024;
-  const char* ev = getenv("FEM_MG_BLOCK_NN");
-  if (ev) small = atoi(ev);
-  const long long budget = FEM_BLOCK_SMEM_MAX / sizeof(double);
+  // First level handled by the coarse-level team: the coarsest levels of at
+  // most FEM_MG_TEAM_NN nodes.
+  int small = FEM_MG_TEAM_NN;
+  if (const char* ev = getenv("FEM_MG_TEAM_NN")) small = atoi(ev);
   int bf = nlev - 1;
-  long long need = 3LL * c->lv[nlev - 1].g.nn + 3LL * c->lv[nlev - 1].g.nn;
-  for (int l = nlev - 2; l >= 0; --l) {
-    const long long nd = need + 3LL * c->lv[l].g.nn;
-    if (c->lv[l].g.nn > small || nd > budget) break;
-    need = nd;
-    bf = l;
-  }
-  c->block_smem = (need <= budget && getenv("FEM_MG_BLOCK_GLOBAL") == nullptr) ? (int)need : 0;
+  for (int l = nlev - 2; l >= 0 && c->lv[l].g.nn <= small; --l) bf = l;
   c->block_from = bf;
   return FEM_OK;
 }
@@ -627,7 +616,6 @@ static void fill_cg_args(fem_ctx* c, CgArgs& A) {
   A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS, c->trace, c->trace_cap};
   A.nlev = c->nlev;
   A.block_from = c->block_from;
-  A.block_smem = c->block_smem;
   A.pinned = c->set_zeroP;
   A.coarse_maxiter = 1000;
   A.coarse_tol = c->coarse_tol;
@@ -653,6 +641,7 @@ static void fill_cg_args(fem_ctx* c, CgArgs& A) {
     M.sum_colw = L.sum_colw;
     M.sum_rc = L.sum_rc;
     M.sum_rcD = L.sum_rcD;
+    M.inv_nn = 1.0 / (double)L.g.nn;
     M.x = L.x;
     M.r = (l == 0) ? c->pr : L.r;
     M.t = L.t;
@@ -661,8 +650,16 @@ static void fill_cg_args(fem_ctx* c, CgArgs& A) {
   if (c->nlev == 1 || !c->lv[0].pin) A.lv[0].pin = c->pmask;
 }
 
+// CTAs of the coarse-level multigrid team for a launch of `grid` CTAs
+static int team_size(int grid) {
+  int t = FEM_MG_TEAM;
+  if (const char* ev = getenv("FEM_MG_TEAM")) t = atoi(ev);
+  if (t < 1) t = 1;
+  return t < grid ? t : grid;
+}
+
 static int reset_sync(fem_ctx* c, cudaStream_t s) {
-  FEM_CHECK(cudaMemsetAsync(c->bar, 0, sizeof(unsigned int), s));  // arrival count only
+  FEM_CHECK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned int), s));  // grid and team arrival counts
   FEM_CHECK(cudaMemsetAsync(c->err, 0, sizeof(int), s));
   return FEM_OK;
 }
@@ -684,6 +681,7 @@ static int run_cg(fem_ctx* c, const double* b, double* x, double tol, double ato
   A.final_rr = nullptr;
   FEM_TRY(reset_sync(c, s));
   const int grid = ctx_grid_for(c, c->g.nn);
+  A.team = team_size(grid);
   double* cr = c->cr ? c->cr : c->pz;
   double* cp = c->cp ? c->cp : c->pz;
   double* cq = c->cq ? c->cq : c->pz;
@@ -703,7 +701,9 @@ extern "C" int fem_mg_vcycle(fem_ctx* c, const double* r, double* z, cudaStream_
   fill_cg_args(c, A);
   FEM_CHECK(cudaMemcpyAsync(c->pr, r, sizeof(double) * c->g.nn, cudaMemcpyDeviceToDevice, s));
   FEM_TRY(reset_sync(c, s));
-  return fem_launch_vcycle(A, ctx_grid_for(c, c->g.nn), c->cr, c->cp, c->cq, z, s);
+  const int grid = ctx_grid_for(c, c->g.nn);
+  A.team = team_size(grid);
+  return fem_launch_vcycle(A, grid, c->cr, c->cp, c->cq, z, s);
 }
 
 static int run_bicgstab(fem_ctx* c, int ncomp, const MatCombo& op, const uint8_t* mask, const double* b, double* x,

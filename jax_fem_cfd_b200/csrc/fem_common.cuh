@@ -172,7 +172,7 @@ __device__ __forceinline__ bool fem_watchdog_fired(const int* err) {
 
 struct FemSync {
   unsigned int* count;    // arrivals in the current barrier generation
-  unsigned int* gen;      // barrier generation
+  unsigned int* team_count;  // arrivals at the coarse-level team barrier (SubTeam)
   int* err;               // sticky error flags (FEM_ERR_*)
   double* partials;       // [slot][cta] partial sums
   int nslots;
@@ -198,15 +198,27 @@ __device__ __forceinline__ unsigned long long fem_globaltimer() {
 // every CTA leaves the kernel at its next barrier instead of hanging the GPU.
 #define FEM_BARRIER_TIMEOUT_NS 2000000000ull
 
-// Diagnostic trace mark (CTA 0, thread 0): appends %globaltimer | (tag << 56).
-__device__ __forceinline__ void fem_trace_mark(const FemSync& s, unsigned long long tag) {
-  if (s.trace && blockIdx.x == 0 && threadIdx.x == 0) {
-    const unsigned long long n = s.trace[0] + 1;
-    if ((int)n < s.trace_cap) {
-      s.trace[n] = (fem_globaltimer() & 0x00FFFFFFFFFFFFFFull) | (tag << 56);
-      s.trace[0] = n;
-    }
+// Diagnostic trace (CTA 0, thread 0): appends %globaltimer | (tag << 56) to
+// trace[1..], trace[0] = count. The running count lives in shared memory
+// (fem_trace_init at kernel start), so a mark is two stores and no load.
+__device__ __forceinline__ int* fem_trace_count() {
+  __shared__ int n;
+  return &n;
+}
+__device__ __forceinline__ void fem_trace_init(const FemSync& s) {
+  if (s.trace && blockIdx.x == 0 && threadIdx.x == 0) *fem_trace_count() = (int)s.trace[0];
+}
+__device__ __forceinline__ void fem_trace_put(unsigned long long* tr, int cap, unsigned long long tag) {
+  int* cnt = fem_trace_count();
+  const int n = *cnt + 1;
+  if (n < cap) {
+    tr[n] = (fem_globaltimer() & 0x00FFFFFFFFFFFFFFull) | (tag << 56);
+    tr[0] = (unsigned long long)n;
+    *cnt = n;
   }
+}
+__device__ __forceinline__ void fem_trace_mark(const FemSync& s, unsigned long long tag) {
+  if (s.trace && blockIdx.x == 0 && threadIdx.x == 0) fem_trace_put(s.trace, s.trace_cap, tag);
 }
 
 // Shared-memory staging. fem_stage issues dst[q] = src[idx(q)] for q < n: by
@@ -244,55 +256,112 @@ __device__ __forceinline__ int fem_wrap(int v, int n) {
 // Grid barrier on a monotonic arrival counter (reset to 0 before each launch):
 // barrier number k of the launch completes when the counter reaches
 // k * gridDim.x. One fire-and-forget release-add per CTA, then acquire polling.
+// Bounded barrier on a monotonic arrival counter shared by `parties` CTAs
+// (thread 0 of each; reset to 0 before each launch): barrier number k of the
+// launch completes when the counter reaches k * parties. Ordering: the CTA's
+// writes reach thread 0 through __syncthreads, its release-add publishes them
+// at gpu scope, the pollers' acquire-load of the final count orders every later
+// read after them, and the closing __syncthreads passes that on to the CTA's
+// other threads. Returns false on timeout (or a timeout raised elsewhere).
+struct FemNoPartials {
+  __device__ __forceinline__ void warp_part(double*) const {}
+  __device__ __forceinline__ void store(const FemSync*, const double*) const {}
+};
+// K per-thread values bound for K partial slots, summed as part of a barrier:
+// warps reduce by a fixed shuffle tree, thread 0 adds the warp sums in warp
+// order and writes this CTA's partials right before it arrives.
+template <int K>
+struct FemPartials {
+  double* v;         // the thread's K values (summed in place)
+  const int* slots;  // K slot numbers
+  __device__ __forceinline__ void warp_part(double* smem) const {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < K; ++q) smem[q * 16 + warp] = v[q];
+  }
+  __device__ __forceinline__ void store(const FemSync* s, const double* smem) const {
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += smem[q * 16 + w];
+      s->partials[(size_t)slots[q] * gridDim.x + blockIdx.x] = t;
+    }
+  }
+};
+
+template <class Parts = FemNoPartials>
+__device__ __forceinline__ bool fem_counter_barrier(const FemSync* s, unsigned int* cnt, unsigned int* round,
+                                                    int parties, unsigned long long tag, const Parts& parts = Parts(),
+                                                    double* smem = nullptr) {
+  __shared__ int s_ok;
+  parts.warp_part(smem);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    parts.store(s, smem);
+    int ok = 1;
+    const unsigned int target = (*round + 1u) * (unsigned)parties;
+    *round = *round + 1u;
+    int* err = s->err;
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(cnt), "r"(1u) : "memory");
+    if (parties > 1) {
+      const unsigned long long t0 = fem_globaltimer();
+      unsigned int polls = 0;
+      while (fem_ld_acquire(cnt) < target) {
+        if (((++polls) & 63u) == 0u) {
+          if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) { ok = 0; break; }
+          if (fem_globaltimer() - t0 > FEM_BARRIER_TIMEOUT_NS) {
+            atomicOr(err, FEM_ERR_BARRIER_TIMEOUT);
+            ok = 0;
+            break;
+          }
+        }
+      }
+    }
+    if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
+    s_ok = ok;
+    if (s->trace && blockIdx.x == 0) fem_trace_put(s->trace, s->trace_cap, tag);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Every CTA of the launch (cooperative, all co-resident).
 struct GridTeam {
   const FemSync* s;     // the launch's barrier state (shared-memory copy of the kernel arguments)
-  unsigned int* round;  // per-CTA count of completed barriers (shared memory, thread 0, starts at 0)
+  unsigned int* round;  // per-CTA count of completed grid barriers (shared memory, thread 0, starts at 0)
   __device__ __forceinline__ int rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
   __device__ __forceinline__ int size() const { return gridDim.x * blockDim.x; }
   __device__ __forceinline__ int cta() const { return blockIdx.x; }
   __device__ __forceinline__ int ncta() const { return gridDim.x; }
-  // Returns false if the kernel must stop (timeout or error raised elsewhere).
-  // Ordering: the CTA's writes reach thread 0 through __syncthreads, its
-  // release-add publishes them at gpu scope, the pollers' acquire-load of the
-  // final count orders every later read after them, and the closing
-  // __syncthreads passes that on to the CTA's other threads.
-  __device__ bool sync() const {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int ok = 1;
-      const unsigned int target = (*round + 1u) * gridDim.x;
-      *round = *round + 1u;
-      unsigned int* cnt = s->count;
-      int* err = s->err;
-      asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(cnt), "r"(1u) : "memory");
-      if (gridDim.x > 1) {
-        const unsigned long long t0 = fem_globaltimer();
-        unsigned int polls = 0;
-        while (fem_ld_acquire(cnt) < target) {
-          if (((++polls) & 63u) == 0u) {
-            if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) { ok = 0; break; }
-            if (fem_globaltimer() - t0 > FEM_BARRIER_TIMEOUT_NS) {
-              atomicOr(err, FEM_ERR_BARRIER_TIMEOUT);
-              ok = 0;
-              break;
-            }
-          }
-        }
-      }
-      if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
-      s_ok = ok;
-      unsigned long long* tr = s->trace;
-      if (tr && blockIdx.x == 0) {
-        const unsigned long long n = tr[0] + 1;
-        if ((int)n < s->trace_cap) {
-          tr[n] = (fem_globaltimer() & 0x00FFFFFFFFFFFFFFull) | (31ull << 56);
-          tr[0] = n;
-        }
-      }
-    }
-    __syncthreads();
-    return s_ok != 0;
+  __device__ bool sync() const { return fem_counter_barrier(s, s->count, round, gridDim.x, 31); }
+  // reduce K values into K partial slots and sync, in one step (smem: 16*K doubles)
+  template <int K>
+  __device__ bool reduce_sync(double (&v)[K], const int (&slots)[K], double* smem) const {
+    return fem_counter_barrier(s, s->count, round, gridDim.x, 31, FemPartials<K>{v, slots}, smem);
+  }
+};
+
+// The first n CTAs of the launch (the coarse multigrid levels), with their own
+// arrival counter; the other CTAs do not take part.
+struct SubTeam {
+  const FemSync* s;
+  unsigned int* round;  // per-CTA count of completed team barriers (shared memory)
+  int n;
+  __device__ __forceinline__ int rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+  __device__ __forceinline__ int size() const { return n * blockDim.x; }
+  __device__ __forceinline__ int cta() const { return blockIdx.x; }
+  __device__ __forceinline__ int ncta() const { return n; }
+  __device__ bool sync() const { return fem_counter_barrier(s, s->team_count, round, n, 30); }
+  template <int K>
+  __device__ bool reduce_sync(double (&v)[K], const int (&slots)[K], double* smem) const {
+    return fem_counter_barrier(s, s->team_count, round, n, 30, FemPartials<K>{v, slots}, smem);
   }
 };
 
@@ -357,35 +426,52 @@ struct GridReducer {
   // every slot (all loads of a thread in flight at once), warps combine theirs
   // by a fixed shuffle tree, and every thread adds the warp sums in warp order:
   // the same order, hence the same bits, in every CTA. Uses smem[0, 16*K).
+  // Split in two so that other loads (a phase's staging copies) can be issued
+  // between them: result_begin issues this thread's partial loads,
+  // result_end combines them (both called by every thread of the CTA).
   template <int K>
-  __device__ __forceinline__ void result_slots(double (&out)[K], const int (&slots)[K], double* smem) const {
-    static_assert(K <= 8, "result_slots: at most 8 slots");
-    const int G = gridDim.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int nwd = (G + 31) >> 5;
+  struct Pending {
+    double acc[K];
+  };
+  __device__ __forceinline__ int data_warps() const {
+    int nwd = (gridDim.x + 31) >> 5;
     if (nwd > 16) nwd = 16;
     if (nwd > (int)(blockDim.x >> 5)) nwd = blockDim.x >> 5;
+    return nwd;
+  }
+  template <int K>
+  __device__ __forceinline__ Pending<K> result_begin(const int (&slots)[K]) const {
+    static_assert(K <= 8, "result_slots: at most 8 slots");
+    Pending<K> p;
+    const int G = gridDim.x, nwd = data_warps();
     const double* __restrict__ part = s->partials;
+#pragma unroll
+    for (int q = 0; q < K; ++q) p.acc[q] = 0.0;
+    if ((int)(threadIdx.x >> 5) < nwd) {
+      // first column: plain loads, not consumed here (result_end waits for them)
+      if ((int)threadIdx.x < G)
+#pragma unroll
+        for (int q = 0; q < K; ++q) p.acc[q] = __ldcg(&part[(size_t)slots[q] * G + threadIdx.x]);
+      for (int c = threadIdx.x + nwd * 32; c < G; c += nwd * 32) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) p.acc[q] += __ldcg(&part[(size_t)slots[q] * G + c]);
+      }
+    }
+    return p;
+  }
+  template <int K>
+  __device__ __forceinline__ void result_end(Pending<K>& p, double (&out)[K], double* smem) const {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwd = data_warps();
     __syncthreads();
     if (warp < nwd) {
-      double acc[K];
-#pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] = 0.0;
-      for (int c = threadIdx.x; c < G; c += nwd * 32) {
-        double v[K];
-#pragma unroll
-        for (int q = 0; q < K; ++q) v[q] = __ldcg(&part[(size_t)slots[q] * G + c]);
-#pragma unroll
-        for (int q = 0; q < K; ++q) acc[q] += v[q];
-      }
 #pragma unroll
       for (int q = 0; q < K; ++q) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        for (int o = 16; o > 0; o >>= 1) p.acc[q] += __shfl_xor_sync(0xffffffffu, p.acc[q], o);
       }
       if (lane == 0)
 #pragma unroll
-        for (int q = 0; q < K; ++q) smem[q * 16 + warp] = acc[q];
+        for (int q = 0; q < K; ++q) smem[q * 16 + warp] = p.acc[q];
     }
     __syncthreads();
 #pragma unroll
@@ -395,6 +481,11 @@ struct GridReducer {
       out[q] = t;
     }
     __syncthreads();
+  }
+  template <int K>
+  __device__ __forceinline__ void result_slots(double (&out)[K], const int (&slots)[K], double* smem) const {
+    Pending<K> p = result_begin<K>(slots);
+    result_end<K>(p, out, smem);
   }
   template <int K>
   __device__ __forceinline__ void result(double (&out)[K], int slot, double* smem) const {

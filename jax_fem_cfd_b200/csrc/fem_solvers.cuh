@@ -49,6 +49,7 @@ struct MgLevel {
   double sum_colw;        // sum over nodes of the prolongation column sums (levels >= 1)
   double sum_rc;          // sum over nodes of the restriction row sums c = R 1 (levels >= 1)
   double sum_rcD;         // sum of c / diag
+  double inv_nn;          // 1 / nn (means)
   double* x;              // level correction X_n
   double* r;              // level residual R_n (level 0: the CG residual)
   double* t;              // scratch (fine residual before restriction / prolongated x)
@@ -57,7 +58,8 @@ struct MgLevel {
 struct CgArgs {
   FemSync sync;
   int nlev;            // multigrid levels (level 0 = the problem mesh)
-  int block_from;      // first level solved by CTA 0 alone (<= nlev - 1)
+  int block_from;      // first level handled by the coarse-level team (<= nlev - 1)
+  int team;            // CTAs in the coarse-level team (the first ones of the grid)
   int prec;
   int pinned;          // 1: set_zeroP (rows / values on gamma_p zeroed); 0: mean-zero
   int center_rhs;      // mean-zero: subtract mean(b) first (solvers/standard.py:106)
@@ -72,7 +74,6 @@ struct CgArgs {
   int* status;         // device out: FEM_ERR_* of this solve
   double* final_rr;    // device out: final r.r (diagnostics)
   int post;            // final pin / mean fix of solvers/standard.py:119-123
-  int block_smem;      // doubles of dynamic smem for the CTA-0 levels (0: they stay in global memory)
   MgLevel lv[FEM_MAX_LEVELS];
 };
 
@@ -160,25 +161,33 @@ __device__ __forceinline__ double* fem_affine_cache() {
   __shared__ double c[2 * FEM_MAX_LEVELS];
   return c;
 }
-template <class Red>
-__device__ __forceinline__ LevelAffine fem_level_affine(const Red& red, const CgArgs& A, int m, double* smem) {
+// Slots of the sums behind a level's affine terms (a third, ignored one at level 0).
+__device__ __forceinline__ void fem_level_affine_slots(int m, int (&sl)[3]) {
+  sl[0] = SL_R(m);
+  sl[1] = SL_R(m) + 1;
+  sl[2] = m > 0 ? SL_T(m - 1) : SL_R(m);
+}
+__device__ __forceinline__ LevelAffine fem_level_affine_from(const CgArgs& A, int m, const double (&u)[3]) {
   const MgLevel& L = A.lv[m];
   LevelAffine f;
   if (m == 0) {
-    double u[2];
-    red.template result<2>(u, SL_R(0), smem);
     f.alpha = 0.0;
-    f.beta = u[0] / L.g.nn;
+    f.beta = u[0] * L.inv_nn;
     f.sum_rhD = u[1] - f.beta * L.sum_invD;
   } else {
-    double u[3];
-    const int sl[3] = {SL_R(m), SL_R(m) + 1, SL_T(m - 1)};
-    red.template result_slots<3>(u, sl, smem);
-    f.alpha = u[2] / A.lv[m - 1].g.nn;
-    f.beta = (u[0] - f.alpha * L.sum_rc) / L.g.nn;
+    f.alpha = u[2] * A.lv[m - 1].inv_nn;
+    f.beta = (u[0] - f.alpha * L.sum_rc) * L.inv_nn;
     f.sum_rhD = u[1] - f.alpha * L.sum_rcD - f.beta * L.sum_invD;
   }
   return f;
+}
+template <class Red>
+__device__ __forceinline__ LevelAffine fem_level_affine(const Red& red, const CgArgs& A, int m, double* smem) {
+  int sl[3];
+  fem_level_affine_slots(m, sl);
+  double u[3];
+  red.template result_slots<3>(u, sl, smem);
+  return fem_level_affine_from(A, m, u);
 }
 
 // Down-sweep step n -> n+1 in one phase: pre-smooth from zero
@@ -200,15 +209,28 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
   const bool pinned = A.pinned;
   LevelAffine f{0.0, 0.0, 0.0};
   double mx = 0.0;
-  if (!pinned) {
-    f = fem_level_affine(red, A, n, smem);
-    mx = (2.0 / 3.0) * f.sum_rhD / nn;
+  bool have_f = pinned;
+  // the level's affine terms (mean-zero): partial loads issued now, combined
+  // after the first tile's copies have been issued
+  int asl[3];
+  fem_level_affine_slots(n, asl);
+  typename Red::template Pending<3> pend{};
+  if (!pinned) pend = red.template result_begin<3>(asl);
+  fem_trace_mark(A.sync, 16);
+  auto read_affine = [&]() {
+    if (have_f) return;
+    double u3[3];
+    fem_trace_mark(A.sync, 17);
+    red.template result_end<3>(pend, u3, smem);
+    fem_trace_mark(A.sync, 18);
+    f = fem_level_affine_from(A, n, u3);
+    mx = (2.0 / 3.0) * f.sum_rhD * L.inv_nn;
     if (threadIdx.x == 0) {
       fem_affine_cache()[2 * n] = f.alpha;
       fem_affine_cache()[2 * n + 1] = f.beta;
     }
-  }
-  fem_trace_mark(A.sync, 1);
+    have_f = true;
+  };
   const double* u = L.r;
   const double* iDv = pinned ? L.winvD : L.invD;
   const double* tab = L.tab;
@@ -262,6 +284,8 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
       const int Rr = min(R0 + ky, cuy - 1), Cc = min(C0 + kx, cux - 1);
       return Rr * cux + Cc;
     });
+    read_affine();
+    fem_trace_mark(A.sync, 1);
     fem_stage_wait();
     fem_trace_mark(A.sync, 2);
     // xh on the staged region (pinned: winvD is 0 on gamma_p, which also marks it)
@@ -339,12 +363,12 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
     }
     __syncthreads();
   }
+  read_affine();  // CTAs without a tile still cache the level's terms for the up-sweep
   fem_trace_mark(A.sync, 4);
   if (!pinned) {
     const int sl[3] = {SL_T(n), SL_R(n + 1), SL_R(n + 1) + 1};
-    red.template reduce_slots<3>(acc, sl, smem);
+    return tm.template reduce_sync<3>(acc, sl, smem);
   }
-  fem_trace_mark(A.sync, 5);
   return tm.sync();
 }
 
@@ -443,17 +467,24 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
   const bool pinned = A.pinned;
   double mX = 0.0, mP = 0.0;
   LevelAffine f{0.0, 0.0, 0.0};
-  if (!pinned) {
+  bool have_m = pinned;
+  // the coarse correction's means (mean-zero): partial loads issued now,
+  // combined after the first tile's copies have been issued
+  const int msl[2] = {SL_X(n + 1), SL_X(n + 1) + 1};
+  typename Red::template Pending<2> pend{};
+  if (!pinned) pend = red.template result_begin<2>(msl);
+  auto read_means = [&]() {
+    if (have_m) return;
     double v[2];
-    red.template result<2>(v, SL_X(n + 1), smem);  // its __syncthreads also publishes the cache
-    mX = v[0] / C.g.nn;
-    mP = (v[1] - mX * C.sum_colw) / nn;
+    red.template result_end<2>(pend, v, smem);  // its __syncthreads also publishes the cache
+    mX = v[0] * C.inv_nn;
+    mP = (v[1] - mX * C.sum_colw) * L.inv_nn;
     if (n > 0) {
       f.alpha = fem_affine_cache()[2 * n];
       f.beta = fem_affine_cache()[2 * n + 1];
     }
-  }
-  fem_trace_mark(A.sync, 11);
+    have_m = true;
+  };
   const int ux = g.nnx, uy = g.nny, cux = C.lat.ux(), cuy = C.lat.uy();
   const bool per = g.periodic;
   const int nc = fem_axis_ncls(KIND, per);
@@ -477,7 +508,7 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
   double* sw = sy + NS;                     // pinned only
   double* sc = sy + nf * NS;                // coarse X_{n+1}, CXB x CYB
   double* sr = sc + CXB * CYB;              // rhs of owned nodes, 32 x TY
-  double* sd = sr + 32 * TY;                // diag of owned nodes
+  double* sd = sr + 32 * TY;                // 1 / diag of owned nodes
   const int nty = (uy + TY - 1) / TY, ntile = ntx * nty;
   const double* tabo = L.tab_off;
   const double w = 2.0 / 3.0;
@@ -524,7 +555,9 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
       return cr * cux + cc;
     });
     fem_stage(sr, L.r, 32 * TY, oidx);
-    fem_stage(sd, L.diag, 32 * TY, oidx);
+    fem_stage(sd, L.invD, 32 * TY, oidx);
+    read_means();
+    fem_trace_mark(A.sync, 11);
     fem_stage_wait();
     // y = X_n + P X_{n+1} in place (the arithmetic of fem_interp_at)
     for (int q = threadIdx.x; q < NS; q += blockDim.x) {
@@ -564,7 +597,7 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
         const double yi = sy[qc];
         const double rhv = sr[ty * 32 + tx];
         const double rv = (!pinned && n > 0) ? rhv - f.alpha * fem_restrict_rowsum(L.lat, yy, x) - f.beta : rhv;
-        double xn = w * (rv - off) / sd[ty * 32 + tx] + (1.0 - w) * yi;
+        double xn = w * (rv - off) * sd[ty * 32 + tx] + (1.0 - w) * yi;
         if (pinned && sw[qc] == 0.0) xn = 0.0;
         L.t[yy * ux + x] = xn;
         if (n == 0) {
@@ -579,105 +612,52 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
     __syncthreads();
   }
   fem_trace_mark(A.sync, 12);
-  if (n == 0 || !pinned) red.template reduce<2>(a, SL_X(n), smem);
-  fem_trace_mark(A.sync, 13);
-  if (!tm.sync()) return false;
-  return true;
+  if (n == 0 || !pinned) {
+    const int sl[2] = {SL_X(n), SL_X(n) + 1};
+    return tm.template reduce_sync<2>(a, sl, smem);
+  }
+  return tm.sync();
 }
 
 // Full V-cycle on r = lv[0].r; result in lv[0].t (raw; mean-zero subtracts
-// SL_X(0)[0]/nn lazily). Levels >= block_from run in CTA 0.
+// SL_X(0)[0]/nn lazily). Levels < block_from run on the whole grid; levels from
+// block_from down run on the team of the first A.team CTAs (SubTeam barriers,
+// data in global memory), the coarsest solve in CTA 0. Grid-produced sums are
+// read over all CTA columns; team phases write only the team's columns (the
+// rest of those slots stay zero), so the same reads stay exact.
 template <int KIND>
 __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr, const CgArgs& A, double* smem,
-                                       double* bstore, double* cg_r, double* cg_p, double* cg_q) {
+                                       unsigned int* team_round, double* cg_r, double* cg_p, double* cg_q) {
   const int N = A.nlev, s = A.block_from;
   for (int n = 0; n < s; ++n)
     if (!mg_down<KIND>(gt, gr, A, n, smem)) return false;
-  if (blockIdx.x == 0) {
-    const BlockTeam bt;
-    const BlockReducer br{bstore};
-    // Levels >= s: with block_smem their x / r / t vectors and the coarse-CG
-    // scratch live in dynamic shared memory (no L2 round trips between the
-    // CTA-local phases); the level-s residual is copied in, x_s copied out.
-    __shared__ __align__(16) CgArgs sAb;
-    extern __shared__ double dyn[];
-    const bool in_smem = A.block_smem > 0;
-    const CgArgs& B = in_smem ? sAb : A;
-    if (in_smem) {
-      {
-        const int* src = reinterpret_cast<const int*>(&A);
-        int* dst = reinterpret_cast<int*>(&sAb);
-        for (int i = threadIdx.x; i < (int)(sizeof(CgArgs) / 4); i += blockDim.x) dst[i] = src[i];
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double* p = dyn + 128 + FEM_TILE_SMEM + FEM_TAB_SMEM;
-        for (int n = s; n < N; ++n) {
-          const int m = A.lv[n].g.nn;
-          sAb.lv[n].x = p;
-          sAb.lv[n].r = p + m;
-          sAb.lv[n].t = p + 2 * m;
-          p += 3 * m;
-        }
-      }
-      __syncthreads();
-      const double* __restrict__ rsrc = A.lv[s].r;
-      double* __restrict__ rdst = sAb.lv[s].r;
-      for (int i = threadIdx.x; i < A.lv[s].g.nn; i += blockDim.x) rdst[i] = rsrc[i];
-      const int mc = A.lv[N - 1].g.nn;
-      double* p = dyn + 128 + FEM_TILE_SMEM + FEM_TAB_SMEM;
-      for (int n = s; n < N; ++n) p += 3 * A.lv[n].g.nn;
-      cg_r = p;
-      cg_p = p + mc;
-      cg_q = p + 2 * mc;
-      __syncthreads();
-    }
-    // import the grid-produced sums of level s
-    if (!B.pinned) {
-      double v[2], t[1] = {0.0};
-      gr.result<2>(v, SL_R(s), smem);
-      if (s > 0) gr.result<1>(t, SL_T(s - 1), smem);
-      if (threadIdx.x == 0) {
-        bstore[SL_R(s)] = v[0];
-        bstore[SL_R(s) + 1] = v[1];
-        if (s > 0) bstore[SL_T(s - 1)] = t[0];
-      }
-      __syncthreads();
-    }
-    fem_trace_mark(A.sync, 6);
-    for (int n = s; n < N - 1; ++n) mg_down<KIND>(bt, br, B, n, smem);
+  if ((int)blockIdx.x < A.team) {
+    const SubTeam tt{gt.s, team_round, A.team};
+    for (int n = s; n < N - 1; ++n)
+      if (!mg_down<KIND>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 7);
-    mg_coarse<KIND>(br, B, smem, cg_r, cg_p, cg_q);
-    fem_trace_mark(A.sync, 8);
-    const MgLevel& Lc = B.lv[N - 1];
-    if (N == 1) {
-      // single level: the coarse solve is the whole preconditioner; r.z pieces
-      double a[2] = {0.0, 0.0};
-      for (int i = threadIdx.x; i < Lc.g.nn; i += blockDim.x) {
-        a[0] += Lc.t[i];
-        a[1] += Lc.r[i] * Lc.t[i];
+    if (blockIdx.x == 0) {
+      mg_coarse<KIND>(gr, A, smem, cg_r, cg_p, cg_q);
+      fem_trace_mark(A.sync, 8);
+      const MgLevel& Lc = A.lv[N - 1];
+      if (N == 1) {
+        // single level: the coarse solve is the whole preconditioner; r.z pieces
+        double a[2] = {0.0, 0.0};
+        for (int i = threadIdx.x; i < Lc.g.nn; i += blockDim.x) {
+          a[0] += Lc.t[i];
+          a[1] += Lc.r[i] * Lc.t[i];
+        }
+        gr.reduce<2>(a, SL_X(0), smem);
+      } else if (!A.pinned) {
+        double a[2] = {0.0, 0.0};
+        for (int i = threadIdx.x; i < Lc.g.nn; i += blockDim.x) mg_xsums(Lc, i, Lc.t[i], a);
+        gr.reduce<2>(a, SL_X(N - 1), smem);
       }
-      br.reduce<2>(a, SL_X(0), smem);
-      __syncthreads();
-    } else if (!B.pinned) {
-      double a[2] = {0.0, 0.0};
-      for (int i = threadIdx.x; i < Lc.g.nn; i += blockDim.x) mg_xsums(Lc, i, Lc.t[i], a);
-      br.reduce<2>(a, SL_X(N - 1), smem);
-      __syncthreads();
     }
-    fem_trace_mark(A.sync, 9);
-    for (int n = N - 2; n >= s; --n) mg_up<KIND>(bt, br, B, n, smem);
+    if (!tt.sync()) return false;
+    for (int n = N - 2; n >= s; --n)
+      if (!mg_up<KIND>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 10);
-    if (in_smem) {
-      const double* __restrict__ xs = sAb.lv[s].t;
-      double* __restrict__ xd = A.lv[s].t;
-      for (int i = threadIdx.x; i < A.lv[s].g.nn; i += blockDim.x) xd[i] = xs[i];
-    }
-    // export the level-s sums for the grid (CTA 0 column; other columns stay zero)
-    if (threadIdx.x == 0 && (s == 0 || !A.pinned)) {
-      A.sync.partials[(size_t)SL_X(s) * gridDim.x] = bstore[SL_X(s)];
-      A.sync.partials[(size_t)(SL_X(s) + 1) * gridDim.x] = bstore[SL_X(s) + 1];
-    }
   }
   if (!gt.sync()) return false;
   for (int n = s - 1; n >= 0; --n)

@@ -355,10 +355,16 @@ __device__ __forceinline__ int fem_tile_rows(int nx, int ny, int nplanes, int ha
   return th;
 }
 
-template <int KIND, int NSRC, class Team, class Comb, class Body>
+struct FemNoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+// pre() runs once per CTA while its first tile's copies are in flight (every
+// thread, before comb is used; a CTA without a tile runs it after the loop).
+template <int KIND, int NSRC, class Team, class Comb, class Body, class Pre = FemNoHook>
 __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid& g, const double* tab,
                                                   double* __restrict__ sm, const double* const (&src)[NSRC],
-                                                  const Comb& comb, const Body& body) {
+                                                  const Comb& comb, const Body& body, const Pre& pre = Pre()) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
   constexpr bool D3 = (KIND == FEM_HEX8);
   const int WR = blockDim.x >> 5;  // warps = rows per pass
@@ -385,6 +391,7 @@ __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid&
     };
 #pragma unroll
     for (int k = 0; k < NSRC; ++k) fem_stage(sm + k * NS, src[k], NS, gidx);
+    if (t == tm.cta()) pre();
     fem_stage_wait();
     for (int s = threadIdx.x; s < NS; s += blockDim.x) {
       double v[NSRC];
@@ -413,6 +420,7 @@ __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid&
     }
     __syncthreads();
   }
+  if (tm.cta() >= ntile) pre();
 }
 
 // Tiled element-by-element product with per-element coefficients m(e, a, b, nen)

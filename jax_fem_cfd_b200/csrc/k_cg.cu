@@ -5,8 +5,8 @@
 // Preconditioner application z = M r; returns gamma = r . z.
 template <int KIND>
 __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer& gr, const CgArgs& A, double* smem,
-                              double* bstore, double* cg_r, double* cg_p, double* cg_q, double rr, double r2d,
-                              double& gamma, double& mz) {
+                              unsigned int* team_round, double* cg_r, double* cg_p, double* cg_q, double rr, double r2d,
+                              double& gamma, double& mz, bool defer = false) {
   const MgLevel& L0 = A.lv[0];
   const int nn = L0.g.nn;
   mz = 0.0;
@@ -19,7 +19,8 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
     return true;
   }
   if (A.prec == FEM_PREC_MG) {
-    if (!mg_vcycle<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return false;
+    if (!mg_vcycle<KIND>(gt, gr, A, smem, team_round, cg_r, cg_p, cg_q)) return false;
+    if (defer) return true;  // the caller reads gamma and mz (cg_mg_results) later
     if (A.pinned) {
       double s[2];
       gr.result<2>(s, SL_X(0), smem);
@@ -28,7 +29,7 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
       double s[3];
       const int sl[3] = {SL_X(0), SL_X(0) + 1, SL_R(0)};
       gr.result_slots<3>(s, sl, smem);
-      mz = s[0] / nn;
+      mz = s[0] * L0.inv_nn;
       gamma = s[1] - mz * s[2];
     }
     return true;
@@ -66,17 +67,37 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
   return true;
 }
 
+// gamma = r.z and the lazy mean mz of z after a V-cycle (mean-zero: z - mean z),
+// from the slots {SL_X(0), SL_X(0) + 1, SL_R(0)}
+__device__ __forceinline__ void cg_mg_slots(int (&sl)[3]) {
+  sl[0] = SL_X(0);
+  sl[1] = SL_X(0) + 1;
+  sl[2] = SL_R(0);
+}
+__device__ __forceinline__ void cg_mg_from(const CgArgs& A, const double (&s)[3], double& gamma, double& mz) {
+  if (A.pinned) {
+    gamma = s[1];
+    mz = 0.0;
+  } else {
+    mz = s[0] * A.lv[0].inv_nn;
+    gamma = s[1] - mz * s[2];
+  }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q) {
-  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables, then CTA-0 levels
+  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables
   extern __shared__ double smem[];
-  __shared__ double bstore[FEM_NSLOTS];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
+  fem_trace_init(sA.sync);
   fem_tables_to_smem<KIND>(sA, smem + 128 + FEM_TILE_SMEM);
   const CgArgs& A = sA;
-  __shared__ unsigned int s_round;
-  if (threadIdx.x == 0) s_round = 0u;
+  __shared__ unsigned int s_round, s_team_round;
+  if (threadIdx.x == 0) {
+    s_round = 0u;
+    s_team_round = 0u;
+  }
   const GridTeam gt{&A.sync, &s_round};
   const GridReducer gr{&A.sync};
   const MgLevel& L0 = A.lv[0];
@@ -114,7 +135,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
         a2[1] += ri * ri;
         a3[0] += ri;
         a3[1] += ri * L0.invD[i];
-        a1[0] += ri * ri / D[i];
+        a1[0] += ri * ri * L0.invD[i];
       });
       gr.reduce<2>(a2, SL_BB, smem);
       gr.reduce<2>(a3, SL_R(0), smem);
@@ -127,9 +148,10 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
     rr = bb_rr[1];
     const double atol2 = fmax(A.tol * A.tol * bb_rr[0], A.atol * A.atol);
     double gamma, mz;
-    if (!cg_apply_prec<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, r2d[0], gamma, mz)) goto done;
+    if (!cg_apply_prec<KIND>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q, rr, r2d[0], gamma, mz)) goto done;
     double beta = 0.0;
     bool have_p = false;
+    bool pending = false;  // MG: gamma / mz of the last V-cycle are read in the next phase A
     int cur = 0;
     double rs = (A.prec == FEM_PREC_NONE) ? gamma : rr;
     const unsigned long long t_start = fem_globaltimer_early();
@@ -151,6 +173,20 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
           else zv = v[0];
           return have_p ? zv + beta * v[1] : zv;
         };
+        // pending V-cycle sums: loads issued here, combined while the copies fly
+        int msl[3];
+        cg_mg_slots(msl);
+        GridReducer::Pending<3> mpend{};
+        if (pending) mpend = gr.result_begin<3>(msl);
+        auto pre = [&]() {
+          if (!pending) return;
+          double s3[3], gamma_;
+          gr.result_end<3>(mpend, s3, smem);
+          cg_mg_from(A, s3, gamma_, mz);
+          beta = gamma_ / gamma;
+          gamma = gamma_;
+          pending = false;
+        };
         double a[1] = {0.0};
         fem_tiled_stencil<KIND, 3>(gt, g, L0.tab, smem + 128, srcA, comb,
                                    [&](int i, int, int, int, double q, double pn) {
@@ -158,9 +194,10 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
                                      if (pin0 && pin0[i]) q = 0.0;
                                      A.Ap[i] = q;
                                      a[0] += pn * q;
-                                   });
-        gr.reduce<1>(a, SL_PAP, smem);
-        if (!gt.sync()) goto done;
+                                   },
+                                   pre);
+        const int slp[1] = {SL_PAP};
+        if (!gt.reduce_sync<1>(a, slp, smem)) goto done;
       }
       double pap[1];
       gr.result<1>(pap, SL_PAP, smem);
@@ -172,7 +209,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
         const int stride = gt.size();
         const double* __restrict__ iD0 = L0.invD;
         for (int i0 = gt.rank(); i0 < nn; i0 += U * stride) {
-          double xv[U], pv[U], rv[U], av[U], iv[U], dv[U];
+          double xv[U], pv[U], rv[U], av[U], iv[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int i = i0 + u * stride;
@@ -182,7 +219,6 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
               rv[u] = A.r[i];
               av[u] = A.Ap[i];
               iv[u] = iD0[i];
-              dv[u] = D[i];
             }
           }
 #pragma unroll
@@ -195,14 +231,13 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
               a4[0] += ri * ri;
               a4[1] += ri;
               a4[2] += ri * iv[u];
-              a4[3] += ri * ri / dv[u];
+              a4[3] += ri * ri * iv[u];
             }
           }
         }
         const int sl4[4] = {SL_RR, SL_R(0), SL_R(0) + 1, SL_RZ};
-        gr.reduce_slots<4>(a4, sl4, smem);
         fem_watchdog_arm(A.sync.err, t_start);
-        if (!gt.sync()) goto done;
+        if (!gt.reduce_sync<4>(a4, sl4, smem)) goto done;
       }
       ++k;
       double t2[2];
@@ -217,10 +252,15 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
         gamma_ = t1[0];
       } else {
         if (!(rr > atol2 && k < A.maxiter)) break;  // z of a final iteration is never used
-        if (!cg_apply_prec<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q, rr, t1[0], gamma_, mz)) goto done;
+        const bool defer = (prec == FEM_PREC_MG);
+        if (!cg_apply_prec<KIND>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q, rr, t1[0], gamma_, mz, defer))
+          goto done;
+        pending = defer;
       }
-      beta = gamma_ / gamma;
-      gamma = gamma_;
+      if (!pending) {
+        beta = gamma_ / gamma;
+        gamma = gamma_;
+      }
       have_p = true;
       cur ^= 1;
       rs = (prec == FEM_PREC_NONE) ? gamma : rr;
@@ -259,15 +299,18 @@ done:
 template <int KIND>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q,
                                                             double* z) {
-  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables, then CTA-0 levels
+  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables
   extern __shared__ double smem[];
-  __shared__ double bstore[FEM_NSLOTS];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
+  fem_trace_init(sA.sync);
   fem_tables_to_smem<KIND>(sA, smem + 128 + FEM_TILE_SMEM);
   const CgArgs& A = sA;
-  __shared__ unsigned int s_round;
-  if (threadIdx.x == 0) s_round = 0u;
+  __shared__ unsigned int s_round, s_team_round;
+  if (threadIdx.x == 0) {
+    s_round = 0u;
+    s_team_round = 0u;
+  }
   const GridTeam gt{&A.sync, &s_round};
   const GridReducer gr{&A.sync};
   const MgLevel& L0 = A.lv[0];
@@ -281,10 +324,10 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double
   }
   gr.reduce<2>(a, SL_R(0), smem);
   if (!gt.sync()) return;
-  if (!mg_vcycle<KIND>(gt, gr, A, smem, bstore, cg_r, cg_p, cg_q)) return;
+  if (!mg_vcycle<KIND>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q)) return;
   double sx[2];
   gr.result<2>(sx, SL_X(0), smem);
-  const double mz = A.pinned ? 0.0 : sx[0] / nn;
+  const double mz = A.pinned ? 0.0 : sx[0] * L0.inv_nn;
   for (int i = gt.rank(); i < nn; i += gt.size()) z[i] = L0.t[i] - mz;
 }
 
@@ -315,18 +358,18 @@ int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq,
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq};
   return coop_launch(cg_fn(A.lv[0].g.kind), grid, args, s, "k_cg",
-                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM + A.block_smem) * sizeof(double));
+                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * sizeof(double));
 }
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq, &z};
   return coop_launch(vc_fn(A.lv[0].g.kind), grid, args, s, "k_vcycle",
-                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM + A.block_smem) * sizeof(double));
+                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * sizeof(double));
 }
 int fem_coop_occupancy_cg(int* occ) {
   int m = 1 << 30;
   for (int kind = 0; kind < 3; ++kind) {
-    // allow the CTA-0 multigrid levels up to FEM_BLOCK_SMEM_MAX bytes of dynamic smem
+    // allow the dynamic smem of the tile buffer and the stencil tables
     if (cudaFuncSetAttribute(cg_fn(kind), cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_DYN_SMEM_MAX) !=
             cudaSuccess ||
         cudaFuncSetAttribute(vc_fn(kind), cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_DYN_SMEM_MAX) !=
