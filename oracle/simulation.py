@@ -81,6 +81,11 @@ def simple_mesh(mc, ns):
     mesh_func = mesh_func_for(mc)
     node_coords, nconn, surfnodes, bconns, nvecs = mesh_func(*mc.num_elem, *mc.domain_size)
     ndim = len(mc.num_elem)
+    if ndim == 3:
+        # build-defined 3D boundary integral: on the geometric face quads (the
+        # reference's D/T/F/B rows are not per-face quads, see mesh.create_mesh_3d)
+        from .mesh import bconns_3d_faces
+        bconns = bconns_3d_faces(*mc.num_elem)
     nn = node_coords.shape[0]
     h = mc.domain_size[0] / mc.num_elem[0]
     bconn = nvec = gamma_d = U_d = None
