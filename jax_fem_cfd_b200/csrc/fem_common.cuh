@@ -172,7 +172,7 @@ __device__ __forceinline__ bool fem_watchdog_fired(const int* err) {
 
 struct FemSync {
   unsigned int* count;    // arrivals in the current barrier generation
-  unsigned int* team_count;  // arrivals at the coarse-level team barrier (SubTeam)
+  unsigned int* team_count;  // arrivals at the coarse-level team barrier (GridTeam::team)
   int* err;               // sticky error flags (FEM_ERR_*)
   double* partials;       // [slot][cta] partial sums
   int nslots;
@@ -236,6 +236,27 @@ __device__ __forceinline__ void fem_stage(double* dst, const double* src, int n,
     }
   } else {
     for (int q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[idx(q)];
+  }
+}
+// Row-wise staging of an SH x SW region: dst[r * SW + c] = src[rowbase(r) + colx(c)].
+// Each thread owns one column (its wrapped / clamped x is computed once) and
+// walks rows, so an element costs one multiply-add instead of a full 2D
+// index decomposition.
+template <class RowBase, class ColX>
+__device__ __forceinline__ void fem_stage_2d(double* dst, const double* src, int SW, int SH, const RowBase& rowbase,
+                                             const ColX& colx) {
+  if (src == nullptr) return;
+  const int tpr = blockDim.x / SW;  // rows in flight per pass
+  const int c = threadIdx.x % SW, r0 = threadIdx.x / SW;
+  if (r0 >= tpr) return;
+  const int gx = colx(c);
+  if (__isGlobal(src)) {
+    for (int r = r0; r < SH; r += tpr) {
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + r * SW + c);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src + rowbase(r) + gx) : "memory");
+    }
+  } else {
+    for (int r = r0; r < SH; r += tpr) dst[r * SW + c] = src[rowbase(r) + gx];
   }
 }
 __device__ __forceinline__ void fem_stage_wait() {
@@ -332,36 +353,31 @@ __device__ __forceinline__ bool fem_counter_barrier(const FemSync* s, unsigned i
   return s_ok != 0;
 }
 
-// Every CTA of the launch (cooperative, all co-resident).
+// A set of CTAs that synchronise on one arrival counter: every CTA of the
+// launch (grid(): cooperative, all co-resident), or the first n CTAs (team():
+// the coarse multigrid levels, with their own counter). One type for both, so
+// the phase functions are compiled once.
 struct GridTeam {
   const FemSync* s;     // the launch's barrier state (shared-memory copy of the kernel arguments)
-  unsigned int* round;  // per-CTA count of completed grid barriers (shared memory, thread 0, starts at 0)
-  __device__ __forceinline__ int rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
-  __device__ __forceinline__ int size() const { return gridDim.x * blockDim.x; }
-  __device__ __forceinline__ int cta() const { return blockIdx.x; }
-  __device__ __forceinline__ int ncta() const { return gridDim.x; }
-  __device__ bool sync() const { return fem_counter_barrier(s, s->count, round, gridDim.x, 31); }
-  // reduce K values into K partial slots and sync, in one step (smem: 16*K doubles)
-  template <int K>
-  __device__ bool reduce_sync(double (&v)[K], const int (&slots)[K], double* smem) const {
-    return fem_counter_barrier(s, s->count, round, gridDim.x, 31, FemPartials<K>{v, slots}, smem);
+  unsigned int* cnt;    // arrival counter (global)
+  unsigned int* round;  // per-CTA count of completed barriers on cnt (shared memory, thread 0, starts at 0)
+  int n;                // CTAs taking part: blockIdx.x < n
+  unsigned int tag;     // trace tag of its barriers
+  __device__ static GridTeam grid(const FemSync* s, unsigned int* round) {
+    return GridTeam{s, s->count, round, (int)gridDim.x, 31u};
   }
-};
-
-// The first n CTAs of the launch (the coarse multigrid levels), with their own
-// arrival counter; the other CTAs do not take part.
-struct SubTeam {
-  const FemSync* s;
-  unsigned int* round;  // per-CTA count of completed team barriers (shared memory)
-  int n;
+  __device__ static GridTeam team(const FemSync* s, unsigned int* round, int n) {
+    return GridTeam{s, s->team_count, round, n, 30u};
+  }
   __device__ __forceinline__ int rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
   __device__ __forceinline__ int size() const { return n * blockDim.x; }
   __device__ __forceinline__ int cta() const { return blockIdx.x; }
   __device__ __forceinline__ int ncta() const { return n; }
-  __device__ bool sync() const { return fem_counter_barrier(s, s->team_count, round, n, 30); }
+  __device__ bool sync() const { return fem_counter_barrier(s, cnt, round, n, tag); }
+  // reduce K values into K partial slots and sync, in one step (smem: 16*K doubles)
   template <int K>
   __device__ bool reduce_sync(double (&v)[K], const int (&slots)[K], double* smem) const {
-    return fem_counter_barrier(s, s->team_count, round, n, 30, FemPartials<K>{v, slots}, smem);
+    return fem_counter_barrier(s, cnt, round, n, tag, FemPartials<K>{v, slots}, smem);
   }
 };
 

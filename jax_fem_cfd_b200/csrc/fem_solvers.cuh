@@ -277,8 +277,17 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
       }
       return gy * ux + gx;
     };
-    fem_stage(su, u, NS, fidx);
-    fem_stage(sx, iDv, NS, fidx);
+    auto rowb = [&](int r) -> int {
+      int gy = fy0 - R + r;
+      gy = g.periodic ? fem_wrap(gy, uy) : (gy < 0 ? 0 : (gy >= uy ? uy - 1 : gy));
+      return gy * ux;
+    };
+    auto colx = [&](int c) -> int {
+      const int gx = fx0 - R + c;
+      return g.periodic ? fem_wrap(gx, ux) : (gx < 0 ? 0 : (gx >= ux ? ux - 1 : gx));
+    };
+    fem_stage_2d(su, u, SW, SH, rowb, colx);
+    fem_stage_2d(sx, iDv, SW, SH, rowb, colx);
     fem_stage(sci, C.invD, CTX * CTY, [&](int q) -> int {
       const int ky = q / CTX, kx = q - ky * CTX;
       const int Rr = min(R0 + ky, cuy - 1), Cc = min(C0 + kx, cux - 1);
@@ -540,8 +549,17 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
       const int ty = q >> 5, x = min(x0 + (q & 31), ux - 1), y = min(y0 + ty, uy - 1);
       return y * ux + x;
     };
-    fem_stage(sy, L.x, NS, fidx);
-    if (pinned) fem_stage(sw, L.winvD, NS, fidx);
+    auto rowb = [&](int r) -> int {
+      int fr = gy0 + r;
+      fr = per ? fem_wrap(fr, uy) : (fr < 0 ? 0 : (fr >= uy ? uy - 1 : fr));
+      return fr * ux;
+    };
+    auto colx = [&](int c) -> int {
+      const int fc = gx0 + c;
+      return per ? fem_wrap(fc, ux) : (fc < 0 ? 0 : (fc >= ux ? ux - 1 : fc));
+    };
+    fem_stage_2d(sy, L.x, SX, SY, rowb, colx);
+    if (pinned) fem_stage_2d(sw, L.winvD, SX, SY, rowb, colx);
     fem_stage(sc, C.t, CXB * CYB, [&](int q) -> int {
       const int i = q / CXB, j = q - i * CXB;
       int cr = cr0 + i, cc = cc0 + j;
@@ -621,7 +639,7 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
 
 // Full V-cycle on r = lv[0].r; result in lv[0].t (raw; mean-zero subtracts
 // SL_X(0)[0]/nn lazily). Levels < block_from run on the whole grid; levels from
-// block_from down run on the team of the first A.team CTAs (SubTeam barriers,
+// block_from down run on the team of the first A.team CTAs (GridTeam::team barriers,
 // data in global memory), the coarsest solve in CTA 0. Grid-produced sums are
 // read over all CTA columns; team phases write only the team's columns (the
 // rest of those slots stay zero), so the same reads stay exact.
@@ -632,7 +650,7 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
   for (int n = 0; n < s; ++n)
     if (!mg_down<KIND>(gt, gr, A, n, smem)) return false;
   if ((int)blockIdx.x < A.team) {
-    const SubTeam tt{gt.s, team_round, A.team};
+    const GridTeam tt = GridTeam::team(gt.s, team_round, A.team);
     for (int n = s; n < N - 1; ++n)
       if (!mg_down<KIND>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 7);

@@ -389,8 +389,22 @@ __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid&
       if (D3) gz = gz < 0 ? 0 : (gz >= g.nnz ? g.nnz - 1 : gz);
       return (gz * g.nny + gy) * g.nnx + gx;
     };
+    if constexpr (D3) {
 #pragma unroll
-    for (int k = 0; k < NSRC; ++k) fem_stage(sm + k * NS, src[k], NS, gidx);
+      for (int k = 0; k < NSRC; ++k) fem_stage(sm + k * NS, src[k], NS, gidx);
+    } else {
+      auto rowb = [&](int r) -> int {
+        int gy = y0 + r;
+        gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
+        return gy * g.nnx;
+      };
+      auto colx = [&](int c) -> int {
+        const int gx = x0 + c;
+        return g.periodic ? fem_wrap(gx, g.nnx) : (gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx));
+      };
+#pragma unroll
+      for (int k = 0; k < NSRC; ++k) fem_stage_2d(sm + k * NS, src[k], SX, SY, rowb, colx);
+    }
     if (t == tm.cta()) pre();
     fem_stage_wait();
     for (int s = threadIdx.x; s < NS; s += blockDim.x) {

@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
   __shared__ unsigned int s_round;
   if (threadIdx.x == 0) s_round = 0u;
   fem_trace_init(A.sync);
-  const GridTeam gt{&A.sync, &s_round};
+  const GridTeam gt = GridTeam::grid(&A.sync, &s_round);
   const GridReducer gr{&A.sync};
   const int nn = A.g.nn;
   const size_t N = nn;

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
     s_round = 0u;
     s_team_round = 0u;
   }
-  const GridTeam gt{&A.sync, &s_round};
+  const GridTeam gt = GridTeam::grid(&A.sync, &s_round);
   const GridReducer gr{&A.sync};
   const MgLevel& L0 = A.lv[0];
   const FemGrid& g = L0.g;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double
     s_round = 0u;
     s_team_round = 0u;
   }
-  const GridTeam gt{&A.sync, &s_round};
+  const GridTeam gt = GridTeam::grid(&A.sync, &s_round);
   const GridReducer gr{&A.sync};
   const MgLevel& L0 = A.lv[0];
   const int nn = L0.g.nn;
