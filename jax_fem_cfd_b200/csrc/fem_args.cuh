@@ -2,6 +2,7 @@
 #pragma once
 #include <stdint.h>
 #include "fem_solvers.cuh"
+#include "fem_conv.cuh"
 
 #define FEM_THREADS 512
 #define FEM_OP_THREADS 256
@@ -25,6 +26,11 @@ struct BiArgs {
   int maxiter;
   int* iters;
   int* status;
+  // convection applied from Gauss-point factors (fem_conv.cuh) instead of op.B:
+  // op.B is then unused and the operator is op.alpha op.A + cv_coef Ce
+  const double* cvf;
+  double cv_coef;
+  FemQuadTab qt;
 };
 
 struct StepArgs {
@@ -33,6 +39,7 @@ struct StepArgs {
   double dt, rho, mu, theta;
   const double *Me, *Le, *Ge, *M;  // shared element matrices and lumped mass
   const double* Ce;
+  const double* vcv;                // if set: (mu Le + rho Ce) U_n, precomputed (Ce is then unused)
   const uint8_t* dmask;             // ndim*nn
   const uint8_t* pmask;             // nn (pinned pressure)
   int pinned;
@@ -75,6 +82,11 @@ int fem_launch_dot(const double* x, const double* y, int n, double* part, double
 int fem_launch_axpby(double a, const double* x, double b, double* y, int n, cudaStream_t s);
 int fem_launch_scatter(const int64_t* idx, const double* vals, double value, int n, double* out, cudaStream_t s);
 int fem_launch_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cudaStream_t s);
+
+int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,
+                            cudaStream_t s);
+int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc,
+                          double alpha, const double* Ash, const double* x, double* y, cudaStream_t s);
 
 int fem_coop_occupancy_cg(int* occ);
 int fem_coop_occupancy_bi(int* occ);

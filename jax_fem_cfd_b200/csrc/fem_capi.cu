@@ -121,6 +121,10 @@ struct fem_ctx {
   double *rhsU = nullptr, *Uhat = nullptr, *gPn = nullptr, *Ustar = nullptr, *rhsP = nullptr;  // step
   double *Ce = nullptr, *Ce2 = nullptr, *Ct = nullptr, *Mt = nullptr, *Ek = nullptr, *tau = nullptr;  // per element
   double *dotpart = nullptr, *Fe = nullptr;
+  double* vcv = nullptr;   // (mu Le + rho Ce(U_n)) U_n of the on-the-fly step (ndim*nn)
+  double* cvf = nullptr;   // Gauss-point factors of Ce(U_n) (3 nq per element, structure of arrays)
+  FemQuadTab qt{};         // Gauss table of the mesh (2D), for on-the-fly convection
+  int conv_otf = 0;        // fem_step4 applies Ce without building it (2D kinds)
   int Fe_cap = 0;
   int* flags = nullptr;  // device scratch ints
   // optional stage timing
@@ -245,7 +249,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
                   c->rhsU, c->Uhat, c->gPn, c->Ustar, c->rhsP, c->Ce, c->Ce2, c->Ct, c->Mt, c->Ek, c->tau,
-                  c->dotpart, c->Fe, c->flags};
+                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
@@ -302,6 +306,8 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
                      &c->Ustar})
     FEM_ALLOC(*p, vn);
   FEM_ALLOC(c->Ce, (size_t)g.ne * per);
+  FEM_ALLOC(c->vcv, vn);
+  if (g.kind != FEM_HEX8) FEM_ALLOC(c->cvf, (size_t)3 * c->nq * g.ne);
   FEM_ALLOC(c->dotpart, 4096);
   cudaStream_t s = 0;
   FEM_CHECK(cudaMemset(c->bar, 0, 2 * sizeof(unsigned int)));
@@ -336,6 +342,23 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   FEM_TRY(fem_launch_invdiag(g.nn, c->Ldiag, c->pmask, L0.invD, L0.winvD, s));
   c->nlev = 1;
   FEM_CHECK(cudaDeviceSynchronize());
+  // Gauss table for the on-the-fly convection of fem_step4 (2D kinds)
+  if (g.kind != FEM_HEX8 && c->nq <= FEM_QT_MAX && nen <= FEM_QT_MAX) {
+    double hw[FEM_QT_MAX], hN[FEM_QT_MAX * FEM_QT_MAX], hdN[2 * FEM_QT_MAX * FEM_QT_MAX];
+    FEM_CHECK(cudaMemcpy(hw, c->wq, sizeof(double) * c->nq, cudaMemcpyDeviceToHost));
+    FEM_CHECK(cudaMemcpy(hN, c->N, sizeof(double) * c->nq * nen, cudaMemcpyDeviceToHost));
+    FEM_CHECK(cudaMemcpy(hdN, c->dN, sizeof(double) * c->nq * 2 * nen, cudaMemcpyDeviceToHost));
+    for (int q = 0; q < c->nq; ++q) {
+      c->qt.w[q] = hw[q];
+      for (int b = 0; b < nen; ++b) {
+        c->qt.N[q][b] = hN[q * nen + b];
+        c->qt.dx[q][b] = hdN[(q * 2 + 0) * nen + b];
+        c->qt.dy[q][b] = hdN[(q * 2 + 1) * nen + b];
+      }
+    }
+    const char* ev = getenv("FEM_CONV_OTF");
+    c->conv_otf = (ev && atoi(ev) == 0) ? 0 : 1;
+  }
   return FEM_OK;
 }
 
@@ -707,7 +730,8 @@ extern "C" int fem_mg_vcycle(fem_ctx* c, const double* r, double* z, cudaStream_
 }
 
 static int run_bicgstab(fem_ctx* c, int ncomp, const MatCombo& op, const uint8_t* mask, const double* b, double* x,
-                        double tol, double atol, int maxiter, int* iters, int* status, cudaStream_t s) {
+                        double tol, double atol, int maxiter, int* iters, int* status, cudaStream_t s,
+                        const double* cvf = nullptr, double cv_coef = 0.0) {
   if (ncomp < 1 || ncomp > c->ndim) return FEM_E_ARG;  // workspace holds ndim*nn per vector
   BiArgs A;
   memset(&A, 0, sizeof(A));
@@ -729,6 +753,9 @@ static int run_bicgstab(fem_ctx* c, int ncomp, const MatCombo& op, const uint8_t
   A.maxiter = maxiter > 0 ? maxiter : 10 * ncomp * c->g.nn;  // utils/jax_iterative_solvers.py:181-183
   A.iters = iters;
   A.status = status;
+  A.cvf = cvf;
+  A.cv_coef = cv_coef;
+  A.qt = c->qt;
   FEM_TRY(reset_sync(c, s));
   return fem_launch_bicgstab(ncomp, A, ctx_grid_for(c, c->g.nn), s);
 }
@@ -754,8 +781,15 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   const double theta = 0.5;
   c->nev = 0;
   stage_mark(c, s);
-  // 1. Ce(U_n), beta = 1/2 (solvers/standard.py:152)
-  FEM_TRY(fem_launch_convection(g, quad_of(c), Un, 0.5, 0, c->Ce, s));
+  // 1. Ce(U_n), beta = 1/2 (solvers/standard.py:152). On-the-fly (2D): Ce is
+  // never built; instead (mu Le + rho Ce) U_n of the momentum rhs is applied here.
+  const bool otf = c->conv_otf && c->cvf && g.kind != FEM_HEX8 && nd == 2;
+  if (otf) {
+    FEM_TRY(fem_launch_conv_factors(g, c->qt, Un, 0.5, c->cvf, s));
+    FEM_TRY(fem_launch_conv_apply(2, g, c->qt, c->cvf, rho, mu, c->Le, Un, c->vcv, s));
+  } else {
+    FEM_TRY(fem_launch_convection(g, quad_of(c), Un, 0.5, 0, c->Ce, s));
+  }
   stage_mark(c, s);
   // 2. momentum rhs, x0 and G P_n (solvers/standard.py:31-37)
   StepArgs S;
@@ -769,7 +803,8 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   S.Le = c->Le;
   S.Ge = c->Ge;
   S.M = c->M;
-  S.Ce = c->Ce;
+  S.Ce = otf ? nullptr : c->Ce;
+  S.vcv = otf ? c->vcv : nullptr;
   S.dmask = c->has_dmask ? c->dmask : nullptr;
   S.pmask = c->pmask;
   S.pinned = c->set_zeroP;
@@ -777,8 +812,13 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   // 3. BiCGSTAB on (rho/dt) Me + theta (rho Ce + mu Le), identity rows on gamma_d (:20-28, :41)
   FEM_TRY(fem_launch_lincomb(nen * nen, rho / dt, c->Me, theta * mu, c->Le, c->Kd, s));
   stage_mark(c, s);
-  const MatCombo op{c->Kd, 1.0, c->Ce, theta * rho, 0, nullptr, 0.0};
-  FEM_TRY(run_bicgstab(c, nd, op, S.dmask, c->rhsU, c->Uhat, tol, 0.0, 0, iters, status, s));
+  if (otf) {
+    const MatCombo op{c->Kd, 1.0, nullptr, 0.0, 0, nullptr, 0.0};
+    FEM_TRY(run_bicgstab(c, nd, op, S.dmask, c->rhsU, c->Uhat, tol, 0.0, 0, iters, status, s, c->cvf, theta * rho));
+  } else {
+    const MatCombo op{c->Kd, 1.0, c->Ce, theta * rho, 0, nullptr, 0.0};
+    FEM_TRY(run_bicgstab(c, nd, op, S.dmask, c->rhsU, c->Uhat, tol, 0.0, 0, iters, status, s));
+  }
   stage_mark(c, s);
   // 4. U* = U_hat + (dt/rho) G P_n / M (:156)
   FEM_TRY(fem_launch_ustar(nd * g.nn, dt / rho, c->Uhat, c->gPn, c->M, c->Ustar, s));

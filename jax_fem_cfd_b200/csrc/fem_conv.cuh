@@ -1,0 +1,206 @@
+// Convection operator applied without materialising Ce. The conservative
+// convection element matrix of core/element_calc.py:165-185,
+//   Ce_e[a][b] = sum_q w_q N_a(q) (u_q . grad N_b(q)) + beta sum_q w_q N_a(q) (div u)_q N_b(q),
+// acts on an element vector x_e as
+//   (Ce_e x_e)_a = sum_q w_q N_a(q) [ u_q . grad x_q + beta (div u)_q x_q ],
+// with u_q, (div u)_q, x_q and grad x_q interpolated at the Gauss points from the
+// element's nodal values. u is fixed for a whole solve, so its Gauss-point
+// factors (27 doubles per Q2 element instead of Ce's 81) are formed once and every
+// operator apply interpolates only x. The mesh is uniform, so one table of Gauss
+// weights, shape functions and physical derivatives serves every element; it is
+// passed by value in the kernel parameters.
+#pragma once
+#include "fem_stencil.cuh"
+
+#define FEM_QT_MAX 9
+struct FemQuadTab {
+  double w[FEM_QT_MAX];
+  double N[FEM_QT_MAX][FEM_QT_MAX];   // [q][node]
+  double dx[FEM_QT_MAX][FEM_QT_MAX];  // d N_node / dx at q
+  double dy[FEM_QT_MAX][FEM_QT_MAX];  // d N_node / dy at q
+};
+
+template <int KIND>
+struct KQ;
+template <>
+struct KQ<FEM_Q1_2D> {
+  static constexpr int NQ = 4;
+};
+template <>
+struct KQ<FEM_Q2_2D> {
+  static constexpr int NQ = 9;
+};
+
+// Gauss-point factors of Ce(u) for one element (2D kinds): for each point q,
+// f[3q] = w_q u_q, f[3q+1] = w_q v_q, f[3q+2] = w_q beta (div u)_q, so that
+// (Ce x)_a = sum_q N_a(q) (f[3q] dx x_q + f[3q+1] dy x_q + f[3q+2] x_q).
+template <int KIND>
+__device__ __forceinline__ void fem_conv_factors(const FemQuadTab& T, const double (&ux)[KI<KIND>::NEN],
+                                                 const double (&uy)[KI<KIND>::NEN], double bd,
+                                                 double (&f)[3 * KQ<KIND>::NQ]) {
+  constexpr int NEN = KI<KIND>::NEN, NQ = KQ<KIND>::NQ;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double uqx = 0.0, uqy = 0.0, div = 0.0;
+#pragma unroll
+    for (int b = 0; b < NEN; ++b) {
+      uqx += T.N[q][b] * ux[b];
+      uqy += T.N[q][b] * uy[b];
+      div += T.dx[q][b] * ux[b] + T.dy[q][b] * uy[b];
+    }
+    f[3 * q] = T.w[q] * uqx;
+    f[3 * q + 1] = T.w[q] * uqy;
+    f[3 * q + 2] = T.w[q] * (bd * div);
+  }
+}
+
+// y_a = cc (Ce x)_a + alpha (Ash x)_a for one element from its Gauss-point
+// factors (fac(k) = factor k of this element). The Gauss-point loop is not
+// unrolled (indexed table reads): that keeps only x, the accumulators and one
+// point's temporaries live, which the 128-register budget of the persistent
+// solver allows without spills.
+template <int KIND, class Fac>
+__device__ __forceinline__ void fem_conv_element(const FemQuadTab& T, const double (&xl)[KI<KIND>::NEN],
+                                                 const Fac& fac, double cc, double alpha, const double* Ash,
+                                                 double (&y)[KI<KIND>::NEN]) {
+  constexpr int NEN = KI<KIND>::NEN, NQ = KQ<KIND>::NQ;
+  double acc[NEN];
+#pragma unroll
+  for (int a = 0; a < NEN; ++a) acc[a] = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < NQ; ++q) {
+    double xq = 0.0, gx = 0.0, gy = 0.0;
+#pragma unroll
+    for (int b = 0; b < NEN; ++b) {
+      xq += T.N[q][b] * xl[b];
+      gx += T.dx[q][b] * xl[b];
+      gy += T.dy[q][b] * xl[b];
+    }
+    const double sq = (fac(3 * q) * gx + fac(3 * q + 1) * gy) + fac(3 * q + 2) * xq;
+#pragma unroll
+    for (int a = 0; a < NEN; ++a) acc[a] += T.N[q][a] * sq;
+  }
+#pragma unroll
+  for (int a = 0; a < NEN; ++a) {
+    double sh = 0.0;
+    if (Ash) {
+#pragma unroll
+      for (int b = 0; b < NEN; ++b) sh += Ash[a * NEN + b] * xl[b];
+    }
+    y[a] = alpha * sh + cc * acc[a];
+  }
+}
+
+// Local node index of element-local lattice offset (i, j) (inverse of kdi/kdj).
+template <int KIND>
+__device__ __forceinline__ int fem_local_node(int i, int j) {
+  if (KIND == FEM_Q2_2D) {
+    // quad9 order: (0,0) (1,0) (2,0) (2,1) (2,2) (1,2) (0,2) (0,1) (1,1)
+    constexpr int t[9] = {0, 1, 2, 7, 8, 3, 6, 5, 4};
+    return t[j * 3 + i];
+  }
+  constexpr int t[4] = {0, 1, 3, 2};  // quad4: (0,0) (1,0) (1,1) (0,1)
+  return t[j * 2 + i];
+}
+
+// Smem doubles of fem_tiled_conv for NC components and blockDim threads.
+__host__ __device__ constexpr int fem_conv_smem(int kind, int nc, int threads) {
+  return (kind == FEM_Q2_2D)
+             ? nc * (32 + 4) * (threads / 32 + 4) + (31 / 2 + 2) * ((threads / 32 - 1) / 2 + 2) * nc * 9
+             : nc * (32 + 2) * (threads / 32 + 2) + (31 + 2) * ((threads / 32 - 1) + 2) * nc * 4;
+}
+
+// Tiled application of y = alpha Ash x + cc Ce x (2D, NC components of x given by
+// load(node, c); Ce through its Gauss-point factors fq, structure of arrays
+// fq[k * ne + e], k < 3 NQ). For each 32 x (blockDim/32) tile of owned nodes: x
+// on the tile plus its halo is staged in smem, every element touching the tile
+// computes its rows for all components once (elements on tile borders are
+// computed by both tiles), and each owned node sums the rows of its incident
+// elements in a fixed order: body(n, y[NC], x_center[NC]). Deterministic, no
+// atomics.
+template <int KIND, int NC, class Team, class Load, class Body>
+__device__ __forceinline__ void fem_tiled_conv(const Team& tm, const FemGrid& g, double* __restrict__ sm,
+                                               const Load& load, const double* __restrict__ fq, const FemQuadTab& T,
+                                               double cc, double alpha, const double* Ash, const Body& body) {
+  static_assert(KIND != FEM_HEX8, "2D kinds only");
+  constexpr int R = KI<KIND>::R, S = KI<KIND>::S, NEN = KI<KIND>::NEN;
+  const int TY = blockDim.x >> 5;
+  const int SX = 32 + 2 * R, SY = TY + 2 * R, NS = SX * SY;
+  const int EX = 31 / S + 2, EY = (TY - 1) / S + 2, NE = EX * EY;
+  double* sx = sm;              // NC * NS
+  double* sy = sx + NC * NS;    // NE * NC * NEN
+  const size_t ne = g.ne;
+  const int ntx = (g.nnx + 31) >> 5, nty = (g.nny + TY - 1) / TY, ntile = ntx * nty;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int t = tm.cta(); t < ntile; t += tm.ncta()) {
+    const int by = t / ntx, bx = t - by * ntx;
+    const int x0 = bx * 32 - R, y0 = by * TY - R;
+    for (int s = threadIdx.x; s < NS; s += blockDim.x) {
+      const int ly = s / SX, lx = s - ly * SX;
+      int gx = x0 + lx, gy = y0 + ly;
+      if (g.periodic) {
+        gx = fem_wrap(gx, g.nnx);
+        gy = fem_wrap(gy, g.nny);
+      } else {
+        gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
+        gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);
+      }
+      const int j = gy * g.nnx + gx;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sx[c * NS + s] = load(j, c);
+    }
+    __syncthreads();
+    // element rows: element (ex0 + lex, ey0 + ley), its node (i, j) at staged
+    // (R - S + S lex + i, R - S + S ley + j)
+    const int ex0 = bx * 32 / S - 1, ey0 = by * TY / S - 1;
+    for (int w = threadIdx.x; w < NE * NC; w += blockDim.x) {
+      const int el = w % NE, c = w / NE;
+      const int ley = el / EX, lex = el - ley * EX;
+      const int ex = ex0 + lex, ey = ey0 + ley;
+      double y[NEN];
+      if (g.periodic || (ex >= 0 && ex < g.nex && ey >= 0 && ey < g.ney)) {
+        const size_t e = (size_t)fem_wrap(ey, g.ney) * g.nex + fem_wrap(ex, g.nex);
+        const int base = (R - S + S * ley) * SX + (R - S + S * lex);
+        double xl[NEN];
+#pragma unroll
+        for (int b = 0; b < NEN; ++b) xl[b] = sx[c * NS + base + kdj<KIND>(b) * SX + kdi<KIND>(b)];
+        fem_conv_element<KIND>(T, xl, [&](int k) { return __ldg(fq + k * ne + e); }, cc, alpha, Ash, y);
+      } else {
+#pragma unroll
+        for (int a = 0; a < NEN; ++a) y[a] = 0.0;
+      }
+#pragma unroll
+      for (int a = 0; a < NEN; ++a) sy[(el * NC + c) * NEN + a] = y[a];
+    }
+    __syncthreads();
+    const int x = bx * 32 + tx, yy = by * TY + ty;
+    if (x < g.nnx && yy < g.nny) {
+      double v[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[c] = 0.0;
+      // incident elements: node local (tx, ty) is element-local (i, j) of element
+      // lex = (tx + S - i) / S, ley = (ty + S - j) / S when divisible
+#pragma unroll
+      for (int j = 0; j <= S; ++j) {
+        if ((ty + S - j) % S) continue;
+        const int ley = (ty + S - j) / S, ey = ey0 + ley;
+        if (!g.periodic && (ey < 0 || ey >= g.ney)) continue;
+#pragma unroll
+        for (int i = 0; i <= S; ++i) {
+          if ((tx + S - i) % S) continue;
+          const int lex = (tx + S - i) / S, ex = ex0 + lex;
+          if (!g.periodic && (ex < 0 || ex >= g.nex)) continue;
+          const int el = ley * EX + lex, a = fem_local_node<KIND>(i, j);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) v[c] += sy[(el * NC + c) * NEN + a];
+        }
+      }
+      double ctr[NC];
+      const int cen = (ty + R) * SX + tx + R;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) ctr[c] = sx[c * NS + cen];
+      body(yy * g.nnx + x, v, ctr);
+    }
+    __syncthreads();
+  }
+}

@@ -1,4 +1,5 @@
 // Persistent cooperative BiCGSTAB kernel on element-by-element operators.
+#include "fem_b200.h"
 #include "fem_args.cuh"
 
 
@@ -14,11 +15,23 @@ __device__ __forceinline__ void bi_apply(const BiArgs& A, const MatCombo& op, in
   }
 }
 
-template <int KIND, int NC>
-__global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
+// The operator apply of the solver: the element-by-element product of op, or
+// (OTF) op.alpha op.A + cv_coef Ce from Gauss-point factors, Ce never materialised.
+template <int KIND, int NC, bool OTF, class Team, class Load, class Body>
+__device__ __forceinline__ void bi_tiled_apply(const Team& tm, const BiArgs& A, const MatCombo& op, double* tsm,
+                                               const Load& load, const Body& body) {
+  if constexpr (OTF) {
+    fem_tiled_conv<KIND, NC>(tm, A.g, tsm, load, A.cvf, A.qt, A.cv_coef, op.alpha, op.A, body);
+  } else {
+    fem_tiled_ebe<KIND, NC>(tm, A.g, tsm, load, op, body);
+  }
+}
+
+template <int KIND, int NC, bool OTF>
+__global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_constant__ BiArgs A) {
   __shared__ double smem[128];
   __shared__ double sAsh[81];
-  __shared__ double tsm[3 * 1836];
+  extern __shared__ double tsm[];  // staging of the tiled operator (dynamic)
   MatCombo op = A.op;
   if (op.A) {
     for (int t = threadIdx.x; t < KI<KIND>::NEN * KI<KIND>::NEN; t += blockDim.x) sAsh[t] = op.A[t];
@@ -38,7 +51,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
   {
     {
       double a[2] = {0.0, 0.0};
-      fem_tiled_ebe<KIND, NC>(gt, A.g, tsm, [&](int j, int c) { return A.x[j + c * N]; }, op,
+      bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, [&](int j, int c) { return A.x[j + c * N]; },
                               [&](int i, const double(&Ax)[NC], const double(&xc)[NC]) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
@@ -79,7 +92,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
           return r[o] + beta * (pold[o] - omega * qold[o]);
         };
         double a[1] = {0.0};
-        fem_tiled_ebe<KIND, NC>(gt, A.g, tsm, pn, op, [&](int i, const double(&qv)[NC], const double(&pc)[NC]) {
+        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, pn, [&](int i, const double(&qv)[NC], const double(&pc)[NC]) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
             const size_t o = i + c * N;
@@ -101,7 +114,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(BiArgs A) {
       };
       {
         double a[3] = {0.0, 0.0, 0.0};
-        fem_tiled_ebe<KIND, NC>(gt, A.g, tsm, sv, op, [&](int i, const double(&tvv)[NC], const double(&sc)[NC]) {
+        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, sv, [&](int i, const double(&tvv)[NC], const double(&sc)[NC]) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
             const size_t o = i + c * N;
@@ -171,33 +184,52 @@ done:
 
 
 
-static const void* bi_fn(int kind, int ncomp) {
-  if (kind == FEM_Q1_2D) return ncomp == 1 ? (const void*)k_bicgstab<FEM_Q1_2D, 1> : (const void*)k_bicgstab<FEM_Q1_2D, 2>;
-  if (kind == FEM_Q2_2D) return ncomp == 1 ? (const void*)k_bicgstab<FEM_Q2_2D, 1> : (const void*)k_bicgstab<FEM_Q2_2D, 2>;
-  return ncomp == 1 ? (const void*)k_bicgstab<FEM_HEX8, 1> : (const void*)k_bicgstab<FEM_HEX8, 3>;
+static const void* bi_fn(int kind, int ncomp, bool otf) {
+  if (otf) return kind == FEM_Q1_2D ? (const void*)k_bicgstab<FEM_Q1_2D, 2, true>
+                                    : (const void*)k_bicgstab<FEM_Q2_2D, 2, true>;
+  if (kind == FEM_Q1_2D)
+    return ncomp == 1 ? (const void*)k_bicgstab<FEM_Q1_2D, 1, false> : (const void*)k_bicgstab<FEM_Q1_2D, 2, false>;
+  if (kind == FEM_Q2_2D)
+    return ncomp == 1 ? (const void*)k_bicgstab<FEM_Q2_2D, 1, false> : (const void*)k_bicgstab<FEM_Q2_2D, 2, false>;
+  return ncomp == 1 ? (const void*)k_bicgstab<FEM_HEX8, 1, false> : (const void*)k_bicgstab<FEM_HEX8, 3, false>;
+}
+// dynamic smem (doubles) of the tiled operator: the EBE gather of fem_tiled_ebe
+// needs NC (32+2R)(16+2R)(3 in 3D); the on-the-fly convection fem_conv_smem
+static int bi_smem_doubles(int kind, int ncomp, bool otf) {
+  if (otf) return fem_conv_smem(kind, 2, FEM_THREADS);
+  return 3 * 1836;
 }
 
 int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s) {
   BiArgs a = A;
   void* args[] = {&a};
+  const bool otf = A.cvf != nullptr;
+  if (otf && (A.g.kind == FEM_HEX8 || ncomp != 2)) return FEM_E_ARG;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(FEM_THREADS);
   cfg.stream = s;
+  cfg.dynamicSmemBytes = (size_t)bi_smem_doubles(A.g.kind, ncomp, otf) * sizeof(double);
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeCooperative;
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  cudaLaunchKernelExC(&cfg, bi_fn(A.g.kind, ncomp), args);
+  cudaLaunchKernelExC(&cfg, bi_fn(A.g.kind, ncomp, otf), args);
   return fem_after_launch("k_bicgstab");
 }
 int fem_coop_occupancy_bi(int* occ) {
   int m = 1 << 30;
   for (int kind = 0; kind < 3; ++kind)
-    for (int nc = 1; nc <= 2; ++nc) {
+    for (int v = 0; v < 3; ++v) {
+      const bool otf = (v == 2);
+      if (otf && kind == FEM_HEX8) continue;
+      const int nc = otf ? 2 : v + 1;
+      const void* fn = bi_fn(kind, nc, otf);
+      const int dyn = bi_smem_doubles(kind, nc, otf) * (int)sizeof(double);
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) return -1;
       int a = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, bi_fn(kind, nc), FEM_THREADS, 0) != cudaSuccess) return -1;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, fn, FEM_THREADS, dyn) != cudaSuccess) return -1;
       m = a < m ? a : m;
     }
   *occ = m;

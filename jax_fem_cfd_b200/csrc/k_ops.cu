@@ -1,4 +1,5 @@
 // Element-product, element-matrix, transfer, boundary and blas-1 kernels.
+#include "fem_b200.h"
 #include "fem_args.cuh"
 
 
@@ -325,4 +326,85 @@ int fem_launch_scatter(const int64_t* idx, const double* vals, double value, int
 int fem_launch_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cudaStream_t s) {
   k_make_mask<<<fem_nblocks(n, 256), 256, 0, s>>>(idx, n, len, mask);
   return fem_after_launch("k_make_mask");
+}
+
+// ------------------------------------------------- on-the-fly convection ----
+// Gauss-point factors of Ce(U) (fem_conv_factors), one thread per element,
+// structure of arrays fq[k * ne + e].
+template <int KIND>
+__global__ void __launch_bounds__(256) k_conv_factors(FemGrid g, const __grid_constant__ FemQuadTab qt,
+                                                      const double* __restrict__ U, double bd,
+                                                      double* __restrict__ fq) {
+  constexpr int NEN = KI<KIND>::NEN, NQ = KQ<KIND>::NQ, S = KI<KIND>::S;
+  const size_t nn = g.nn, ne = g.ne;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.ne; e += gridDim.x * blockDim.x) {
+    const int ey = e / g.nex, ex = e - ey * g.nex;
+    double ux[NEN], uy[NEN];
+#pragma unroll
+    for (int b = 0; b < NEN; ++b) {
+      int i = S * ex + kdi<KIND>(b), j = S * ey + kdj<KIND>(b);
+      if (g.periodic) {
+        i = i >= g.nnx ? i - g.nnx : i;
+        j = j >= g.nny ? j - g.nny : j;
+      }
+      const size_t n = (size_t)j * g.nnx + i;
+      ux[b] = U[n];
+      uy[b] = U[n + nn];
+    }
+    double f[3 * NQ];
+    fem_conv_factors<KIND>(qt, ux, uy, bd, f);
+#pragma unroll
+    for (int k = 0; k < 3 * NQ; ++k) fq[k * ne + e] = f[k];
+  }
+}
+
+// y = alpha Ash x + cc Ce x over the whole lattice, one tile per CTA.
+template <int KIND, int NC>
+__global__ void __launch_bounds__(FEM_THREADS) k_conv_apply(FemGrid g, const __grid_constant__ FemQuadTab qt,
+                                                            const double* __restrict__ fq, double cc, double alpha,
+                                                            const double* __restrict__ Ash,
+                                                            const double* __restrict__ x, double* __restrict__ y) {
+  extern __shared__ double sm[];
+  __shared__ double sA[81];
+  constexpr int NEN = KI<KIND>::NEN;
+  if (Ash)
+    for (int t = threadIdx.x; t < NEN * NEN; t += blockDim.x) sA[t] = Ash[t];
+  __syncthreads();
+  const size_t nn = g.nn;
+  struct Tiles {
+    __device__ __forceinline__ int cta() const { return blockIdx.x; }
+    __device__ __forceinline__ int ncta() const { return gridDim.x; }
+  } tm;
+  fem_tiled_conv<KIND, NC>(tm, g, sm, [&](int j, int c) { return x[j + c * nn]; }, fq, qt, cc, alpha,
+                           Ash ? sA : nullptr, [&](int i, const double(&v)[NC], const double(&)[NC]) {
+#pragma unroll
+                             for (int c = 0; c < NC; ++c) y[i + c * nn] = v[c];
+                           });
+}
+
+int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,
+                            cudaStream_t s) {
+  if (g.kind == FEM_HEX8) return FEM_E_ARG;
+  const int nb = fem_nblocks(g.ne, 256);
+  if (g.kind == FEM_Q1_2D)
+    k_conv_factors<FEM_Q1_2D><<<nb, 256, 0, s>>>(g, qt, U, bd, fq);
+  else
+    k_conv_factors<FEM_Q2_2D><<<nb, 256, 0, s>>>(g, qt, U, bd, fq);
+  return fem_after_launch("k_conv_factors");
+}
+
+int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc,
+                          double alpha, const double* Ash, const double* x, double* y, cudaStream_t s) {
+  if (g.kind == FEM_HEX8 || ncomp != 2) return FEM_E_ARG;
+  const int ty = FEM_THREADS / 32;
+  const int ntile = ((g.nnx + 31) / 32) * ((g.nny + ty - 1) / ty);
+  const int dyn = fem_conv_smem(g.kind, 2, FEM_THREADS) * (int)sizeof(double);
+  if (g.kind == FEM_Q1_2D) {
+    cudaFuncSetAttribute(k_conv_apply<FEM_Q1_2D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    k_conv_apply<FEM_Q1_2D, 2><<<ntile, FEM_THREADS, dyn, s>>>(g, qt, fq, cc, alpha, Ash, x, y);
+  } else {
+    cudaFuncSetAttribute(k_conv_apply<FEM_Q2_2D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    k_conv_apply<FEM_Q2_2D, 2><<<ntile, FEM_THREADS, dyn, s>>>(g, qt, fq, cc, alpha, Ash, x, y);
+  }
+  return fem_after_launch("k_conv_apply");
 }

@@ -20,7 +20,12 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_mom_rhs(StepArgs S, const do
     fem_ij(g, n, ix, iy, iz);
     double ms[ND], v[ND], gp[ND];
     fem_gather_k<KIND, ND>(g, ix, iy, iz, ms_m, src, ms);
-    fem_gather_k<KIND, ND>(g, ix, iy, iz, vc, src, v);
+    if (S.vcv) {
+#pragma unroll
+      for (int c = 0; c < ND; ++c) v[c] = S.vcv[n + c * N];
+    } else {
+      fem_gather_k<KIND, ND>(g, ix, iy, iz, vc, src, v);
+    }
     fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return Pn[j]; }, gp);
 #pragma unroll
     for (int c = 0; c < ND; ++c) {
