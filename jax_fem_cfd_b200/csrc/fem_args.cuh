@@ -86,7 +86,7 @@ int fem_launch_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cuda
 int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,
                             cudaStream_t s);
 int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc,
-                          double alpha, const double* Ash, const double* x, double* y, cudaStream_t s);
+                          double alpha, const double* Ash, const double* x, double* y, int grid, cudaStream_t s);
 
 int fem_coop_occupancy_cg(int* occ);
 int fem_coop_occupancy_bi(int* occ);

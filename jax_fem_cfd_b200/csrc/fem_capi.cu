@@ -786,7 +786,7 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   const bool otf = c->conv_otf && c->cvf && g.kind != FEM_HEX8 && nd == 2;
   if (otf) {
     FEM_TRY(fem_launch_conv_factors(g, c->qt, Un, 0.5, c->cvf, s));
-    FEM_TRY(fem_launch_conv_apply(2, g, c->qt, c->cvf, rho, mu, c->Le, Un, c->vcv, s));
+    FEM_TRY(fem_launch_conv_apply(2, g, c->qt, c->cvf, rho, mu, c->Le, Un, c->vcv, c->sms, s));
   } else {
     FEM_TRY(fem_launch_convection(g, quad_of(c), Un, 0.5, 0, c->Ce, s));
   }

@@ -103,51 +103,76 @@ __device__ __forceinline__ int fem_local_node(int i, int j) {
   return t[j * 2 + i];
 }
 
-// Smem doubles of fem_tiled_conv for NC components and blockDim threads.
-__host__ __device__ constexpr int fem_conv_smem(int kind, int nc, int threads) {
-  return (kind == FEM_Q2_2D)
-             ? nc * (32 + 4) * (threads / 32 + 4) + (31 / 2 + 2) * ((threads / 32 - 1) / 2 + 2) * nc * 9
-             : nc * (32 + 2) * (threads / 32 + 2) + (31 + 2) * ((threads / 32 - 1) + 2) * nc * 4;
-}
+// Dynamic smem of fem_tiled_conv (doubles); the tile height adapts to it.
+#define FEM_CONV_SMEM 16384
 
-// Tiled application of y = alpha Ash x + cc Ce x (2D, NC components of x given by
-// load(node, c); Ce through its Gauss-point factors fq, structure of arrays
-// fq[k * ne + e], k < 3 NQ). For each 32 x (blockDim/32) tile of owned nodes: x
-// on the tile plus its halo is staged in smem, every element touching the tile
-// computes its rows for all components once (elements on tile borders are
-// computed by both tiles), and each owned node sums the rows of its incident
-// elements in a fixed order: body(n, y[NC], x_center[NC]). Deterministic, no
-// atomics.
-template <int KIND, int NC, class Team, class Load, class Body>
+// Tiled application of y = alpha Ash x + cc Ce x (2D, NC components). x is
+// comb(s, v) of NSRC source vectors (v[k] = src[k][c*nn + node] at staged point
+// s), Ce enters through its Gauss-point factors fq (structure of arrays
+// fq[k * ne + e], k < 3 NQ). Each CTA takes one tile of 32 x TY owned nodes (TY
+// even, chosen so one round of tiles covers the lattice, capped by
+// FEM_CONV_SMEM): the sources on the tile plus its halo are staged by cp.async
+// and combined in smem, every element touching the tile computes its rows for
+// all components once (border elements are computed by both tiles), and each
+// owned node sums the rows of its incident elements in a fixed order:
+// body(n, y[NC], x_center[NC]). Deterministic, no atomics. pre() runs once per
+// CTA while the first tile's copies are in flight.
+template <int KIND, int NC, int NSRC, class Team, class Comb, class Body, class Pre = FemNoHook>
 __device__ __forceinline__ void fem_tiled_conv(const Team& tm, const FemGrid& g, double* __restrict__ sm,
-                                               const Load& load, const double* __restrict__ fq, const FemQuadTab& T,
-                                               double cc, double alpha, const double* Ash, const Body& body) {
+                                               const double* const (&src)[NSRC], const Comb& comb,
+                                               const double* __restrict__ fq, const FemQuadTab& T, double cc,
+                                               double alpha, const double* Ash, const Body& body,
+                                               const Pre& pre = Pre()) {
   static_assert(KIND != FEM_HEX8, "2D kinds only");
   constexpr int R = KI<KIND>::R, S = KI<KIND>::S, NEN = KI<KIND>::NEN;
-  const int TY = blockDim.x >> 5;
-  const int SX = 32 + 2 * R, SY = TY + 2 * R, NS = SX * SY;
-  const int EX = 31 / S + 2, EY = (TY - 1) / S + 2, NE = EX * EY;
-  double* sx = sm;              // NC * NS
-  double* sy = sx + NC * NS;    // NE * NC * NEN
-  const size_t ne = g.ne;
-  const int ntx = (g.nnx + 31) >> 5, nty = (g.nny + TY - 1) / TY, ntile = ntx * nty;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  constexpr int SX = 32 + 2 * R, EX = 31 / S + 2;
+  const int WR = blockDim.x >> 5;
+  const int ntx = (g.nnx + 31) >> 5;
+  // tile height: a multiple of S, one round of tiles, within FEM_CONV_SMEM
+  auto need = [&](int ty) {
+    const int ns = SX * (ty + 2 * R), ne_t = EX * ((ty - 1) / S + 2);
+    const int a = NSRC * NC * ns, b = NC * ns + ne_t * NC * NEN;
+    return a > b ? a : b;
+  };
+  int TY;
+  {
+    int nty_t = tm.ncta() / ntx;
+    if (nty_t < 1) nty_t = 1;
+    TY = (g.nny + nty_t - 1) / nty_t;
+    TY = ((TY + S - 1) / S) * S;
+    while (TY > S && need(TY) > FEM_CONV_SMEM) TY -= S;
+  }
+  const int SY = TY + 2 * R, NS = SX * SY;
+  const int EY = (TY - 1) / S + 2, NE = EX * EY;
+  double* sx = sm;              // NC * NS: the combined x (over the first source's slots)
+  double* sy = sx + NC * NS;    // NE * NC * NEN element rows (over the other sources' slots)
+  const size_t nn = g.nn, ne = g.ne;
+  const int nty = (g.nny + TY - 1) / TY, ntile = ntx * nty;
+  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
   for (int t = tm.cta(); t < ntile; t += tm.ncta()) {
     const int by = t / ntx, bx = t - by * ntx;
     const int x0 = bx * 32 - R, y0 = by * TY - R;
-    for (int s = threadIdx.x; s < NS; s += blockDim.x) {
-      const int ly = s / SX, lx = s - ly * SX;
-      int gx = x0 + lx, gy = y0 + ly;
-      if (g.periodic) {
-        gx = fem_wrap(gx, g.nnx);
-        gy = fem_wrap(gy, g.nny);
-      } else {
-        gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
-        gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);
-      }
-      const int j = gy * g.nnx + gx;
+    auto rowb = [&](int r) -> int {
+      int gy = y0 + r;
+      gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
+      return gy * g.nnx;
+    };
+    auto colx = [&](int c) -> int {
+      const int gx = x0 + c;
+      return g.periodic ? fem_wrap(gx, g.nnx) : (gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx));
+    };
 #pragma unroll
-      for (int c = 0; c < NC; ++c) sx[c * NS + s] = load(j, c);
+    for (int k = 0; k < NSRC; ++k)
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        fem_stage_2d(sm + (k * NC + c) * NS, src[k] ? src[k] + c * nn : nullptr, SX, SY, rowb, colx);
+    if (t == tm.cta()) pre();
+    fem_stage_wait();
+    for (int s = threadIdx.x; s < NC * NS; s += blockDim.x) {
+      double v[NSRC];
+#pragma unroll
+      for (int k = 0; k < NSRC; ++k) v[k] = sm[k * NC * NS + s];
+      sx[s] = comb(s, v);
     }
     __syncthreads();
     // element rows: element (ex0 + lex, ey0 + ley), its node (i, j) at staged
@@ -173,34 +198,37 @@ __device__ __forceinline__ void fem_tiled_conv(const Team& tm, const FemGrid& g,
       for (int a = 0; a < NEN; ++a) sy[(el * NC + c) * NEN + a] = y[a];
     }
     __syncthreads();
-    const int x = bx * 32 + tx, yy = by * TY + ty;
-    if (x < g.nnx && yy < g.nny) {
-      double v[NC];
+    for (int ty = ty0; ty < TY; ty += WR) {
+      const int x = bx * 32 + tx, yy = by * TY + ty;
+      if (x < g.nnx && yy < g.nny) {
+        double v[NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) v[c] = 0.0;
-      // incident elements: node local (tx, ty) is element-local (i, j) of element
-      // lex = (tx + S - i) / S, ley = (ty + S - j) / S when divisible
+        for (int c = 0; c < NC; ++c) v[c] = 0.0;
+        // incident elements: node local (tx, ty) is element-local (i, j) of element
+        // lex = (tx + S - i) / S, ley = (ty + S - j) / S when divisible
 #pragma unroll
-      for (int j = 0; j <= S; ++j) {
-        if ((ty + S - j) % S) continue;
-        const int ley = (ty + S - j) / S, ey = ey0 + ley;
-        if (!g.periodic && (ey < 0 || ey >= g.ney)) continue;
+        for (int j = 0; j <= S; ++j) {
+          if ((ty + S - j) % S) continue;
+          const int ley = (ty + S - j) / S, ey = ey0 + ley;
+          if (!g.periodic && (ey < 0 || ey >= g.ney)) continue;
 #pragma unroll
-        for (int i = 0; i <= S; ++i) {
-          if ((tx + S - i) % S) continue;
-          const int lex = (tx + S - i) / S, ex = ex0 + lex;
-          if (!g.periodic && (ex < 0 || ex >= g.nex)) continue;
-          const int el = ley * EX + lex, a = fem_local_node<KIND>(i, j);
+          for (int i = 0; i <= S; ++i) {
+            if ((tx + S - i) % S) continue;
+            const int lex = (tx + S - i) / S, ex = ex0 + lex;
+            if (!g.periodic && (ex < 0 || ex >= g.nex)) continue;
+            const int el = ley * EX + lex, a = fem_local_node<KIND>(i, j);
 #pragma unroll
-          for (int c = 0; c < NC; ++c) v[c] += sy[(el * NC + c) * NEN + a];
+            for (int c = 0; c < NC; ++c) v[c] += sy[(el * NC + c) * NEN + a];
+          }
         }
-      }
-      double ctr[NC];
-      const int cen = (ty + R) * SX + tx + R;
+        double ctr[NC];
+        const int cen = (ty + R) * SX + tx + R;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) ctr[c] = sx[c * NS + cen];
-      body(yy * g.nnx + x, v, ctr);
+        for (int c = 0; c < NC; ++c) ctr[c] = sx[c * NS + cen];
+        body(yy * g.nnx + x, v, ctr);
+      }
     }
     __syncthreads();
   }
+  if (tm.cta() >= ntile) pre();
 }

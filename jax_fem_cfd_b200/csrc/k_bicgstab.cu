@@ -15,13 +15,15 @@ __device__ __forceinline__ void bi_apply(const BiArgs& A, const MatCombo& op, in
   }
 }
 
-// The operator apply of the solver: the element-by-element product of op, or
-// (OTF) op.alpha op.A + cv_coef Ce from Gauss-point factors, Ce never materialised.
-template <int KIND, int NC, bool OTF, class Team, class Load, class Body>
+// The operator apply of the solver: the element-by-element product of op on
+// load(j, c), or (OTF) op.alpha op.A + cv_coef Ce from Gauss-point factors on
+// comb of the staged sources (Ce never materialised).
+template <int KIND, int NC, bool OTF, int NSRC, class Team, class Load, class Comb, class Body>
 __device__ __forceinline__ void bi_tiled_apply(const Team& tm, const BiArgs& A, const MatCombo& op, double* tsm,
-                                               const Load& load, const Body& body) {
+                                               const Load& load, const double* const (&src)[NSRC],
+                                               const Comb& comb, const Body& body) {
   if constexpr (OTF) {
-    fem_tiled_conv<KIND, NC>(tm, A.g, tsm, load, A.cvf, A.qt, A.cv_coef, op.alpha, op.A, body);
+    fem_tiled_conv<KIND, NC, NSRC>(tm, A.g, tsm, src, comb, A.cvf, A.qt, A.cv_coef, op.alpha, op.A, body);
   } else {
     fem_tiled_ebe<KIND, NC>(tm, A.g, tsm, load, op, body);
   }
@@ -51,7 +53,9 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_consta
   {
     {
       double a[2] = {0.0, 0.0};
-      bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, [&](int j, int c) { return A.x[j + c * N]; },
+      const double* sx0[1] = {A.x};
+      bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, [&](int j, int c) { return A.x[j + c * N]; }, sx0,
+                                    [](int, const double(&v)[1]) { return v[0]; },
                               [&](int i, const double(&Ax)[NC], const double(&xc)[NC]) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
@@ -92,7 +96,10 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_consta
           return r[o] + beta * (pold[o] - omega * qold[o]);
         };
         double a[1] = {0.0};
-        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, pn, [&](int i, const double(&qv)[NC], const double(&pc)[NC]) {
+        const double* spn[3] = {r, pold, qold};
+        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, pn, spn,
+                                      [&](int, const double(&v)[3]) { return v[0] + beta * (v[1] - omega * v[2]); },
+                                      [&](int i, const double(&qv)[NC], const double(&pc)[NC]) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
             const size_t o = i + c * N;
@@ -114,7 +121,9 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_consta
       };
       {
         double a[3] = {0.0, 0.0, 0.0};
-        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, sv, [&](int i, const double(&tvv)[NC], const double(&sc)[NC]) {
+        const double* ssv[2] = {r, qnew};
+        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, sv, ssv,
+                                      [&](int, const double(&v)[2]) { return v[0] - alpha_ * v[1]; }, [&](int i, const double(&tvv)[NC], const double(&sc)[NC]) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
             const size_t o = i + c * N;
@@ -196,7 +205,7 @@ static const void* bi_fn(int kind, int ncomp, bool otf) {
 // dynamic smem (doubles) of the tiled operator: the EBE gather of fem_tiled_ebe
 // needs NC (32+2R)(16+2R)(3 in 3D); the on-the-fly convection fem_conv_smem
 static int bi_smem_doubles(int kind, int ncomp, bool otf) {
-  if (otf) return fem_conv_smem(kind, 2, FEM_THREADS);
+  if (otf) return FEM_CONV_SMEM;
   return 3 * 1836;
 }
 

@@ -375,8 +375,9 @@ __global__ void __launch_bounds__(FEM_THREADS) k_conv_apply(FemGrid g, const __g
     __device__ __forceinline__ int cta() const { return blockIdx.x; }
     __device__ __forceinline__ int ncta() const { return gridDim.x; }
   } tm;
-  fem_tiled_conv<KIND, NC>(tm, g, sm, [&](int j, int c) { return x[j + c * nn]; }, fq, qt, cc, alpha,
-                           Ash ? sA : nullptr, [&](int i, const double(&v)[NC], const double(&)[NC]) {
+  const double* src[1] = {x};
+  fem_tiled_conv<KIND, NC, 1>(tm, g, sm, src, [](int, const double(&v)[1]) { return v[0]; }, fq, qt, cc, alpha,
+                              Ash ? sA : nullptr, [&](int i, const double(&v)[NC], const double(&)[NC]) {
 #pragma unroll
                              for (int c = 0; c < NC; ++c) y[i + c * nn] = v[c];
                            });
@@ -394,11 +395,10 @@ int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double
 }
 
 int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc,
-                          double alpha, const double* Ash, const double* x, double* y, cudaStream_t s) {
-  if (g.kind == FEM_HEX8 || ncomp != 2) return FEM_E_ARG;
-  const int ty = FEM_THREADS / 32;
-  const int ntile = ((g.nnx + 31) / 32) * ((g.nny + ty - 1) / ty);
-  const int dyn = fem_conv_smem(g.kind, 2, FEM_THREADS) * (int)sizeof(double);
+                          double alpha, const double* Ash, const double* x, double* y, int grid, cudaStream_t s) {
+  if (g.kind == FEM_HEX8 || ncomp != 2 || grid < 1) return FEM_E_ARG;
+  const int ntile = grid;  // one tile per CTA (tile height adapts to the grid)
+  const int dyn = FEM_CONV_SMEM * (int)sizeof(double);
   if (g.kind == FEM_Q1_2D) {
     cudaFuncSetAttribute(k_conv_apply<FEM_Q1_2D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     k_conv_apply<FEM_Q1_2D, 2><<<ntile, FEM_THREADS, dyn, s>>>(g, qt, fq, cc, alpha, Ash, x, y);
