@@ -125,14 +125,17 @@ def cg_algorithmic_bytes(level_nn, iters, block_from):
     return total * w
 
 
-def bicgstab_algorithmic_bytes(nn, ne, nen, ndim, iters):
-    """k_bicgstab: per operator apply the per-element Ce (ne*nen^2) plus the
-    vectors of the phase; 3 phases per iteration (see fem_solvers kernels)."""
+def bicgstab_algorithmic_bytes(nn, ne, nen, ndim, iters, nq=9):
+    """k_bicgstab with the on-the-fly convection operator: each operator apply
+    reads the Gauss-point factors of Ce(U_n) (3 nq per element, instead of Ce's
+    nen^2) plus the vectors of its phase; 3 phases per iteration (see the
+    kernel): apply on p (reads r, p_old, q_old, rhat; writes p, q), apply on s
+    (reads r, q; writes t), update (reads x, p, r, q, t, rhat; writes x, r)."""
     w = 8
     vec = ndim * nn
-    ce = ne * nen * nen
-    init = ce + 6 * vec
-    per_it = (ce + 6 * vec) + (ce + 4 * vec) + 7 * vec
+    fac = 3 * nq * ne
+    init = fac + 6 * vec
+    per_it = (fac + 6 * vec) + (fac + 3 * vec) + 8 * vec
     return (init + iters * per_it) * w
 
 
