@@ -221,21 +221,17 @@ __device__ __forceinline__ void fem_trace_mark(const FemSync& s, unsigned long l
   if (s.trace && blockIdx.x == 0 && threadIdx.x == 0) fem_trace_put(s.trace, s.trace_cap, tag);
 }
 
-// Shared-memory staging. fem_stage issues dst[q] = src[idx(q)] for q < n: by
-// 8-byte cp.async (no register round trip, every copy of the thread in flight)
-// when src is global memory, by plain copies when src is itself in shared
-// memory (the CTA-0 coarse levels). fem_stage_wait completes all of them and
-// makes them visible to the whole CTA.
+// Shared-memory staging from global memory. fem_stage issues dst[q] = src[idx(q)]
+// for q < n by 8-byte cp.async (no register round trip, every copy of the
+// thread in flight); fem_stage_wait completes all of them and makes them visible
+// to the whole CTA. Sources are global-memory vectors (one code path keeps the
+// persistent solvers' hot code small).
 template <class Idx>
 __device__ __forceinline__ void fem_stage(double* dst, const double* src, int n, const Idx& idx) {
   if (src == nullptr) return;  // unused source slot
-  if (__isGlobal(src)) {
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-      const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + q);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src + idx(q)) : "memory");
-    }
-  } else {
-    for (int q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[idx(q)];
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + q);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src + idx(q)) : "memory");
   }
 }
 // Row-wise staging of an SH x SW region: dst[r * SW + c] = src[rowbase(r) + colx(c)].
@@ -250,13 +246,9 @@ __device__ __forceinline__ void fem_stage_2d(double* dst, const double* src, int
   const int c = threadIdx.x % SW, r0 = threadIdx.x / SW;
   if (r0 >= tpr) return;
   const int gx = colx(c);
-  if (__isGlobal(src)) {
-    for (int r = r0; r < SH; r += tpr) {
-      const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + r * SW + c);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src + rowbase(r) + gx) : "memory");
-    }
-  } else {
-    for (int r = r0; r < SH; r += tpr) dst[r * SW + c] = src[rowbase(r) + gx];
+  for (int r = r0; r < SH; r += tpr) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + r * SW + c);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src + rowbase(r) + gx) : "memory");
   }
 }
 __device__ __forceinline__ void fem_stage_wait() {
