@@ -198,7 +198,7 @@ __device__ __forceinline__ LevelAffine fem_level_affine(const Red& red, const Cg
 // are staged in one batch; xh, t (on the region plus one node) and the
 // restriction are then formed from smem only. Each CTA writes x_n and sums t
 // only on the fine nodes its tile owns.
-template <int KIND, class Team, class Red>
+template <int KIND, bool PIN, class Team, class Red>
 __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArgs& A, int n, double* smem) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
   fem_trace_mark(A.sync, 15);
@@ -206,7 +206,7 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
   const MgLevel& C = A.lv[n + 1];
   const FemGrid& g = L.g;
   const int nn = g.nn;
-  const bool pinned = A.pinned;
+  constexpr bool pinned = PIN;  // A.pinned, fixed per kernel instantiation
   LevelAffine f{0.0, 0.0, 0.0};
   double mx = 0.0;
   bool have_f = pinned;
@@ -384,7 +384,7 @@ __device__ __noinline__ bool mg_down(const Team& tm, const Red& red, const CgArg
 // Coarsest level (solution written to L.t). Pinned: CG to coarse_tol with maxiter coarse_maxiter on
 // L with gamma_p rows zeroed (core/multigrid.py:278-287). Mean-zero: one Jacobi
 // sweep from zero (core/multigrid.py:289-301). Runs in CTA 0 (BlockTeam).
-template <int KIND, class Red>
+template <int KIND, bool PIN, class Red>
 __device__ __noinline__ void mg_coarse(const Red& red, const CgArgs& A, double* smem, double* cg_r, double* cg_p,
                                        double* cg_q) {
   const BlockTeam tm;
@@ -392,7 +392,7 @@ __device__ __noinline__ void mg_coarse(const Red& red, const CgArgs& A, double* 
   const MgLevel& L = A.lv[n];
   const FemGrid& g = L.g;
   const int nn = g.nn;
-  if (!A.pinned) {
+  if (!PIN) {
     const LevelAffine f = fem_level_affine(red, A, n, smem);
     const double mx = (2.0 / 3.0) * f.sum_rhD / nn;
     const int ux = L.lat.ux();
@@ -465,7 +465,7 @@ __device__ __forceinline__ void mg_xsums(const MgLevel& L, int i, double xi, dou
 // The prolongated iterate y = X_n + P X_{n+1} (- means, or 0 on gamma_p) is
 // formed in smem; the sweep then reads smem only. For n == 0 the result is
 // z = M r and the phase also accumulates the r.z pieces.
-template <int KIND, class Team, class Red>
+template <int KIND, bool PIN, class Team, class Red>
 __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs& A, int n, double* smem) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
   fem_trace_mark(A.sync, 14);
@@ -473,7 +473,7 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
   const MgLevel& C = A.lv[n + 1];
   const FemGrid& g = L.g;
   const int nn = g.nn;
-  const bool pinned = A.pinned;
+  constexpr bool pinned = PIN;  // A.pinned, fixed per kernel instantiation
   double mX = 0.0, mP = 0.0;
   LevelAffine f{0.0, 0.0, 0.0};
   bool have_m = pinned;
@@ -643,19 +643,19 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
 // data in global memory), the coarsest solve in CTA 0. Grid-produced sums are
 // read over all CTA columns; team phases write only the team's columns (the
 // rest of those slots stay zero), so the same reads stay exact.
-template <int KIND>
+template <int KIND, bool PIN>
 __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr, const CgArgs& A, double* smem,
                                        unsigned int* team_round, double* cg_r, double* cg_p, double* cg_q) {
   const int N = A.nlev, s = A.block_from;
   for (int n = 0; n < s; ++n)
-    if (!mg_down<KIND>(gt, gr, A, n, smem)) return false;
+    if (!mg_down<KIND, PIN>(gt, gr, A, n, smem)) return false;
   if ((int)blockIdx.x < A.team) {
     const GridTeam tt = GridTeam::team(gt.s, team_round, A.team);
     for (int n = s; n < N - 1; ++n)
-      if (!mg_down<KIND>(tt, gr, A, n, smem)) return false;
+      if (!mg_down<KIND, PIN>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 7);
     if (blockIdx.x == 0) {
-      mg_coarse<KIND>(gr, A, smem, cg_r, cg_p, cg_q);
+      mg_coarse<KIND, PIN>(gr, A, smem, cg_r, cg_p, cg_q);
       fem_trace_mark(A.sync, 8);
       const MgLevel& Lc = A.lv[N - 1];
       if (N == 1) {
@@ -666,7 +666,7 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
           a[1] += Lc.r[i] * Lc.t[i];
         }
         gr.reduce<2>(a, SL_X(0), smem);
-      } else if (!A.pinned) {
+      } else if (!PIN) {
         double a[2] = {0.0, 0.0};
         for (int i = threadIdx.x; i < Lc.g.nn; i += blockDim.x) mg_xsums(Lc, i, Lc.t[i], a);
         gr.reduce<2>(a, SL_X(N - 1), smem);
@@ -674,11 +674,11 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
     }
     if (!tt.sync()) return false;
     for (int n = N - 2; n >= s; --n)
-      if (!mg_up<KIND>(tt, gr, A, n, smem)) return false;
+      if (!mg_up<KIND, PIN>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 10);
   }
   if (!gt.sync()) return false;
   for (int n = s - 1; n >= 0; --n)
-    if (!mg_up<KIND>(gt, gr, A, n, smem)) return false;
+    if (!mg_up<KIND, PIN>(gt, gr, A, n, smem)) return false;
   return true;
 }

@@ -3,7 +3,7 @@
 
 
 // Preconditioner application z = M r; returns gamma = r . z.
-template <int KIND>
+template <int KIND, bool PIN>
 __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer& gr, const CgArgs& A, double* smem,
                               unsigned int* team_round, double* cg_r, double* cg_p, double* cg_q, double rr, double r2d,
                               double& gamma, double& mz, bool defer = false) {
@@ -19,9 +19,9 @@ __device__ __noinline__ bool cg_apply_prec(const GridTeam& gt, const GridReducer
     return true;
   }
   if (A.prec == FEM_PREC_MG) {
-    if (!mg_vcycle<KIND>(gt, gr, A, smem, team_round, cg_r, cg_p, cg_q)) return false;
+    if (!mg_vcycle<KIND, PIN>(gt, gr, A, smem, team_round, cg_r, cg_p, cg_q)) return false;
     if (defer) return true;  // the caller reads gamma and mz (cg_mg_results) later
-    if (A.pinned) {
+    if (PIN) {
       double s[2];
       gr.result<2>(s, SL_X(0), smem);
       gamma = s[1];
@@ -74,8 +74,9 @@ __device__ __forceinline__ void cg_mg_slots(int (&sl)[3]) {
   sl[1] = SL_X(0) + 1;
   sl[2] = SL_R(0);
 }
+template <bool PIN>
 __device__ __forceinline__ void cg_mg_from(const CgArgs& A, const double (&s)[3], double& gamma, double& mz) {
-  if (A.pinned) {
+  if (PIN) {
     gamma = s[1];
     mz = 0.0;
   } else {
@@ -84,7 +85,7 @@ __device__ __forceinline__ void cg_mg_from(const CgArgs& A, const double (&s)[3]
   }
 }
 
-template <int KIND>
+template <int KIND, bool PIN>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q) {
   // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables
   extern __shared__ double smem[];
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
   const MgLevel& L0 = A.lv[0];
   const FemGrid& g = L0.g;
   const int nn = g.nn;
-  const uint8_t* pin0 = A.pinned ? L0.pin : nullptr;
+  const uint8_t* pin0 = PIN ? L0.pin : nullptr;
   const double* __restrict__ D = L0.diag;
   int k = 0;
   double rr = 0.0;
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
     rr = bb_rr[1];
     const double atol2 = fmax(A.tol * A.tol * bb_rr[0], A.atol * A.atol);
     double gamma, mz;
-    if (!cg_apply_prec<KIND>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q, rr, r2d[0], gamma, mz)) goto done;
+    if (!cg_apply_prec<KIND, PIN>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q, rr, r2d[0], gamma, mz)) goto done;
     double beta = 0.0;
     bool have_p = false;
     bool pending = false;  // MG: gamma / mz of the last V-cycle are read in the next phase A
@@ -182,7 +183,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
           if (!pending) return;
           double s3[3], gamma_;
           gr.result_end<3>(mpend, s3, smem);
-          cg_mg_from(A, s3, gamma_, mz);
+          cg_mg_from<PIN>(A, s3, gamma_, mz);
           beta = gamma_ / gamma;
           gamma = gamma_;
           pending = false;
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
       } else {
         if (!(rr > atol2 && k < A.maxiter)) break;  // z of a final iteration is never used
         const bool defer = (prec == FEM_PREC_MG);
-        if (!cg_apply_prec<KIND>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q, rr, t1[0], gamma_, mz, defer))
+        if (!cg_apply_prec<KIND, PIN>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q, rr, t1[0], gamma_, mz, defer))
           goto done;
         pending = defer;
       }
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
     }
     // final modification of solvers/standard.py:119-123
     if (A.post) {
-      if (A.pinned) {
+      if (PIN) {
         for (int i = gt.rank(); i < nn; i += gt.size())
           if (pin0 && pin0[i]) A.x[i] = 0.0;
       } else {
@@ -296,7 +297,7 @@ done:
 
 
 
-template <int KIND>
+template <int KIND, bool PIN>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q,
                                                             double* z) {
   // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables
@@ -324,10 +325,10 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double
   }
   gr.reduce<2>(a, SL_R(0), smem);
   if (!gt.sync()) return;
-  if (!mg_vcycle<KIND>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q)) return;
+  if (!mg_vcycle<KIND, PIN>(gt, gr, A, smem, &s_team_round, cg_r, cg_p, cg_q)) return;
   double sx[2];
   gr.result<2>(sx, SL_X(0), smem);
-  const double mz = A.pinned ? 0.0 : sx[0] * L0.inv_nn;
+  const double mz = PIN ? 0.0 : sx[0] * L0.inv_nn;
   for (int i = gt.rank(); i < nn; i += gt.size()) z[i] = L0.t[i] - mz;
 }
 
@@ -346,45 +347,47 @@ static int coop_launch(const void* fn, int grid, void** args, cudaStream_t s, co
   return fem_after_launch(what);
 }
 
-static const void* cg_fn(int kind) {
-  return kind == FEM_Q1_2D ? (const void*)k_cg<FEM_Q1_2D>
-                           : (kind == FEM_Q2_2D ? (const void*)k_cg<FEM_Q2_2D> : (const void*)k_cg<FEM_HEX8>);
+// kernels by element kind and pressure mode (pinned gamma_p rows or mean-zero)
+template <bool PIN>
+static const void* cg_fn_p(int kind) {
+  return kind == FEM_Q1_2D ? (const void*)k_cg<FEM_Q1_2D, PIN>
+                           : (kind == FEM_Q2_2D ? (const void*)k_cg<FEM_Q2_2D, PIN> : (const void*)k_cg<FEM_HEX8, PIN>);
 }
-static const void* vc_fn(int kind) {
-  return kind == FEM_Q1_2D ? (const void*)k_vcycle<FEM_Q1_2D>
-                           : (kind == FEM_Q2_2D ? (const void*)k_vcycle<FEM_Q2_2D> : (const void*)k_vcycle<FEM_HEX8>);
+template <bool PIN>
+static const void* vc_fn_p(int kind) {
+  return kind == FEM_Q1_2D ? (const void*)k_vcycle<FEM_Q1_2D, PIN>
+                           : (kind == FEM_Q2_2D ? (const void*)k_vcycle<FEM_Q2_2D, PIN>
+                                                : (const void*)k_vcycle<FEM_HEX8, PIN>);
 }
+static const void* cg_fn(int kind, int pinned) { return pinned ? cg_fn_p<true>(kind) : cg_fn_p<false>(kind); }
+static const void* vc_fn(int kind, int pinned) { return pinned ? vc_fn_p<true>(kind) : vc_fn_p<false>(kind); }
 int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq};
-  return coop_launch(cg_fn(A.lv[0].g.kind), grid, args, s, "k_cg",
+  return coop_launch(cg_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_cg",
                      (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * sizeof(double));
 }
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq, &z};
-  return coop_launch(vc_fn(A.lv[0].g.kind), grid, args, s, "k_vcycle",
+  return coop_launch(vc_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_vcycle",
                      (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * sizeof(double));
 }
 int fem_coop_occupancy_cg(int* occ) {
   int m = 1 << 30;
-  for (int kind = 0; kind < 3; ++kind) {
-    // allow the dynamic smem of the tile buffer and the stencil tables
-    if (cudaFuncSetAttribute(cg_fn(kind), cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_DYN_SMEM_MAX) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(vc_fn(kind), cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_DYN_SMEM_MAX) !=
-            cudaSuccess)
-      return -1;
-    int a = 0, b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, cg_fn(kind), FEM_THREADS, FEM_DYN_SMEM_MAX) !=
-        cudaSuccess)
-      return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, vc_fn(kind), FEM_THREADS, FEM_DYN_SMEM_MAX) !=
-        cudaSuccess)
-      return -1;
-    m = a < m ? a : m;
-    m = b < m ? b : m;
-  }
+  for (int kind = 0; kind < 3; ++kind)
+    for (int pin = 0; pin < 2; ++pin) {
+      const void* fns[2] = {cg_fn(kind, pin), vc_fn(kind, pin)};
+      for (const void* fn : fns) {
+        // allow the dynamic smem of the tile buffer and the stencil tables
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_DYN_SMEM_MAX) != cudaSuccess)
+          return -1;
+        int a = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, fn, FEM_THREADS, FEM_DYN_SMEM_MAX) != cudaSuccess)
+          return -1;
+        m = a < m ? a : m;
+      }
+    }
   *occ = m;
   return 0;
 }
