@@ -431,7 +431,7 @@ def main():
         "e2e": {"value": whole_job_rate(world, K, r["e2e_ms"]), "unit": "steps/s", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"]},
         "gpu_launches": int(r["launches"]),
-        "roofline": {"kernel": "k_cg (persistent MG-PCG pressure solve)", "bound": "hbm",
+        "roofline": {"kernel": "k_cg<1,0> (persistent MG-PCG pressure solve, Q2, mean-zero)", "bound": "hbm",
                      "achieved": cg_bytes / (cg_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": cg_bytes / (cg_ms * 1e-3) / 1e9 / hbm, "traffic": traffic,
                      "algorithmic_bytes_per_launch": cg_bytes, "avg_launch_ms": cg_ms,
