@@ -82,7 +82,6 @@ static FemLattice lattice_of(const FemGrid& g) {
   return L;
 }
 
-#define FEM_TAB_MAX (64 * 27)
 
 struct CtxLevel {
   FemGrid g;
@@ -123,6 +122,7 @@ struct fem_ctx {
   double *dotpart = nullptr, *Fe = nullptr;
   double* vcv = nullptr;   // (mu Le + rho Ce(U_n)) U_n of the on-the-fly step (ndim*nn)
   double* cvf = nullptr;   // Gauss-point factors of Ce(U_n) (3 nq per element, structure of arrays)
+  double* ebe_tab = nullptr;  // stencil table of the shared matrix of fem_ebe_apply
   FemQuadTab qt{};         // Gauss table of the mesh (2D), for on-the-fly convection
   int conv_otf = 0;        // fem_step4 applies Ce without building it (2D kinds)
   int Fe_cap = 0;
@@ -249,7 +249,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
                   c->rhsU, c->Uhat, c->gPn, c->Ustar, c->rhsP, c->Ce, c->Ce2, c->Ct, c->Mt, c->Ek, c->tau,
-                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf};
+                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
@@ -307,6 +307,7 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
     FEM_ALLOC(*p, vn);
   FEM_ALLOC(c->Ce, (size_t)g.ne * per);
   FEM_ALLOC(c->vcv, vn);
+  FEM_ALLOC(c->ebe_tab, FEM_TAB_MAX);
   if (g.kind != FEM_HEX8) FEM_ALLOC(c->cvf, (size_t)3 * c->nq * g.ne);
   FEM_ALLOC(c->dotpart, 4096);
   cudaStream_t s = 0;
@@ -559,6 +560,12 @@ extern "C" int fem_ebe_apply(fem_ctx* c, int ncomp, const double* x, double* y, 
                              double beta, const double* B, int transB, double gamma, const double* C,
                              cudaStream_t s) {
   if (!c || !x || !y || ncomp < 1 || ncomp > 3) return FEM_E_ARG;
+  if (A && !B && !C) {
+    // shared element matrix only: its assembled stencil (built on the device)
+    // applied by a tiled smem kernel, instead of the per-node element gather
+    FEM_TRY(fem_launch_stencil_build(c->g, A, 0, 0, c->ebe_tab, s));
+    return fem_launch_stencil_apply(ncomp, c->g, c->ebe_tab, alpha, x, y, c->sms, s);
+  }
   const MatCombo m{A, alpha, B, beta, transB, C, gamma};
   return fem_launch_ebe(ncomp, c->g, m, x, y, s);
 }

@@ -165,6 +165,8 @@ __device__ __forceinline__ int fem_axis_rep(int kind, int periodic, int cls, int
   return nel;
 }
 
+// largest stencil table (doubles): 3D hex8, 27 classes x 27 offsets, with room to spare
+#define FEM_TAB_MAX (64 * 27)
 __host__ __device__ __forceinline__ int fem_stencil_ncls(const FemGrid& g) {
   const int n = fem_axis_ncls(g.kind, g.periodic);
   return g.kind == FEM_HEX8 ? n * n * n : n * n;

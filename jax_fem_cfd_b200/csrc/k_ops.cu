@@ -236,6 +236,146 @@ __global__ void k_elem_combine(size_t n, double s_m, const double* __restrict__ 
     out[t] = s_m * Mt[t] + s_c * (C[t] + Ct[t]);
 }
 
+// y = alpha S x for an assembled stencil table S (fem_stencil.cuh), one tile of
+// 32 x (blockDim/32) nodes per CTA (3D: one plane), x staged in smem by cp.async.
+template <int KIND>
+__global__ void __launch_bounds__(512) k_stencil_apply(FemGrid g, const double* __restrict__ tab, double alpha,
+                                                       const double* __restrict__ x, double* __restrict__ y) {
+  extern __shared__ double sm[];
+  __shared__ double stab[FEM_TAB_MAX];
+  const int nt = fem_stencil_ncls(g) * KI<KIND>::NOFF;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) stab[t] = tab[t];
+  __syncthreads();
+  struct Tiles {
+    __device__ __forceinline__ int cta() const { return blockIdx.x; }
+    __device__ __forceinline__ int ncta() const { return gridDim.x; }
+  } tm;
+  const double* src[1] = {x};
+  fem_tiled_stencil<KIND, 1>(tm, g, stab, sm, src, [](int, const double(&v)[1]) { return v[0]; },
+                             [&](int n, int, int, int, double acc, double) { y[n] = alpha * acc; });
+}
+
+// Streaming y = alpha S x (2D kinds) in register strips: a warp owns 32 - 2R
+// node columns and M rows. Its 32 lanes load columns x0 - R .. x0 + 31 - R of
+// rows y0 - R .. y0 + M - 1 + R straight into registers (one coalesced load per
+// row and lane, all issued before any use), the horizontal neighbours come
+// from warp shuffles and each row feeds the W output rows it touches. Strips
+// clear of the top and bottom boundary rows of a Q1 lattice keep their column's
+// 9 coefficients in registers; the others read the table per row. The sum runs
+// over dy, then dx, in ascending order for every node.
+template <int KIND, int M>
+__global__ void __launch_bounds__(256, 3) k_stencil_strip(FemGrid g, const double* __restrict__ tab, double alpha,
+                                                          const double* __restrict__ x, double* __restrict__ y) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF, OW = 32 - 2 * R, NR = M + 2 * R;
+  __shared__ double stab[16 * NOFF];
+  const int nt = fem_stencil_ncls(g) * NOFF;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) stab[t] = tab[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int nc = fem_axis_ncls(KIND, g.periodic);
+  const int ntx = (g.nnx + OW - 1) / OW, nty = (g.nny + M - 1) / M;
+  const int nitem = ntx * nty;  // below nn: fits an int
+  const int wstep = (gridDim.x * blockDim.x) >> 5;
+  for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitem; it += wstep) {
+    const int by = it / ntx, bx = it - by * ntx;
+    const int xg = bx * OW + lane - R, y0 = by * M;
+    const int gx = g.periodic ? fem_wrap(xg, g.nnx) : (xg < 0 ? 0 : (xg >= g.nnx ? g.nnx - 1 : xg));
+    double v[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      int gy = y0 - R + r;
+      gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
+      v[r] = __ldg(x + (size_t)gy * g.nnx + gx);
+    }
+    const bool own = lane >= R && lane < 32 - R && xg < g.nnx;
+    const int cx = own ? fem_axis_cls(KIND, g.periodic, xg, g.nex) : 0;
+    double acc[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) acc[m] = 0.0;
+    const bool fast = KIND == FEM_Q1_2D && (g.periodic || (y0 >= 1 && y0 + M <= g.ney));
+    if (fast) {
+      const double* c = stab + ((g.periodic ? 0 : 1) * nc + cx) * NOFF;
+      double cf[NOFF];
+#pragma unroll
+      for (int o = 0; o < NOFF; ++o) cf[o] = c[o];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        double sh[W];
+        sh[R] = v[r];
+#pragma unroll
+        for (int d = 1; d <= R; ++d) {
+          sh[R + d] = __shfl_down_sync(0xffffffffu, v[r], d);
+          sh[R - d] = __shfl_up_sync(0xffffffffu, v[r], d);
+        }
+#pragma unroll
+        for (int dy = 0; dy < W; ++dy) {
+          const int m = r - dy;
+          if (m >= 0 && m < M) {
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx) acc[m] += cf[dy * W + dx] * sh[dx];
+          }
+        }
+      }
+    } else {
+      int crow[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int yg = y0 + m < g.nny ? y0 + m : g.nny - 1;
+        crow[m] = (fem_axis_cls(KIND, g.periodic, yg, g.ney) * nc + cx) * NOFF;
+      }
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        double sh[W];
+        sh[R] = v[r];
+#pragma unroll
+        for (int d = 1; d <= R; ++d) {
+          sh[R + d] = __shfl_down_sync(0xffffffffu, v[r], d);
+          sh[R - d] = __shfl_up_sync(0xffffffffu, v[r], d);
+        }
+#pragma unroll
+        for (int dy = 0; dy < W; ++dy) {
+          const int m = r - dy;
+          if (m >= 0 && m < M) {
+            const double* c = stab + crow[m] + dy * W;
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx) acc[m] += c[dx] * sh[dx];
+          }
+        }
+      }
+    }
+    if (own) {
+#pragma unroll
+      for (int m = 0; m < M; ++m)
+        if (y0 + m < g.nny) y[(size_t)(y0 + m) * g.nnx + xg] = alpha * acc[m];
+    }
+  }
+}
+
+int fem_launch_stencil_apply(int ncomp, const FemGrid& g, const double* tab, double alpha, const double* x, double* y,
+                             int sms, cudaStream_t s) {
+  for (int c = 0; c < ncomp; ++c) {
+    const size_t o = (size_t)c * g.nn;
+    if (g.kind == FEM_HEX8) {
+      constexpr int T = 512, TY = T / 32;
+      const int grid = ((g.nnx + 31) / 32) * ((g.nny + TY - 1) / TY) * g.nnz;
+      const int dyn = (32 + 2) * (TY + 2) * 3 * (int)sizeof(double);
+      k_stencil_apply<FEM_HEX8><<<grid, T, dyn, s>>>(g, tab, alpha, x + o, y + o);
+    } else {
+      constexpr int M = 8;
+      const int ow = (g.kind == FEM_Q2_2D) ? 28 : 30;
+      const long long nwarp = (long long)((g.nnx + ow - 1) / ow) * ((g.nny + M - 1) / M);
+      const long long need = (nwarp + 7) / 8;
+      const int grid = (int)(need < 3LL * sms ? need : 3LL * sms);
+      if (g.kind == FEM_Q1_2D)
+        k_stencil_strip<FEM_Q1_2D, M><<<grid, 256, 0, s>>>(g, tab, alpha, x + o, y + o);
+      else
+        k_stencil_strip<FEM_Q2_2D, M><<<grid, 256, 0, s>>>(g, tab, alpha, x + o, y + o);
+    }
+    if (int rc = fem_after_launch("k_stencil_apply")) return rc;
+  }
+  return 0;
+}
+
 int fem_launch_ebe(int ncomp, const FemGrid& g, const MatCombo& m, const double* x, double* y, cudaStream_t s) {
   const int nb = fem_nblocks(g.nn, FEM_OP_THREADS);
   FEM_KIND_DISPATCH(g.kind, K, {

@@ -55,6 +55,34 @@ def test_mesh_generation(fn, args):
             np.testing.assert_array_equal(np_(bc[f]), obc[f])
 
 
+@pytest.mark.parametrize("fn,args", [
+    ("create_mesh_2d", (67, 29, 2.0, 1.0)),          # 3 x 4 warp strips, interior fast path, ragged edges
+    ("create_mesh_2d", (2, 1, 1.0, 1.0)),            # one partial strip
+    ("create_mesh_2d", (30, 8, 1.0, 1.0)),           # ney < 9: boundary rows in every strip
+    ("create_mesh_2d_quad9", (17, 13, 1.0, 1.5)),
+    ("create_periodic_mesh_2d", (40, 20, 1.0, 1.0)),
+    ("create_periodic_mesh_2d", (3, 2, 1.0, 1.0)),   # lattice narrower than the strip halo
+    ("create_periodic_mesh_2d_quad9", (24, 10, 1.0, 1.0)),
+    ("create_mesh_3d", (9, 7, 5, 1.0, 1.0, 1.0)),
+])
+def test_shared_matrix_matvec(fn, args):
+    """Products with one shared non-symmetric element matrix (core/element_mult.py:11,38)
+    on lattices of several strips and tiles, two components, vs the oracle's
+    gather / dense product / scatter-add."""
+    from jax_fem_cfd_b200.core import element_mult as em
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from oracle import emult as oem
+    _, nconn, *_ = getattr(rm, fn)(*args)
+    cn = np_(nconn)
+    nn, nen = int(cn.max()) + 1, cn.shape[1]
+    rng = np.random.default_rng(nn)
+    A = rng.standard_normal((nen, nen))
+    x = rng.standard_normal(2 * nn)
+    y = em.consistent_mass_mult(torch.as_tensor(x).cuda(), torch.as_tensor(A).cuda(), nconn, nn, 2)
+    ref = np.concatenate([oem._shared(A, x[c * nn:(c + 1) * nn], cn, nn) for c in range(2)])
+    assert rel(y, ref) < OPS_TOL
+
+
 @pytest.mark.parametrize("key", ["q1", "q2", "q1p", "q2p", "hex"])
 def test_element_data_and_products(key):
     """Element matrices, Ce / Ctau / tau and every element product vs the goldens."""
