@@ -64,8 +64,10 @@ int fem_launch_invdiag(int n, const double* D, const uint8_t* pin, double* invD,
 int fem_launch_level_sums(const FemGrid& g, const FemLattice& lat, const double* diag, double* out, cudaStream_t s);
 
 int fem_launch_ebe(int ncomp, const FemGrid& g, const MatCombo& m, const double* x, double* y, cudaStream_t s);
-int fem_launch_stencil_apply(int ncomp, const FemGrid& g, const double* tab, double alpha, const double* x, double* y,
-                             int sms, cudaStream_t s);
+// y = alpha A x per component for one shared element matrix A, as its assembled
+// stencil (tab: FEM_TAB_MAX doubles of scratch, used by the 3D kind)
+int fem_launch_shared_apply(int ncomp, const FemGrid& g, const double* A, double* tab, double alpha, const double* x,
+                            double* y, int sms, cudaStream_t s);
 int fem_launch_grad(int ndim, const FemGrid& g, const double* Ge, const double* P, double* y, cudaStream_t s);
 int fem_launch_div(int ndim, const FemGrid& g, const double* Ge, const double* U, double* y, cudaStream_t s);
 int fem_launch_convection(const FemGrid& g, const FemQuad& Q, const double* U, double beta, int mode, double* out,

@@ -561,10 +561,9 @@ extern "C" int fem_ebe_apply(fem_ctx* c, int ncomp, const double* x, double* y, 
                              cudaStream_t s) {
   if (!c || !x || !y || ncomp < 1 || ncomp > 3) return FEM_E_ARG;
   if (A && !B && !C) {
-    // shared element matrix only: its assembled stencil (built on the device)
-    // applied by a tiled smem kernel, instead of the per-node element gather
-    FEM_TRY(fem_launch_stencil_build(c->g, A, 0, 0, c->ebe_tab, s));
-    return fem_launch_stencil_apply(ncomp, c->g, c->ebe_tab, alpha, x, y, c->sms, s);
+    // shared element matrix only: its assembled stencil (built on the device),
+    // streamed in register strips, instead of the per-node element gather
+    return fem_launch_shared_apply(ncomp, c->g, A, c->ebe_tab, alpha, x, y, c->sms, s);
   }
   const MatCombo m{A, alpha, B, beta, transB, C, gamma};
   return fem_launch_ebe(ncomp, c->g, m, x, y, s);

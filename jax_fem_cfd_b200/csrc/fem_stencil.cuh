@@ -186,39 +186,44 @@ __device__ __forceinline__ int fem_rel(int v, int c, int n, int periodic) {
   return d;
 }
 
-// Table of the assembled form of shared matrix A (nen x nen): out[cls][off].
-// transpose: use A^T; skip_diag: omit the b == a terms (A with a zero diagonal).
+// Entry t = cls * NOFF + off of the table of the assembled form of shared
+// matrix A (nen x nen): the sum, over the incident elements of the class's
+// representative node (incidence order) and then b ascending, of the A[a][b]
+// whose node b lies at offset off. transpose: use A^T; skip_diag: omit b == a.
+template <int KIND>
+__device__ __forceinline__ double fem_stencil_entry(const FemGrid& g, const double* __restrict__ A, int transpose,
+                                                    int skip_diag, int t) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF, NEN = KI<KIND>::NEN, S = KI<KIND>::S;
+  const int nc = fem_axis_ncls(KIND, g.periodic);
+  const int cls = t / NOFF, want = t - cls * NOFF;
+  const int cx = cls % nc, cy = (cls / nc) % nc, cz = cls / (nc * nc);
+  const int i = fem_axis_rep(KIND, g.periodic, cx, g.nex), j = fem_axis_rep(KIND, g.periodic, cy, g.ney);
+  const int k = (KIND == FEM_HEX8) ? fem_axis_rep(KIND, 0, cz, g.nez) : 0;
+  double acc = 0.0;
+  if (i >= 0 && j >= 0 && k >= 0) {
+    fem_incident_k<KIND>(g, i, j, k, [&](int ie, int je, int ke, int e, int a) {
+      for (int b = 0; b < NEN; ++b) {
+        if (skip_diag && b == a) continue;
+        const int bi = S * ie + kdi<KIND>(b), bj = S * je + kdj<KIND>(b), bk = ke + kdk<KIND>(b);
+        const int dx = fem_rel(bi, i, g.nnx, g.periodic) + R, dy = fem_rel(bj, j, g.nny, g.periodic) + R;
+        const int dz = (KIND == FEM_HEX8) ? (bk - k + R) : 0;
+        if ((dz * W + dy) * W + dx == want) acc += transpose ? A[b * NEN + a] : A[a * NEN + b];
+      }
+    });
+  }
+  return acc;
+}
+// The whole table by the threads of one CTA (out: global or shared memory).
+template <int KIND>
+__device__ __forceinline__ void fem_stencil_table_block(const FemGrid& g, const double* __restrict__ A, int transpose,
+                                                        int skip_diag, double* out) {
+  const int n = fem_stencil_ncls(g) * KI<KIND>::NOFF;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) out[t] = fem_stencil_entry<KIND>(g, A, transpose, skip_diag, t);
+}
 template <int KIND>
 __global__ void k_stencil_build(FemGrid g, const double* __restrict__ A, int transpose, int skip_diag,
                                 double* __restrict__ out) {
-  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF, NEN = KI<KIND>::NEN, S = KI<KIND>::S;
-  const int nc = fem_axis_ncls(KIND, g.periodic);
-  const int ncls = fem_stencil_ncls(g);
-  for (int cls = blockIdx.x * blockDim.x + threadIdx.x; cls < ncls; cls += gridDim.x * blockDim.x) {
-    double acc[NOFF];
-#pragma unroll
-    for (int o = 0; o < NOFF; ++o) acc[o] = 0.0;
-    const int cx = cls % nc, cy = (cls / nc) % nc, cz = cls / (nc * nc);
-    const int i = fem_axis_rep(KIND, g.periodic, cx, g.nex), j = fem_axis_rep(KIND, g.periodic, cy, g.ney);
-    const int k = (KIND == FEM_HEX8) ? fem_axis_rep(KIND, 0, cz, g.nez) : 0;
-    if (i >= 0 && j >= 0 && k >= 0) {
-      fem_incident_k<KIND>(g, i, j, k, [&](int ie, int je, int ke, int e, int a) {
-        for (int b = 0; b < NEN; ++b) {
-          if (skip_diag && b == a) continue;
-          const int bi = S * ie + kdi<KIND>(b), bj = S * je + kdj<KIND>(b), bk = ke + kdk<KIND>(b);
-          const int dx = fem_rel(bi, i, g.nnx, g.periodic) + R, dy = fem_rel(bj, j, g.nny, g.periodic) + R;
-          const int dz = (KIND == FEM_HEX8) ? (bk - k + R) : 0;
-          const double v = transpose ? A[b * NEN + a] : A[a * NEN + b];
-          const int off = (dz * W + dy) * W + dx;
-#pragma unroll
-          for (int o = 0; o < NOFF; ++o)
-            if (o == off) acc[o] += v;
-        }
-      });
-    }
-#pragma unroll
-    for (int o = 0; o < NOFF; ++o) out[(size_t)cls * NOFF + o] = acc[o];
-  }
+  fem_stencil_table_block<KIND>(g, A, transpose, skip_diag, out);
 }
 
 // y = sum_off coef[cls(i,j,k)][off] * src(node(i,j,k) + off)

@@ -262,14 +262,14 @@ __global__ void __launch_bounds__(512) k_stencil_apply(FemGrid g, const double* 
 // from warp shuffles and each row feeds the W output rows it touches. Strips
 // clear of the top and bottom boundary rows of a Q1 lattice keep their column's
 // 9 coefficients in registers; the others read the table per row. The sum runs
-// over dy, then dx, in ascending order for every node.
+// over dy, then dx, in ascending order for every node. Each CTA assembles the
+// stencil table of A in shared memory (fem_stencil_table_block) on entry.
 template <int KIND, int M>
-__global__ void __launch_bounds__(256, 3) k_stencil_strip(FemGrid g, const double* __restrict__ tab, double alpha,
+__global__ void __launch_bounds__(256, 3) k_stencil_strip(FemGrid g, const double* __restrict__ A, double alpha,
                                                           const double* __restrict__ x, double* __restrict__ y) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF, OW = 32 - 2 * R, NR = M + 2 * R;
   __shared__ double stab[16 * NOFF];
-  const int nt = fem_stencil_ncls(g) * NOFF;
-  for (int t = threadIdx.x; t < nt; t += blockDim.x) stab[t] = tab[t];
+  fem_stencil_table_block<KIND>(g, A, 0, 0, stab);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int nc = fem_axis_ncls(KIND, g.periodic);
@@ -281,11 +281,17 @@ __global__ void __launch_bounds__(256, 3) k_stencil_strip(FemGrid g, const doubl
     const int xg = bx * OW + lane - R, y0 = by * M;
     const int gx = g.periodic ? fem_wrap(xg, g.nnx) : (xg < 0 ? 0 : (xg >= g.nnx ? g.nnx - 1 : xg));
     double v[NR];
+    if (y0 >= R && y0 + M + R <= g.nny) {  // all rows inside the lattice: no wrap or clamp
+      const double* p = x + (size_t)(y0 - R) * g.nnx + gx;
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      int gy = y0 - R + r;
-      gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
-      v[r] = __ldg(x + (size_t)gy * g.nnx + gx);
+      for (int r = 0; r < NR; ++r) v[r] = __ldg(p + (size_t)r * g.nnx);
+    } else {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        int gy = y0 - R + r;
+        gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
+        v[r] = __ldg(x + (size_t)gy * g.nnx + gx);
+      }
     }
     const bool own = lane >= R && lane < 32 - R && xg < g.nnx;
     const int cx = own ? fem_axis_cls(KIND, g.periodic, xg, g.nex) : 0;
@@ -351,8 +357,11 @@ __global__ void __launch_bounds__(256, 3) k_stencil_strip(FemGrid g, const doubl
   }
 }
 
-int fem_launch_stencil_apply(int ncomp, const FemGrid& g, const double* tab, double alpha, const double* x, double* y,
-                             int sms, cudaStream_t s) {
+int fem_launch_shared_apply(int ncomp, const FemGrid& g, const double* A, double* tab, double alpha, const double* x,
+                            double* y, int sms, cudaStream_t s) {
+  if (g.kind == FEM_HEX8) {
+    if (int rc = fem_launch_stencil_build(g, A, 0, 0, tab, s)) return rc;
+  }
   for (int c = 0; c < ncomp; ++c) {
     const size_t o = (size_t)c * g.nn;
     if (g.kind == FEM_HEX8) {
@@ -367,9 +376,9 @@ int fem_launch_stencil_apply(int ncomp, const FemGrid& g, const double* tab, dou
       const long long need = (nwarp + 7) / 8;
       const int grid = (int)(need < 3LL * sms ? need : 3LL * sms);
       if (g.kind == FEM_Q1_2D)
-        k_stencil_strip<FEM_Q1_2D, M><<<grid, 256, 0, s>>>(g, tab, alpha, x + o, y + o);
+        k_stencil_strip<FEM_Q1_2D, M><<<grid, 256, 0, s>>>(g, A, alpha, x + o, y + o);
       else
-        k_stencil_strip<FEM_Q2_2D, M><<<grid, 256, 0, s>>>(g, tab, alpha, x + o, y + o);
+        k_stencil_strip<FEM_Q2_2D, M><<<grid, 256, 0, s>>>(g, A, alpha, x + o, y + o);
     }
     if (int rc = fem_after_launch("k_stencil_apply")) return rc;
   }

@@ -271,7 +271,7 @@ __global__ void k_invdiag(int n, const double* __restrict__ D, const uint8_t* __
 int fem_launch_stencil_build(const FemGrid& g, const double* A, int transpose, int skip_diag, double* out,
                              cudaStream_t s) {
   const int ncls = fem_stencil_ncls(g);
-  FEM_KIND_DISPATCH(g.kind, K, (k_stencil_build<K><<<1, 64, 0, s>>>(g, A, transpose, skip_diag, out)));
+  FEM_KIND_DISPATCH(g.kind, K, (k_stencil_build<K><<<1, 512, 0, s>>>(g, A, transpose, skip_diag, out)));
   (void)ncls;
   return fem_after_launch("k_stencil_build");
 }
