@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(512) k_stencil_apply(FemGrid g, const double* 
 // over dy, then dx, in ascending order for every node. Each CTA assembles the
 // stencil table of A in shared memory (fem_stencil_table_block) on entry.
 template <int KIND, int M>
-__global__ void __launch_bounds__(256, 3) k_stencil_strip(FemGrid g, const double* __restrict__ A, double alpha,
+__global__ void __launch_bounds__(256, 2) k_stencil_strip(FemGrid g, const double* __restrict__ A, double alpha,
                                                           const double* __restrict__ x, double* __restrict__ y) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF, OW = 32 - 2 * R, NR = M + 2 * R;
   __shared__ double stab[16 * NOFF];
@@ -370,11 +370,11 @@ int fem_launch_shared_apply(int ncomp, const FemGrid& g, const double* A, double
       const int dyn = (32 + 2) * (TY + 2) * 3 * (int)sizeof(double);
       k_stencil_apply<FEM_HEX8><<<grid, T, dyn, s>>>(g, tab, alpha, x + o, y + o);
     } else {
-      constexpr int M = 8;
+      constexpr int M = 16;
       const int ow = (g.kind == FEM_Q2_2D) ? 28 : 30;
       const long long nwarp = (long long)((g.nnx + ow - 1) / ow) * ((g.nny + M - 1) / M);
       const long long need = (nwarp + 7) / 8;
-      const int grid = (int)(need < 3LL * sms ? need : 3LL * sms);
+      const int grid = (int)(need < 2LL * sms ? need : 2LL * sms);
       if (g.kind == FEM_Q1_2D)
         k_stencil_strip<FEM_Q1_2D, M><<<grid, 256, 0, s>>>(g, A, alpha, x + o, y + o);
       else

@@ -56,13 +56,13 @@ def test_mesh_generation(fn, args):
 
 
 @pytest.mark.parametrize("fn,args", [
-    ("create_mesh_2d", (67, 29, 2.0, 1.0)),          # 3 x 4 warp strips, interior fast path, ragged edges
+    ("create_mesh_2d", (67, 45, 2.0, 1.0)),          # 3 x 3 warp strips, interior fast path, ragged edges
     ("create_mesh_2d", (2, 1, 1.0, 1.0)),            # one partial strip
-    ("create_mesh_2d", (30, 8, 1.0, 1.0)),           # ney < 9: boundary rows in every strip
-    ("create_mesh_2d_quad9", (17, 13, 1.0, 1.5)),
-    ("create_periodic_mesh_2d", (40, 20, 1.0, 1.0)),
+    ("create_mesh_2d", (30, 8, 1.0, 1.0)),           # boundary rows in every strip
+    ("create_mesh_2d_quad9", (17, 23, 1.0, 1.5)),
+    ("create_periodic_mesh_2d", (40, 50, 1.0, 1.0)),
     ("create_periodic_mesh_2d", (3, 2, 1.0, 1.0)),   # lattice narrower than the strip halo
-    ("create_periodic_mesh_2d_quad9", (24, 10, 1.0, 1.0)),
+    ("create_periodic_mesh_2d_quad9", (24, 26, 1.0, 1.0)),
     ("create_mesh_3d", (9, 7, 5, 1.0, 1.0, 1.0)),
 ])
 def test_shared_matrix_matvec(fn, args):
