@@ -255,19 +255,16 @@ def whole_job_rate(world, steps, max_total_ms):
     return world * 1000.0 * steps / max_total_ms
 
 
-def poisson_and_matvec(args):
-    """Reference-published GPU figures on their own sizes (README.md:28-41):
-    MG-PCG Poisson solve on 1024x1024 Q1 elements and the EBE matvec on
-    4096x4096 Q1 elements (beyond L2: a true HBM-roofline kernel)."""
+def poisson(n, solves=5):
+    """MG-PCG Poisson solve on an n x n Q1 unit square: pinned node 0, seeded
+    random rhs, x0 = 0, tol 1e-8, final MG mesh 4x4. Median of `solves` timed
+    solves after 3 warm-up solves, a 256 MiB L2 flush before each."""
     import torch
 
     from jax_fem_cfd_b200 import _lib
     from jax_fem_cfd_b200.context import Context, Mesh, make_mask, ptr, stream
     from jax_fem_cfd_b200.core import multigrid as mg
-    out = {}
     hbm, _ = measured_peaks()
-    # Poisson: pinned node 0, random rhs (seeded), x0 = 0, tol 1e-8, final mesh 4x4
-    n = 1024
     ctx = Context(Mesh(0, False, n, n, 1, 1.0, 1.0))
     pm = make_mask(np.array([0]), ctx.nn)
     ctx.set_bc(None, pm, True)
@@ -281,7 +278,7 @@ def poisson_and_matvec(args):
     stt = torch.zeros(1, dtype=torch.int32, device="cuda")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     times = []
-    for k in range(8):
+    for k in range(3 + solves):
         x.zero_()
         flush.zero_()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -293,10 +290,53 @@ def poisson_and_matvec(args):
         if k >= 3:
             times.append(s.elapsed_time(e))
     ms = float(np.median(times))
-    out["poisson_1024x1024_q1"] = {"metric": "Poisson solves/s (MG-PCG, tol 1e-8)", "value": 1000.0 / ms,
-                                   "ms_per_solve": ms, "iterations": int(it.item()), "elements": n * n,
-                                   "reference_published_ms_unnamed_gpu": 28.0}
+    iters = int(it.item())
+    status = int(stt.item())
+    byts = cg_algorithmic_bytes([ctx.level_info(l)[0] for l in range(ctx.nlev)], iters, None)
     del ctx
+    return {"ms_per_solve": ms, "solves_per_s": 1000.0 / ms, "iterations": iters, "status": status,
+            "elements": n * n, "nodes": (n + 1) ** 2, "algorithmic_bytes": byts,
+            "achieved_gbs": byts / ms / 1e6, "frac_of_hbm": byts / ms / 1e6 / hbm}
+
+
+def poisson_sweep():
+    """Poisson solve times on 2^k x 2^k Q1 meshes, k = 4..12 (16 .. 16.8M
+    elements, the reference README's sweep sizes)."""
+    return {f"poisson_{2 ** k}x{2 ** k}_q1": poisson(2 ** k) for k in range(4, 13)}
+
+
+def serving(count, steps):
+    """Request stream of independent wall-bounded solves (sizes uniform over
+    32^2..256^2 Q1, viscosity log-uniform 1e-3..1e-1, Fourier initial velocity,
+    `steps` steps each): the plain path (one request at a time on the whole
+    device) against the continuous-batching server, saturated (all requests
+    at t = 0) and under Poisson arrivals at 50 % and 90 % of the saturated
+    throughput. Latency = completion - arrival (plain: service time)."""
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")  # streams on separate hardware queues
+    from jax_fem_cfd_b200.serving import Server, make_requests, run_plain
+    reqs = make_requests(count, seed=0, steps=steps)
+    srv = Server(keep_results=False)
+    srv.prewarm(reqs)
+    bad = lambda d: sum(1 for x in d if x["status"] != 0)
+    dp, plain = run_plain(reqs, srv)
+    ds, sat = srv.run(reqs, realtime=False)
+    out = {"workload": f"{count} requests x {steps} steps, Q1 {{32,64,128,256}}^2 wall-bounded, FP64",
+           "plain": dict(plain, failed=bad(dp)), "served_saturated": dict(sat, failed=bad(ds)),
+           "speedup_solves_per_s": sat["solves_per_s"] / plain["solves_per_s"]}
+    for frac in (0.5, 0.9):
+        rate = frac * sat["solves_per_s"]
+        dr, m = srv.run(make_requests(count, seed=0, steps=steps, rate=rate))
+        out[f"served_poisson_{int(frac * 100)}pct"] = dict(m, arrival_rate_per_s=rate, failed=bad(dr))
+    return out
+
+
+def poisson_and_matvec(args):
+    """Reference-published GPU figures on their own sizes (README.md:28-41):
+    MG-PCG Poisson solve on 1024x1024 Q1 elements and the EBE matvec on
+    4096x4096 Q1 elements (beyond L2: a true HBM-roofline kernel)."""
+    r = poisson(1024)
+    out = {"poisson_1024x1024_q1": dict(metric="Poisson solves/s (MG-PCG, tol 1e-8)", value=r["solves_per_s"],
+                                        reference_published_ms_unnamed_gpu=28.0, **r)}
     out.update(matvec())
     return out
 
@@ -397,10 +437,15 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--only", choices=["matvec"], help="run one secondary measurement alone and print it")
+    ap.add_argument("--only", choices=["matvec", "poisson_sweep", "serving"],
+                    help="run one secondary measurement alone and print it")
+    ap.add_argument("--requests", type=int, default=64, help="--only serving: requests in the stream")
+    ap.add_argument("--request-steps", type=int, default=200, help="--only serving: steps per request")
     args = ap.parse_args()
-    if args.only == "matvec":
-        print(json.dumps(matvec()))
+    if args.only:
+        fn = {"matvec": matvec, "poisson_sweep": poisson_sweep,
+              "serving": lambda: serving(args.requests, args.request_steps)}[args.only]
+        print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))

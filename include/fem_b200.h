@@ -281,6 +281,17 @@ int fem_ctx_stage_times(fem_ctx* ctx, float* ms, int max_n);
  * cap = 0 disables tracing. */
 int fem_ctx_set_trace(fem_ctx* ctx, unsigned long long* buf, int cap);
 
+/* Cap on the CTAs of this context's persistent cooperative launches (the PCG,
+ * V-cycle and BiCGSTAB solver kernels); ctas = 0 restores the co-resident
+ * capacity found at create, and ctas above it is clamped to it. *capacity
+ * (optional) receives that capacity (SMs x resident solver CTAs per SM). A
+ * request loop that runs several contexts at once on separate streams gives
+ * each a share of the capacity, so every cooperative grid in flight fits on
+ * the device at the same time. Results depend on the cap (the reduction
+ * partials are per CTA) and are reproducible for a given cap. No reference
+ * counterpart: the reference runs one problem at a time. */
+int fem_ctx_set_max_ctas(fem_ctx* ctx, int ctas, int* capacity);
+
 /* Number of this library's kernel launches issued so far in this process. */
 long long fem_launch_count(void);
 

@@ -60,6 +60,7 @@ SIGNATURES = {
     "fem_ctx_enable_timing": (c_int, [P, c_int]),
     "fem_ctx_stage_times": (c_int, [P, P, c_int]),
     "fem_ctx_set_trace": (c_int, [P, P, c_int]),
+    "fem_ctx_set_max_ctas": (c_int, [P, c_int, P]),
     "fem_launch_count": (c_longlong, []),
     "fem_last_error": (ctypes.c_char_p, []),
 }

@@ -112,7 +112,8 @@ struct fem_ctx {
   unsigned int* bar = nullptr;
   int* err = nullptr;
   double* partials = nullptr;
-  int max_coop = 148;
+  int max_coop = 148;       // CTAs of the persistent cooperative launches
+  int coop_capacity = 148;  // upper bound of max_coop (co-resident capacity)
   // vectors (nn or ndim*nn)
   double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pAp = nullptr, *pb = nullptr;  // CG
   double *br = nullptr, *brh = nullptr, *bp0 = nullptr, *bp1 = nullptr, *bq0 = nullptr, *bq1 = nullptr,
@@ -275,6 +276,7 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   c->max_coop = c->sms * occ;
   const char* ev = getenv("FEM_MAX_CTAS");
   if (ev && atoi(ev) > 0) c->max_coop = std::min(c->max_coop, atoi(ev));
+  c->coop_capacity = c->max_coop;  // partials are sized for this many CTAs
   const FemGrid& g = c->g;
   c->ndim = (g.kind == FEM_HEX8) ? 3 : 2;
   c->nq = g.nen;
@@ -990,6 +992,13 @@ extern "C" int fem_ctx_set_trace(fem_ctx* c, unsigned long long* buf, int cap) {
   if (!c || cap < 0 || (cap > 0 && !buf)) return FEM_E_ARG;
   c->trace = cap > 0 ? buf : nullptr;
   c->trace_cap = cap;
+  return FEM_OK;
+}
+
+extern "C" int fem_ctx_set_max_ctas(fem_ctx* c, int ctas, int* capacity) {
+  if (!c || ctas < 0) return FEM_E_ARG;
+  c->max_coop = (ctas > 0 && ctas < c->coop_capacity) ? ctas : c->coop_capacity;
+  if (capacity) *capacity = c->coop_capacity;
   return FEM_OK;
 }
 

@@ -451,6 +451,128 @@ __device__ __noinline__ void mg_coarse(const Red& red, const CgArgs& A, double* 
   __syncthreads();
 }
 
+// Coarse levels up to this many nodes are solved by one warp (mg_coarse_warp).
+#define FEM_COARSE_WARP_S 4
+#define FEM_COARSE_WARP_NN (32 * FEM_COARSE_WARP_S)
+
+__device__ __forceinline__ double fem_warp_sum(double v) {
+  // xor butterfly: every lane ends with the same bits (each stage adds the same
+  // two values, in either order)
+#pragma unroll
+  for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+  return v;
+}
+
+// The pinned coarsest-level CG of mg_coarse (same start, updates and stop test)
+// run by the 32 lanes of warp 0 alone, for levels of at most FEM_COARSE_WARP_NN
+// nodes: node i = lane + 32 s lives in registers x[s], r[s], p[s]; p goes
+// through shared memory (sp, nn doubles) for the stencil, and the dots are warp
+// sums, so an iteration has no block barrier and no global-memory round trip.
+template <int KIND>
+__device__ __noinline__ void mg_coarse_warp(const CgArgs& A, double* sp) {
+  constexpr int S = FEM_COARSE_WARP_S, R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  const MgLevel& L = A.lv[A.nlev - 1];
+  // the level lives in shared memory next to sp: copy what the loop reads, so
+  // the stores to sp cannot force reloads
+  const int nn = L.g.nn, nnx = L.g.nnx, nny = L.g.nny, nex = L.g.nex, ney = L.g.ney;
+  const int per = L.g.periodic, maxit = A.coarse_maxiter;
+  const double* __restrict__ tab = L.tab;
+  const uint8_t* __restrict__ pin = L.pin;
+  const double* __restrict__ rN = L.r;
+  double* __restrict__ tN = L.t;
+  const int lane = threadIdx.x & 31;
+  const int nc = fem_axis_ncls(KIND, per);
+  double x[S], r[S], p[S];
+  constexpr bool PRE = (W == 3);        // neighbour indices kept in registers (Q1)
+  constexpr int WP = PRE ? W : 1;
+  int cof[S];     // table row of the node's class, -1 past nn or pinned (q = 0)
+  int pos[S];     // (iy << 16) | ix
+  int row[S][WP];  // neighbour rows (times nnx) and columns, wrapped or clamped
+  int col[S][WP];
+  double bs = 0.0;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int i = lane + 32 * s;
+    const bool live = i < nn && !(pin && pin[i]);
+    const double b = live ? rN[i] : 0.0;
+    r[s] = b;
+    p[s] = b;
+    x[s] = 0.0;
+    bs += b * b;
+    const int ix = live ? i % nnx : 0, iy = live ? i / nnx : 0;
+    cof[s] = live ? (fem_axis_cls(KIND, per, iy, ney) * nc + fem_axis_cls(KIND, per, ix, nex)) * NOFF : -1;
+    pos[s] = (iy << 16) | ix;
+#pragma unroll
+    for (int d = 0; d < WP; ++d) {
+      int w = iy + d - R, v = ix + d - R;
+      w = per ? fem_wrap(w, nny) : min(max(w, 0), nny - 1);
+      v = per ? fem_wrap(v, nnx) : min(max(v, 0), nnx - 1);
+      row[s][d] = w * nnx;
+      col[s][d] = v;
+    }
+  }
+  bs = fem_warp_sum(bs);
+  const double atol2 = fmax(A.coarse_tol * A.coarse_tol * bs, 0.0);
+  double gamma = bs;
+  int k = 0;
+  while (gamma > atol2 && k < maxit) {
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+      if (lane + 32 * s < nn) sp[lane + 32 * s] = p[s];
+    __syncwarp();
+    double q[S], pq = 0.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      double y = 0.0;
+      if (cof[s] >= 0) {
+        const double* c = tab + cof[s];
+        if constexpr (PRE) {
+#pragma unroll
+          for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx) y += c[dy * W + dx] * sp[row[s][dy] + col[s][dx]];
+        } else {
+          const int ix = pos[s] & 0xffff, iy = pos[s] >> 16;
+#pragma unroll
+          for (int dy = 0; dy < W; ++dy) {
+            int w = iy + dy - R;
+            w = per ? fem_wrap(w, nny) : min(max(w, 0), nny - 1);
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx) {
+              int v = ix + dx - R;
+              v = per ? fem_wrap(v, nnx) : min(max(v, 0), nnx - 1);
+              y += c[dy * W + dx] * sp[w * nnx + v];
+            }
+          }
+        }
+      }
+      q[s] = y;
+      pq += p[s] * y;
+    }
+    pq = fem_warp_sum(pq);
+    __syncwarp();  // every read of sp before the next iteration writes it
+    const double alpha = gamma / pq;
+    double rr = 0.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      x[s] = x[s] + alpha * p[s];
+      r[s] = r[s] - alpha * q[s];
+      rr += r[s] * r[s];
+    }
+    rr = fem_warp_sum(rr);
+    const double beta = rr / gamma;
+#pragma unroll
+    for (int s = 0; s < S; ++s) p[s] = r[s] + beta * p[s];
+    gamma = rr;
+    ++k;
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int i = lane + 32 * s;
+    if (i < nn) tN[i] = (pin && pin[i]) ? 0.0 : x[s];
+  }
+}
+
 // Sums of a freshly produced level correction X_n (mean-zero bookkeeping).
 __device__ __forceinline__ void mg_xsums(const MgLevel& L, int i, double xi, double (&a)[2]) {
   a[0] += xi;
@@ -655,7 +777,16 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
       if (!mg_down<KIND, PIN>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 7);
     if (blockIdx.x == 0) {
-      mg_coarse<KIND, PIN>(gr, A, smem, cg_r, cg_p, cg_q);
+      bool warp_solve = false;
+      if constexpr (PIN && KIND != FEM_HEX8) warp_solve = A.lv[N - 1].g.nn <= FEM_COARSE_WARP_NN;
+      if (warp_solve) {
+        if constexpr (PIN && KIND != FEM_HEX8) {
+          if (threadIdx.x < 32) mg_coarse_warp<KIND>(A, smem + 128);
+        }
+        __syncthreads();
+      } else {
+        mg_coarse<KIND, PIN>(gr, A, smem, cg_r, cg_p, cg_q);
+      }
       fem_trace_mark(A.sync, 8);
       const MgLevel& Lc = A.lv[N - 1];
       if (N == 1) {

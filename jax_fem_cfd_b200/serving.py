@@ -1,0 +1,330 @@
+"""Serving: continuous batching of independent 2D wall-bounded flow solves.
+
+A request is one Navier-Stokes problem on the unit square (Q1, all walls
+no-slip, pressure pinned at node 0, MG-PCG pressure and BiCGSTAB momentum at
+tol 1e-8), with its own mesh size, viscosity and divergence-free initial
+velocity, run for a fixed number of 4-step projection steps (the step of
+solvers/standard.py:148-165).
+
+The request loop (`Server.run`) is continuous batching, not a queue:
+
+- Requests arrive over time (Poisson arrivals, or all at t = 0). A request is
+  admitted as soon as the device has room for it: a share of the cooperative
+  CTA capacity (its solver kernels are persistent cooperative grids, and the
+  grids of all admitted requests must fit on the device at once) and, when no
+  pooled solver of its size is idle, the HBM a new one needs (free device
+  memory against the footprint measured when the first solver of that size
+  was built).
+- Solvers (context, element matrices, multigrid hierarchy, boundary sets, the
+  velocity / pressure ping-pong buffers) are pooled per mesh size and stay
+  resident: a finished request hands its solver to the next request of that
+  size, so nothing is allocated or freed while requests run.
+- Every admitted request runs on its own CUDA stream, in chunks of steps; up to
+  two chunks per request are queued at a time, so the requests' kernels
+  overlap on the device and a new arrival is never behind a long queue.
+- A request's CTA share depends only on its mesh size, so its results are the
+  same (bit for bit) alone and in any mix: the solver's reductions are
+  deterministic for a given grid.
+
+No reference counterpart: the reference runs one problem per process.
+"""
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .context import ptr
+
+SIZES = (32, 64, 128, 256)
+
+
+@dataclass
+class Request:
+    rid: int
+    n: int                   # Q1 elements per side of the unit square
+    nu: float                # kinematic viscosity (rho = 1, so mu = nu)
+    steps: int
+    dt: float
+    arrival: float           # seconds after the start of the stream
+    U0: np.ndarray = field(repr=False)  # (2 (n+1)^2,) initial velocity, component-major
+
+
+def fourier_velocity(n, seed, kmax=8):
+    """Divergence-free velocity on the (n+1)^2 nodes of the unit square: the
+    curl of a stream function made of the Fourier modes 1 <= |k| <= kmax with
+    seeded N(0,1) cosine and sine coefficients of amplitude 1/|k|^2, scaled to
+    max |u| = 1. Returned as [u; v] (component-major, like the solver's U)."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(0.0, 1.0, n + 1)
+    X, Y = np.meshgrid(x, x)  # node (i, j) -> row j, column i: node id j (n+1) + i
+    u = np.zeros_like(X)
+    v = np.zeros_like(X)
+    for kx in range(-kmax, kmax + 1):
+        for ky in range(0, kmax + 1):
+            k2 = kx * kx + ky * ky
+            if k2 == 0 or k2 > kmax * kmax or (ky == 0 and kx < 0):
+                continue
+            a, b = rng.standard_normal(2) / k2
+            ph = 2.0 * np.pi * (kx * X + ky * Y)
+            # psi = a cos(ph) + b sin(ph); u = dpsi/dy, v = -dpsi/dx
+            d = 2.0 * np.pi * (-a * np.sin(ph) + b * np.cos(ph))
+            u += d * ky
+            v -= d * kx
+    s = np.sqrt(u * u + v * v).max()
+    s = s if s > 0 else 1.0
+    return np.concatenate([u.ravel(), v.ravel()]) / s
+
+
+def make_requests(count, seed=0, sizes=SIZES, nu_range=(1e-3, 1e-1), steps=200, rate=None, kmax=8, cfl=0.25):
+    """Seeded request stream: size uniform over `sizes`, viscosity log-uniform
+    over `nu_range`, Fourier initial velocity (seed = request id + seed), time
+    step dt = cfl * h (|u| <= 1), arrivals Poisson at `rate` per second (all at
+    t = 0 when rate is None)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        n = int(sizes[rng.integers(len(sizes))])
+        nu = float(math.exp(rng.uniform(math.log(nu_range[0]), math.log(nu_range[1]))))
+        if rate:
+            t += float(rng.exponential(1.0 / rate))
+        out.append(Request(i, n, nu, steps, cfl / n, t if rate else 0.0, fourier_velocity(n, seed + i, kmax)))
+    return out
+
+
+def cavity_config(n):
+    """Wall-bounded unit square, Q1, all four faces Dirichlet (U_d = 0),
+    pinned pressure, MG-PCG (final mesh 4 x 4) at tol 1e-8."""
+    from .setup import simulation as sim
+    return sim.Config(mesh="simple", solver="standard",
+                      mesh_config=sim.SimpleMeshConfig(num_elem=[n, n], domain_size=[1.0, 1.0], shape_func_ord=1,
+                                                       periodic=False),
+                      solver_config=sim.StandardSolverConfig(dirichlet_faces=[0, 1, 2, 3], symmetry_faces=[],
+                                                             outlet_faces=[], streamline_diff=False, solver_tol=1e-8,
+                                                             set_zeroP=True, pressure_precond="multigrid",
+                                                             final_multigrid_mesh=[4, 4]))
+
+
+class Slot:
+    """Pooled device state of one mesh size: the solver and its buffers."""
+
+    def __init__(self, n):
+        from .setup import simulation as sim
+        _, timestep, *_rest = sim.setup(cavity_config(n))
+        U_d = _rest[-1]
+        self.n = n
+        self.solver = timestep.solver
+        s = self.solver
+        self.ud = s.u_full(U_d)
+        nn = s.nn
+        dev = s.ctx.dev
+        self.U = [torch.zeros(2 * nn, dtype=torch.float64, device=dev) for _ in range(2)]
+        self.P = [torch.zeros(nn, dtype=torch.float64, device=dev) for _ in range(2)]
+        self.iters = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.U_host = torch.empty(2 * nn, dtype=torch.float64).pin_memory()
+        self.P_host = torch.empty(nn, dtype=torch.float64).pin_memory()
+        self.U0_host = torch.empty(2 * nn, dtype=torch.float64).pin_memory()
+        self.status_host = torch.empty(2, dtype=torch.int32).pin_memory()
+
+    def set_ctas(self, ctas):
+        cap = ctypes.c_int(0)
+        _lib.call("fem_ctx_set_max_ctas", self.solver.ctx.handle, int(ctas), ctypes.byref(cap))
+        return cap.value
+
+    def steps(self, cur, k, dt, mu, stream):
+        """k steps from buffer `cur`; returns the buffer holding the result."""
+        s, h = self.solver, ctypes.c_void_p(stream.cuda_stream)
+        for _ in range(k):
+            nxt = 1 - cur
+            _lib.call("fem_step4", s.ctx.handle, ptr(self.U[cur]), ptr(self.P[cur]), float(dt), 1.0, float(mu),
+                      ptr(self.ud), None, None, float(s.cfg.solver_tol), s.precond, ptr(self.U[nxt]),
+                      ptr(self.P[nxt]), ptr(self.iters), ptr(s.status), h)
+            cur = nxt
+        return cur
+
+
+class _Active:
+    __slots__ = ("req", "slot", "stream", "cur", "enq", "events", "final", "admitted", "ctas")
+
+    def __init__(self, req, slot, stream, ctas):
+        self.req, self.slot, self.stream, self.ctas = req, slot, stream, ctas
+        self.cur, self.enq, self.events, self.final, self.admitted = 0, 0, [], None, 0.0
+
+
+def ctas_for(n, share):
+    """CTA share of a request of mesh size n: about one node per thread (the
+    solver's own sizing for a dedicated device), capped at `share`."""
+    nn = (n + 1) ** 2
+    return max(1, min(share, -(-nn // 512)))
+
+
+class Server:
+    """Continuous-batching request loop over pooled solvers (see module doc).
+
+    share: CTA cap of one request (the device capacity is SMs x resident
+    solver CTAs per SM, 148 on a B200); chunk: steps per queued chunk;
+    hbm_reserve: bytes kept free when building a new solver."""
+
+    def __init__(self, share=37, chunk=10, hbm_reserve=2 << 30, keep_results=True):
+        self.share, self.chunk, self.hbm_reserve = share, chunk, hbm_reserve
+        self.keep_results = keep_results
+        self.pool = {}        # n -> idle Slots
+        self.footprint = {}   # n -> device bytes of one Slot
+        self.streams = []
+        self.capacity = None
+
+    def _new_slot(self, n):
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        slot = Slot(n)
+        torch.cuda.synchronize()
+        used = free0 - torch.cuda.mem_get_info()[0]
+        self.footprint[n] = max(self.footprint.get(n, 0), used, 1 << 20)
+        cap = slot.set_ctas(0)
+        self.capacity = cap if self.capacity is None else min(self.capacity, cap)
+        return slot
+
+    def warm(self, sizes):
+        """Build one pooled solver per size before the clock starts."""
+        for n in sizes:
+            if not self.pool.get(n):
+                self.pool.setdefault(n, []).append(self._new_slot(n))
+
+    def prewarm(self, requests):
+        """Build, before the clock starts, as many solvers per size as can run
+        at once under the CTA capacity (at most one per request of that size),
+        so the loop never builds one (building synchronises the device)."""
+        sizes = sorted({r.n for r in requests})
+        self.warm(sizes)
+        for n in sizes:
+            want = min(sum(r.n == n for r in requests), max(1, self.capacity // ctas_for(n, self.share)))
+            have = len(self.pool[n])
+            for _ in range(want - have):
+                self.pool[n].append(self._new_slot(n))
+
+    def _take_slot(self, n):
+        idle = self.pool.setdefault(n, [])
+        if idle:
+            return idle.pop()
+        if n in self.footprint and torch.cuda.mem_get_info()[0] < self.footprint[n] + self.hbm_reserve:
+            return None
+        return self._new_slot(n)
+
+    def run(self, requests, realtime=True):
+        """Serve `requests` (sorted by arrival); returns per-request records and
+        the stream's metrics. realtime=False admits every request at t = 0."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        if self.capacity is None:
+            self.warm(sorted({r.n for r in reqs}))
+        pending, active, done = [], [], []
+        used = 0
+        nxt = 0
+        free_streams = list(self.streams)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        while nxt < len(reqs) or pending or active:
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and (not realtime or reqs[nxt].arrival <= now):
+                pending.append(reqs[nxt])
+                nxt += 1
+            # admission: FIFO, while the head fits in CTAs and memory
+            while pending:
+                r = pending[0]
+                c = ctas_for(r.n, self.share)
+                if used + c > self.capacity:
+                    break
+                slot = self._take_slot(r.n)
+                if slot is None:
+                    break
+                pending.pop(0)
+                if not free_streams:
+                    st = torch.cuda.Stream()
+                    self.streams.append(st)
+                    free_streams.append(st)
+                a = _Active(r, slot, free_streams.pop(), c)
+                a.admitted = time.perf_counter() - t0
+                slot.set_ctas(c)
+                slot.U0_host.copy_(torch.from_numpy(r.U0))
+                with torch.cuda.stream(a.stream):
+                    slot.U[0].copy_(slot.U0_host, non_blocking=True)
+                    slot.P[0].zero_()
+                used += c
+                active.append(a)
+            # feed and retire
+            for a in list(active):
+                a.events = [e for e in a.events if not e.query()]
+                if a.enq < a.req.steps and len(a.events) < 2:
+                    k = min(self.chunk, a.req.steps - a.enq)
+                    a.cur = a.slot.steps(a.cur, k, a.req.dt, a.req.nu, a.stream)
+                    a.enq += k
+                    ev = torch.cuda.Event()
+                    ev.record(a.stream)
+                    a.events.append(ev)
+                    if a.enq == a.req.steps:
+                        s = a.slot
+                        with torch.cuda.stream(a.stream):
+                            s.U_host.copy_(s.U[a.cur], non_blocking=True)
+                            s.P_host.copy_(s.P[a.cur], non_blocking=True)
+                            s.status_host.copy_(s.solver.status, non_blocking=True)
+                        a.final = torch.cuda.Event()
+                        a.final.record(a.stream)
+                elif a.final is not None and a.final.query():
+                    t = time.perf_counter() - t0
+                    s = a.slot
+                    rec = {"rid": a.req.rid, "n": a.req.n, "arrival": a.req.arrival, "admitted": a.admitted,
+                           "done": t, "latency": t - (a.req.arrival if realtime else 0.0), "ctas": a.ctas,
+                           "status": int(s.status_host[0]) | int(s.status_host[1])}
+                    if self.keep_results:
+                        rec["U"] = s.U_host.numpy().copy()
+                        rec["P"] = s.P_host.numpy().copy()
+                    done.append(rec)
+                    active.remove(a)
+                    used -= a.ctas
+                    self.pool[s.n].append(s)
+                    free_streams.append(a.stream)
+        wall = time.perf_counter() - t0
+        lat = np.array([d["latency"] for d in done])
+        steps = sum(r.steps for r in reqs)
+        return done, {"requests": len(done), "wall_s": wall, "solves_per_s": len(done) / wall,
+                      "steps_per_s": steps / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                      "p99_ms": float(np.percentile(lat, 99) * 1e3), "capacity_ctas": self.capacity,
+                      "share_ctas": self.share}
+
+
+def run_plain(requests, server=None):
+    """The plain FP64 path: the same requests one after another on the whole
+    device (full CTA capacity), each synchronised before the next; returns
+    (records, metrics) like Server.run."""
+    srv = server or Server()
+    srv.warm(sorted({r.n for r in requests}))
+    done = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = torch.cuda.current_stream()
+    for r in requests:
+        slot = srv._take_slot(r.n)
+        slot.set_ctas(0)
+        slot.U0_host.copy_(torch.from_numpy(r.U0))
+        slot.U[0].copy_(slot.U0_host, non_blocking=True)
+        slot.P[0].zero_()
+        cur = slot.steps(0, r.steps, r.dt, r.nu, st)
+        slot.U_host.copy_(slot.U[cur])
+        slot.P_host.copy_(slot.P[cur])
+        t = time.perf_counter() - t0
+        rec = {"rid": r.rid, "n": r.n, "done": t, "latency": t - (done[-1]["done"] if done else 0.0),
+               "status": int(slot.solver.status.max().item())}
+        if srv.keep_results:
+            rec["U"] = slot.U_host.numpy().copy()
+            rec["P"] = slot.P_host.numpy().copy()
+        done.append(rec)
+        srv.pool[r.n].append(slot)
+    wall = time.perf_counter() - t0
+    steps = sum(r.steps for r in requests)
+    lat = np.array([d["latency"] for d in done])
+    return done, {"requests": len(done), "wall_s": wall, "solves_per_s": len(done) / wall,
+                  "steps_per_s": steps / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                  "p99_ms": float(np.percentile(lat, 99) * 1e3)}
