@@ -336,8 +336,10 @@ __device__ __forceinline__ bool fem_counter_barrier(const FemSync* s, unsigned i
           }
         }
       }
+      // a timeout raised by another party; a team of one CTA has none, and
+      // skips this global-memory round trip
+      if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
     }
-    if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
     s_ok = ok;
     if (s->trace && blockIdx.x == 0) fem_trace_put(s->trace, s->trace_cap, tag);
   }
