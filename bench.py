@@ -319,9 +319,13 @@ def serving(count, steps):
     srv.prewarm(reqs)
     bad = lambda d: sum(1 for x in d if x["status"] != 0)
     dp, plain = run_plain(reqs, srv)
-    ds, sat = srv.run(reqs, realtime=False)
+    ds, fixed = srv.run(reqs, realtime=False)
+    tune = srv.autotune(reqs)
+    srv.prewarm(reqs)
+    ds2, sat = srv.run(reqs, realtime=False)
     out = {"workload": f"{count} requests x {steps} steps, Q1 {{32,64,128,256}}^2 wall-bounded, FP64",
-           "plain": dict(plain, failed=bad(dp)), "served_saturated": dict(sat, failed=bad(ds)),
+           "plain": dict(plain, failed=bad(dp)), "served_saturated_untuned": dict(fixed, failed=bad(ds)),
+           "autotune": tune, "served_saturated": dict(sat, failed=bad(ds2)),
            "speedup_solves_per_s": sat["solves_per_s"] / plain["solves_per_s"]}
     for frac in (0.5, 0.9):
         rate = frac * sat["solves_per_s"]

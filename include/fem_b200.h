@@ -292,6 +292,23 @@ int fem_ctx_set_trace(fem_ctx* ctx, unsigned long long* buf, int cap);
  * counterpart: the reference runs one problem at a time. */
 int fem_ctx_set_max_ctas(fem_ctx* ctx, int ctas, int* capacity);
 
+/* nsteps (even, >= 2) consecutive fem_step4 calls captured into one CUDA
+ * graph: step k reads (U0,P0) and writes (U1,P1) for even k and the reverse
+ * for odd k, so after a launch the result is back in (U0,P0). Every argument
+ * has fem_step4's meaning and is fixed in the graph (pointers and scalars): a
+ * new dt or mu needs a new graph. iters / status receive each step's values
+ * (the last step's remain). Nothing runs at capture; fem_graph_launch replays
+ * the steps on any stream, fem_graph_destroy frees the graph. The context must
+ * not have stage timing enabled (FEM_E_STATE). A graph and direct calls on the
+ * same context must not overlap, as for two direct calls. No reference
+ * counterpart: it replaces the host launches of a chunk of time steps. */
+typedef struct fem_graph fem_graph;
+int fem_step4_graph(fem_ctx* ctx, double* U0, double* P0, double* U1, double* P1, double dt, double rho, double mu,
+                    const double* Ud, const double* Fp, const double* F, double tol, int precond, int nsteps,
+                    int* iters, int* status, fem_graph** out);
+int fem_graph_launch(fem_graph* graph, cudaStream_t stream);
+int fem_graph_destroy(fem_graph* graph);
+
 /* Number of this library's kernel launches issued so far in this process. */
 long long fem_launch_count(void);
 

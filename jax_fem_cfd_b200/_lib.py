@@ -61,6 +61,10 @@ SIGNATURES = {
     "fem_ctx_stage_times": (c_int, [P, P, c_int]),
     "fem_ctx_set_trace": (c_int, [P, P, c_int]),
     "fem_ctx_set_max_ctas": (c_int, [P, c_int, P]),
+    "fem_step4_graph": (c_int, [P, P, P, P, P, c_double, c_double, c_double, P, P, P, c_double, c_int, c_int, P, P,
+                                P]),
+    "fem_graph_launch": (c_int, [P, P]),
+    "fem_graph_destroy": (c_int, [P]),
     "fem_launch_count": (c_longlong, []),
     "fem_last_error": (ctypes.c_char_p, []),
 }

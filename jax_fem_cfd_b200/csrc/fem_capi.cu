@@ -133,6 +133,13 @@ struct fem_ctx {
   cudaEvent_t ev[16] = {};
   unsigned long long* trace = nullptr;
   int trace_cap = 0;
+  cudaStream_t cap_stream = nullptr;  // private stream for graph captures (fem_step4_graph)
+};
+
+struct fem_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
 };
 
 static inline void stage_mark(fem_ctx* c, cudaStream_t s) {
@@ -246,6 +253,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   cudaDeviceSynchronize();
   for (int i = 0; i < 16; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
@@ -992,6 +1000,73 @@ extern "C" int fem_ctx_set_trace(fem_ctx* c, unsigned long long* buf, int cap) {
   if (!c || cap < 0 || (cap > 0 && !buf)) return FEM_E_ARG;
   c->trace = cap > 0 ? buf : nullptr;
   c->trace_cap = cap;
+  return FEM_OK;
+}
+
+// ------------------------------------------------------ captured steps ----
+
+extern "C" int fem_step4_graph(fem_ctx* c, double* U0, double* P0, double* U1, double* P1, double dt, double rho,
+                               double mu, const double* Ud, const double* Fp, const double* F, double tol, int precond,
+                               int nsteps, int* iters, int* status, fem_graph** out) {
+  if (!c || !out || !U0 || !P0 || !U1 || !P1 || nsteps < 2 || (nsteps & 1)) return FEM_E_ARG;
+  if (c->timing) return FEM_E_STATE;  // stage events cannot be captured
+  *out = nullptr;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  FEM_CHECK(cudaSetDevice(c->device));
+  int rc = FEM_OK;
+  if (!c->cap_stream) {
+    const cudaError_t e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = set_err("cudaStreamCreateWithFlags", e);
+  }
+  // thread-local capture: work that other host threads issue meanwhile is not captured
+  if (rc == FEM_OK) {
+    const cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) rc = set_err("cudaStreamBeginCapture", e);
+  }
+  if (rc != FEM_OK) {
+    cudaSetDevice(prev);
+    return rc;
+  }
+  for (int k = 0; k < nsteps && rc == FEM_OK; ++k) {
+    const bool even = (k & 1) == 0;
+    rc = fem_step4(c, even ? U0 : U1, even ? P0 : P1, dt, rho, mu, Ud, Fp, F, tol, precond, even ? U1 : U0,
+                   even ? P1 : P0, iters, status, c->cap_stream);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e_end = cudaStreamEndCapture(c->cap_stream, &graph);
+  if (rc == FEM_OK && e_end != cudaSuccess) rc = set_err("cudaStreamEndCapture", e_end);
+  cudaGraphExec_t exec = nullptr;
+  if (rc == FEM_OK) {
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) rc = set_err("cudaGraphInstantiate", e);
+  }
+  if (rc != FEM_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();  // a failed capture leaves no sticky error behind
+    cudaSetDevice(prev);
+    return rc;
+  }
+  fem_graph* g = new fem_graph;
+  g->graph = graph;
+  g->exec = exec;
+  g->device = c->device;
+  *out = g;
+  cudaSetDevice(prev);
+  return FEM_OK;
+}
+
+extern "C" int fem_graph_launch(fem_graph* g, cudaStream_t s) {
+  if (!g || !g->exec) return FEM_E_ARG;
+  FEM_CHECK(cudaGraphLaunch(g->exec, s));
+  return FEM_OK;
+}
+
+extern "C" int fem_graph_destroy(fem_graph* g) {
+  if (!g) return FEM_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
   return FEM_OK;
 }
 

@@ -21,7 +21,11 @@ The request loop (`Server.run`) is continuous batching, not a queue:
   size, so nothing is allocated or freed while requests run.
 - Every admitted request runs on its own CUDA stream, in chunks of steps; up to
   two chunks per request are queued at a time, so the requests' kernels
-  overlap on the device and a new arrival is never behind a long queue.
+  overlap on the device and a new arrival is never behind a long queue. A
+  chunk is one launch of a CUDA graph captured for the request at admission
+  (fem_step4_graph: the chunk's steps with the request's dt and viscosity).
+- The CTA cap of a request can be picked by `Server.autotune`, which serves a
+  short sample of the stream under a few caps and keeps the fastest.
 - A request's CTA share depends only on its mesh size, so its results are the
   same (bit for bit) alone and in any mix: the solver's reductions are
   deterministic for a given grid.
@@ -135,6 +139,15 @@ class Slot:
         _lib.call("fem_ctx_set_max_ctas", self.solver.ctx.handle, int(ctas), ctypes.byref(cap))
         return cap.value
 
+    def graph(self, steps, dt, mu):
+        """A captured chunk of `steps` (even) steps from and back to buffer 0."""
+        s = self.solver
+        h = ctypes.c_void_p()
+        _lib.call("fem_step4_graph", s.ctx.handle, ptr(self.U[0]), ptr(self.P[0]), ptr(self.U[1]), ptr(self.P[1]),
+                  float(dt), 1.0, float(mu), ptr(self.ud), None, None, float(s.cfg.solver_tol), s.precond,
+                  int(steps), ptr(self.iters), ptr(s.status), ctypes.byref(h))
+        return h
+
     def steps(self, cur, k, dt, mu, stream):
         """k steps from buffer `cur`; returns the buffer holding the result."""
         s, h = self.solver, ctypes.c_void_p(stream.cuda_stream)
@@ -148,11 +161,12 @@ class Slot:
 
 
 class _Active:
-    __slots__ = ("req", "slot", "stream", "cur", "enq", "events", "final", "admitted", "ctas")
+    __slots__ = ("req", "slot", "stream", "cur", "enq", "events", "final", "admitted", "ctas", "graph")
 
     def __init__(self, req, slot, stream, ctas):
         self.req, self.slot, self.stream, self.ctas = req, slot, stream, ctas
         self.cur, self.enq, self.events, self.final, self.admitted = 0, 0, [], None, 0.0
+        self.graph = None
 
 
 def ctas_for(n, share):
@@ -169,9 +183,12 @@ class Server:
     solver CTAs per SM, 148 on a B200); chunk: steps per queued chunk;
     hbm_reserve: bytes kept free when building a new solver."""
 
-    def __init__(self, share=37, chunk=10, hbm_reserve=2 << 30, keep_results=True):
-        self.share, self.chunk, self.hbm_reserve = share, chunk, hbm_reserve
+    def __init__(self, share=37, chunk=10, hbm_reserve=2 << 30, keep_results=True, graphs=True):
+        self.share, self.chunk, self.hbm_reserve = share, chunk + (chunk & 1), hbm_reserve
         self.keep_results = keep_results
+        self.graphs = graphs
+        self.graph_error = None
+        self.share_by_size = {}  # n -> fixed CTA share of that size, overriding the cap
         self.pool = {}        # n -> idle Slots
         self.footprint = {}   # n -> device bytes of one Slot
         self.streams = []
@@ -188,6 +205,32 @@ class Server:
         self.capacity = cap if self.capacity is None else min(self.capacity, cap)
         return slot
 
+    def ctas(self, n):
+        return self.share_by_size.get(n) or ctas_for(n, self.share)
+
+    def autotune(self, requests, caps=(8, 16, 37, 74), sample=16, sample_steps=20):
+        """Pick the CTA cap of one request by serving a sample of the stream:
+        the first `sample` requests, cut to `sample_steps` steps each, all at
+        t = 0, once per cap in `caps`; the cap with the most solves per second
+        is kept (self.share). A per-size optimum of steps per second per CTA
+        would favour tiny shares and leave the largest requests to set the
+        makespan, so the tuning runs the actual mix. Returns the table."""
+        import dataclasses
+        trial = [dataclasses.replace(r, steps=min(r.steps, sample_steps), arrival=0.0) for r in requests[:sample]]
+        keep = self.keep_results
+        self.keep_results = False
+        self.share_by_size = {}
+        table = {}
+        for cap in caps:
+            self.share = cap
+            self.prewarm(trial)
+            self.run(trial, realtime=False)  # first pass: graph and stream set-up
+            _, m = self.run(trial, realtime=False)
+            table[cap] = m["solves_per_s"]
+        self.share = max(table, key=table.get)
+        self.keep_results = keep
+        return {"picked": self.share, "sample_solves_per_s": table, "sample": f"{len(trial)} x {sample_steps} steps"}
+
     def warm(self, sizes):
         """Build one pooled solver per size before the clock starts."""
         for n in sizes:
@@ -201,7 +244,7 @@ class Server:
         sizes = sorted({r.n for r in requests})
         self.warm(sizes)
         for n in sizes:
-            want = min(sum(r.n == n for r in requests), max(1, self.capacity // ctas_for(n, self.share)))
+            want = min(sum(r.n == n for r in requests), max(1, self.capacity // self.ctas(n)))
             have = len(self.pool[n])
             for _ in range(want - have):
                 self.pool[n].append(self._new_slot(n))
@@ -234,7 +277,7 @@ class Server:
             # admission: FIFO, while the head fits in CTAs and memory
             while pending:
                 r = pending[0]
-                c = ctas_for(r.n, self.share)
+                c = self.ctas(r.n)
                 if used + c > self.capacity:
                     break
                 slot = self._take_slot(r.n)
@@ -252,6 +295,11 @@ class Server:
                 with torch.cuda.stream(a.stream):
                     slot.U[0].copy_(slot.U0_host, non_blocking=True)
                     slot.P[0].zero_()
+                if self.graphs and r.steps >= self.chunk:
+                    try:
+                        a.graph = slot.graph(self.chunk, r.dt, r.nu)
+                    except _lib.FemError as e:  # capture unsupported here: launch the steps directly
+                        self.graphs, self.graph_error = False, str(e)
                 used += c
                 active.append(a)
             # feed and retire
@@ -259,7 +307,10 @@ class Server:
                 a.events = [e for e in a.events if not e.query()]
                 if a.enq < a.req.steps and len(a.events) < 2:
                     k = min(self.chunk, a.req.steps - a.enq)
-                    a.cur = a.slot.steps(a.cur, k, a.req.dt, a.req.nu, a.stream)
+                    if a.graph is not None and k == self.chunk and a.cur == 0:
+                        _lib.call("fem_graph_launch", a.graph, ctypes.c_void_p(a.stream.cuda_stream))
+                    else:
+                        a.cur = a.slot.steps(a.cur, k, a.req.dt, a.req.nu, a.stream)
                     a.enq += k
                     ev = torch.cuda.Event()
                     ev.record(a.stream)
@@ -282,6 +333,8 @@ class Server:
                         rec["U"] = s.U_host.numpy().copy()
                         rec["P"] = s.P_host.numpy().copy()
                     done.append(rec)
+                    if a.graph is not None:
+                        _lib.call("fem_graph_destroy", a.graph)
                     active.remove(a)
                     used -= a.ctas
                     self.pool[s.n].append(s)
@@ -292,7 +345,8 @@ class Server:
         return done, {"requests": len(done), "wall_s": wall, "solves_per_s": len(done) / wall,
                       "steps_per_s": steps / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
                       "p99_ms": float(np.percentile(lat, 99) * 1e3), "capacity_ctas": self.capacity,
-                      "share_ctas": self.share}
+                      "share_ctas": {n: self.ctas(n) for n in sorted({r.n for r in reqs})},
+                      "graphs": self.graphs, "graph_error": self.graph_error}
 
 
 def run_plain(requests, server=None):

@@ -110,3 +110,24 @@ def test_share_changes_grid_but_not_the_solution(_cuda):
     for d in plain:
         assert rel(s[d["rid"]]["U"], d["U"]) < SOLVE_TOL
         assert rel(s[d["rid"]]["P"], d["P"]) < SOLVE_TOL
+
+
+@pytest.mark.gpu
+def test_autotuned_shares_and_graph_chunks(_cuda):
+    """The autotuner picks a cap from its candidates; chunks replayed from
+    captured graphs give the same bits as the same steps launched one by one."""
+    from jax_fem_cfd_b200.serving import Server, make_requests
+    srv = Server(chunk=2)
+    reqs = make_requests(4, seed=4, sizes=(32, 64), steps=5)
+    t = srv.autotune(reqs, caps=(4, 8), sample=3, sample_steps=2)
+    assert t["picked"] in (4, 8) and srv.share == t["picked"]
+    graphed, m = srv.run(reqs)
+    assert m["graphs"], m["graph_error"]
+    direct = Server(share=srv.share, chunk=2, graphs=False)
+    plain, m2 = direct.run(reqs)
+    assert not m2["graphs"]
+    g = {d["rid"]: d for d in graphed}
+    for d in plain:
+        assert d["status"] == 0 and g[d["rid"]]["status"] == 0
+        np.testing.assert_array_equal(d["U"], g[d["rid"]]["U"])
+        np.testing.assert_array_equal(d["P"], g[d["rid"]]["P"])
