@@ -149,6 +149,52 @@ def test_multigrid_transfers_and_vcycle(key):
     assert rel(z, g["z"]) < (1e-9 if setzero else 1e-12), rel(z, g["z"])
 
 
+@pytest.mark.parametrize("ctas", [0, 8])
+def test_pinned_poisson_solve_tiles(ctas):
+    """MG-PCG pressure solve (core/multigrid.py + solvers/standard.py:85-125,
+    pinned node 0, tol 1e-8) on a 128^2 Q1 lattice vs the oracle. ctas = 8
+    caps the grid so that phase A has more tiles than CTAs and the kernel
+    stages a CTA's next tile while it applies the current one; 0 is the
+    default grid (one tile round)."""
+    import ctypes
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import Context, Mesh, make_mask, ptr, stream
+    from jax_fem_cfd_b200.core import multigrid as gmg
+    from oracle import emult as oem, mesh as om, multigrid as omg, shape as osh, solvers as osv
+    n = 128
+    ctx = Context(Mesh(0, False, n, n, 1, 1.0, 1.0))
+    ctx.set_bc(None, make_mask(np.array([0]), ctx.nn), True)
+    nlev = int(np.log2(n // 4)) + 1
+    gmg.Hierarchy(ctx, nlev, [np.array([0])] * nlev, 1e-8)
+    _lib.call("fem_ctx_set_max_ctas", ctx.handle, ctas, None)
+    b = np.random.default_rng(7).standard_normal(ctx.nn)
+    b[0] = 0.0
+    bg = torch.as_tensor(b, device="cuda")
+    x = torch.zeros_like(bg)
+    it = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("fem_pressure_solve", ctx.handle, ptr(bg), ptr(x), 1e-8, 0.0, 1000, _lib.PREC["multigrid"], 0, 1,
+              ptr(it), ptr(st), stream())
+    nc, nconn, *_ = om.create_mesh_2d(n, n, 1.0, 1.0)
+    wq, N, Nd = osh.quad4_shape_functions(nc[nconn[0]])
+    data = omg.multigrid_setup([n, n], [4, 4], [1.0, 1.0], [], om.create_mesh_2d, osh.quad4_shape_functions, 1, None)
+    from oracle import element as oel
+    Le = oel.laplacian_element_calc(wq, Nd)
+
+    def lhs(v):
+        y = oem.laplacian_element_mult(v, Le, nconn, nc.shape[0])
+        y[0] = 0.0
+        return y
+
+    xo, ito = osv.cg(lhs, b, x0=np.zeros_like(b), tol=1e-8, maxiter=1000,
+                     M=lambda r: omg.v_cycle(r, *data, 1e-8, False, True))
+    xo = xo.copy()
+    xo[0] = 0.0
+    assert int(st.item()) == 0
+    assert int(it.item()) == int(ito)
+    assert rel(x, xo) < SOLVE_TOL
+
+
 def test_generic_krylov_callables():
     """utils.iterative_solvers.cg / bicgstab with callable operators vs the goldens."""
     from jax_fem_cfd_b200.core import element_calc as ec
