@@ -309,6 +309,15 @@ int fem_step4_graph(fem_ctx* ctx, double* U0, double* P0, double* U1, double* P1
 int fem_graph_launch(fem_graph* graph, cudaStream_t stream);
 int fem_graph_destroy(fem_graph* graph);
 
+/* Self-test of failure detection (diagnostics, about 2 s on the GPU): one
+ * CTA waits at the solvers' grid barrier for a party that never arrives, so
+ * the wait ends only by the barrier's time limit, which sets the timeout bit
+ * of the context's error word and returns, as in a solver. *status (device
+ * int) receives FEM_STATUS_BARRIER_TIMEOUT; the context stays usable, since
+ * every solve clears the error word first. No reference counterpart (the
+ * reference has no device-side waits). */
+int fem_selftest_barrier_timeout(fem_ctx* ctx, int* status, cudaStream_t stream);
+
 /* Number of this library's kernel launches issued so far in this process. */
 long long fem_launch_count(void);
 

@@ -92,6 +92,8 @@ int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double
 int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc,
                           double alpha, const double* Ash, const double* x, double* y, int grid, cudaStream_t s);
 
+int fem_launch_selftest_barrier(const FemSync& sync, int* status, cudaStream_t s);
+
 int fem_coop_occupancy_cg(int* occ);
 int fem_coop_occupancy_bi(int* occ);
 int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s);

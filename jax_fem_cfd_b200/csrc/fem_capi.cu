@@ -9,8 +9,16 @@
 #include <mutex>
 #include <new>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "fem_b200.h"
 #include "fem_args.cuh"
+
+// NVTX range over one host entry point (a no-op unless a profiler is attached)
+struct FemRange {
+  explicit FemRange(const char* name) { nvtxRangePushA(name); }
+  ~FemRange() { nvtxRangePop(); }
+};
 
 static std::atomic<long long> g_launches{0};
 static thread_local char g_err[256] = "";
@@ -729,6 +737,7 @@ static int run_cg(fem_ctx* c, const double* b, double* x, double tol, double ato
 
 extern "C" int fem_pressure_solve(fem_ctx* c, const double* b, double* x, double tol, double atol, int maxiter,
                                   int precond, int center_rhs, int post, int* iters, int* status, cudaStream_t s) {
+  const FemRange range("fem_pressure_solve");
   if (!c || !b || !x || !iters || !status || precond < 0 || precond > 4 || maxiter < 0) return FEM_E_ARG;
   if (precond == FEM_PREC_MG && c->nlev < 2) return FEM_E_STATE;
   return run_cg(c, b, x, tol, atol, maxiter, precond, center_rhs, post, iters, status, s);
@@ -780,6 +789,7 @@ extern "C" int fem_bicgstab_solve(fem_ctx* c, int ncomp, double alpha, const dou
                                   const double* B, double gamma, const double* C, const uint8_t* mask,
                                   const double* b, double* x, double tol, double atol, int maxiter, int* iters,
                                   int* status, cudaStream_t s) {
+  const FemRange range("fem_bicgstab_solve");
   if (!c || !b || !x || !iters || !status) return FEM_E_ARG;
   const MatCombo op{Ash, alpha, B, beta, 0, C, gamma};
   return run_bicgstab(c, ncomp, op, mask, b, x, tol, atol, maxiter, iters, status, s);
@@ -788,6 +798,7 @@ extern "C" int fem_bicgstab_solve(fem_ctx* c, int ncomp, double alpha, const dou
 extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double dt, double rho, double mu,
                          const double* Ud, const double* Fp, const double* F, double tol, int precond, double* Uo,
                          double* Po, int* iters, int* status, cudaStream_t s) {
+  const FemRange range("fem_step4");
   if (!c || !Un || !Pn || !Uo || !Po || !iters || !status) return FEM_E_ARG;
   if (c->has_dmask && !Ud) return FEM_E_ARG;
   if (precond < 0 || precond > 4) return FEM_E_ARG;
@@ -1068,6 +1079,13 @@ extern "C" int fem_graph_destroy(fem_graph* g) {
   if (g->graph) cudaGraphDestroy(g->graph);
   delete g;
   return FEM_OK;
+}
+
+extern "C" int fem_selftest_barrier_timeout(fem_ctx* c, int* status, cudaStream_t s) {
+  if (!c || !status) return FEM_E_ARG;
+  FEM_TRY(reset_sync(c, s));
+  const FemSync S{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS, nullptr, 0};
+  return fem_launch_selftest_barrier(S, status, s);
 }
 
 extern "C" int fem_ctx_set_max_ctas(fem_ctx* c, int ctas, int* capacity) {

@@ -557,3 +557,21 @@ int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, con
   }
   return fem_after_launch("k_conv_apply");
 }
+
+// Self-test of the grid barrier's time limit: one CTA waits at a counter
+// barrier for one more party than the launch has, so the wait can only end
+// through the FEM_BARRIER_TIMEOUT_NS limit. It then sets FEM_ERR_BARRIER_TIMEOUT
+// in the error word and returns, as a solver kernel does; status receives the
+// error word (0 if the barrier had completed).
+__global__ void k_selftest_barrier(FemSync sync, int* __restrict__ status) {
+  __shared__ unsigned int round;
+  if (threadIdx.x == 0) round = 0u;
+  __syncthreads();
+  const bool ok = fem_counter_barrier(&sync, sync.count, &round, (int)gridDim.x + 1, 31u);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *status = ok ? 0 : (*(volatile int*)sync.err & FEM_ERR_BARRIER_TIMEOUT);
+}
+
+int fem_launch_selftest_barrier(const FemSync& sync, int* status, cudaStream_t s) {
+  k_selftest_barrier<<<1, 64, 0, s>>>(sync, status);
+  return fem_after_launch("k_selftest_barrier");
+}
