@@ -59,7 +59,9 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed
+    region: sampling is live before the region starts (the first sample is
+    waited for), and only the samples taken after that one are summarised."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -69,13 +71,22 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.path = tempfile.mktemp(suffix=".csv")
+        self.skip = 0
 
     def __enter__(self):
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.proc.poll() is None:
+                with open(self.path) as g:
+                    n = sum(1 for r in g if r.strip())
+                if n:
+                    self.skip = n
+                    break
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -94,6 +105,7 @@ class ClockSampler:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
         except Exception:
             rows = []
+        rows = rows[self.skip:] or rows
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[1]) for r in rows]
@@ -435,7 +447,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=256)
