@@ -67,8 +67,17 @@ __device__ __forceinline__ void fem_conv_element(const FemQuadTab& T, const doub
   double acc[NEN];
 #pragma unroll
   for (int a = 0; a < NEN; ++a) acc[a] = 0.0;
+  // the factors of Gauss point q + 1 are loaded while point q is evaluated (the
+  // loop stays rolled, so the loads would otherwise wait inside each iteration)
+  double f0 = fac(0), f1 = fac(1), f2 = fac(2);
 #pragma unroll 1
   for (int q = 0; q < NQ; ++q) {
+    double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+    if (q + 1 < NQ) {
+      n0 = fac(3 * q + 3);
+      n1 = fac(3 * q + 4);
+      n2 = fac(3 * q + 5);
+    }
     double xq = 0.0, gx = 0.0, gy = 0.0;
 #pragma unroll
     for (int b = 0; b < NEN; ++b) {
@@ -76,7 +85,10 @@ __device__ __forceinline__ void fem_conv_element(const FemQuadTab& T, const doub
       gx += T.dx[q][b] * xl[b];
       gy += T.dy[q][b] * xl[b];
     }
-    const double sq = (fac(3 * q) * gx + fac(3 * q + 1) * gy) + fac(3 * q + 2) * xq;
+    const double sq = (f0 * gx + f1 * gy) + f2 * xq;
+    f0 = n0;
+    f1 = n1;
+    f2 = n2;
 #pragma unroll
     for (int a = 0; a < NEN; ++a) acc[a] += T.N[q][a] * sq;
   }
