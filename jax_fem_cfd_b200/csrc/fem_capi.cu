@@ -279,6 +279,84 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   delete c;
 }
 
+// The 1D factors of a Q2 Gauss table (see FemQuadTab): by partition of unity,
+// nx[q][i] = N[q][(i,1)] / sum_i' N[q][(i',1)] and ny[q][j] likewise along the
+// middle column; the derivative factors divide dx / dy by the other direction's
+// middle value. Gauss points are grouped into columns qx and rows qy by equal
+// factors, and every entry of N, dx and dy is checked against the products
+// (relative 1e-12). Returns false if the table does not factor.
+static bool q2_tensor_factors(FemQuadTab& T) {
+  int node[3][3];
+  for (int b = 0; b < 9; ++b) node[(FEM_Q2_DI >> (2 * b)) & 3u][(FEM_Q2_DJ >> (2 * b)) & 3u] = b;  // [i][j]
+  double fx[9][3], fy[9][3], gx[9][3], gy[9][3];
+  for (int q = 0; q < 9; ++q) {
+    double sx = 0.0, sy = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      sx += T.N[q][node[k][1]];
+      sy += T.N[q][node[1][k]];
+    }
+    if (std::fabs(sx) < 1e-6 || std::fabs(sy) < 1e-6) return false;
+    const double mx = T.N[q][node[1][1]] / sy, my = T.N[q][node[1][1]] / sx;  // nx[q][1], ny[q][1]
+    if (std::fabs(mx) < 1e-6 || std::fabs(my) < 1e-6) return false;
+    for (int k = 0; k < 3; ++k) {
+      fx[q][k] = T.N[q][node[k][1]] / sx;
+      fy[q][k] = T.N[q][node[1][k]] / sy;
+      gx[q][k] = T.dx[q][node[k][1]] / sx;
+      gy[q][k] = T.dy[q][node[1][k]] / sy;
+    }
+  }
+  auto same = [](const double* a, const double* b) {
+    for (int k = 0; k < 3; ++k)
+      if (std::fabs(a[k] - b[k]) > 1e-12 * (1.0 + std::fabs(a[k]))) return false;
+    return true;
+  };
+  int colq[3], rowq[3], nc = 0, nr = 0, qxof[9], qyof[9];
+  for (int q = 0; q < 9; ++q) {
+    int cx = -1, cy = -1;
+    for (int k = 0; k < nc; ++k)
+      if (same(fx[q], fx[colq[k]])) cx = k;
+    for (int k = 0; k < nr; ++k)
+      if (same(fy[q], fy[rowq[k]])) cy = k;
+    if (cx < 0) {
+      if (nc == 3) return false;
+      colq[nc] = q;
+      cx = nc++;
+    }
+    if (cy < 0) {
+      if (nr == 3) return false;
+      rowq[nr] = q;
+      cy = nr++;
+    }
+    qxof[q] = cx;
+    qyof[q] = cy;
+  }
+  if (nc != 3 || nr != 3) return false;
+  int seen[3][3] = {};
+  for (int q = 0; q < 9; ++q) {
+    if (seen[qyof[q]][qxof[q]]++) return false;
+    T.qi[qyof[q]][qxof[q]] = q;
+  }
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 3; ++i) {
+      T.nx[k][i] = fx[colq[k]][i];
+      T.ddx[k][i] = gx[colq[k]][i];
+      T.ny[k][i] = fy[rowq[k]][i];
+      T.ddy[k][i] = gy[rowq[k]][i];
+    }
+  for (int q = 0; q < 9; ++q)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const int b = node[i][j], qx = qxof[q], qy = qyof[q];
+        const double n = T.nx[qx][i] * T.ny[qy][j], ddx = T.ddx[qx][i] * T.ny[qy][j],
+                     ddy = T.nx[qx][i] * T.ddy[qy][j];
+        const double sc = 1.0 + std::fabs(T.dx[q][b]) + std::fabs(T.dy[q][b]);
+        if (std::fabs(n - T.N[q][b]) > 1e-12 || std::fabs(ddx - T.dx[q][b]) > 1e-12 * sc ||
+            std::fabs(ddy - T.dy[q][b]) > 1e-12 * sc)
+          return false;
+      }
+  return true;
+}
+
 static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   if (!make_grid(m->kind, m->periodic, m->nex, m->ney, m->nez, c->g)) return FEM_E_ARG;
   c->device = device;
@@ -377,6 +455,9 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
     }
     const char* ev = getenv("FEM_CONV_OTF");
     c->conv_otf = (ev && atoi(ev) == 0) ? 0 : 1;
+    // Q2: the tensor factors of the on-the-fly operator; without them (a table
+    // that does not factor) fem_step4 builds Ce explicitly
+    if (g.kind == FEM_Q2_2D && !q2_tensor_factors(c->qt)) c->conv_otf = 0;
   }
   return FEM_OK;
 }

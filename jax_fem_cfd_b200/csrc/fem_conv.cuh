@@ -18,6 +18,11 @@ struct FemQuadTab {
   double N[FEM_QT_MAX][FEM_QT_MAX];   // [q][node]
   double dx[FEM_QT_MAX][FEM_QT_MAX];  // d N_node / dx at q
   double dy[FEM_QT_MAX][FEM_QT_MAX];  // d N_node / dy at q
+  // Q2 tensor factors (filled and checked on the host): N[q][b] = nx[qx][i] ny[qy][j],
+  // dx[q][b] = ddx[qx][i] ny[qy][j], dy[q][b] = nx[qx][i] ddy[qy][j] for node b at
+  // element-local lattice offset (i, j) and Gauss point q = qi[qy][qx]
+  double nx[3][3], ny[3][3], ddx[3][3], ddy[3][3];
+  int qi[3][3];
 };
 
 template <int KIND>
@@ -62,7 +67,12 @@ __device__ __forceinline__ void fem_conv_factors(const FemQuadTab& T, const doub
 template <int KIND, class Fac>
 __device__ __forceinline__ void fem_conv_element(const FemQuadTab& T, const double (&xl)[KI<KIND>::NEN],
                                                  const Fac& fac, double cc, double alpha, const double* Ash,
-                                                 double (&y)[KI<KIND>::NEN]) {
+                                                 double (&y)[KI<KIND>::NEN]);
+
+template <int KIND, class Fac>
+__device__ __forceinline__ void fem_conv_element_loop(const FemQuadTab& T, const double (&xl)[KI<KIND>::NEN],
+                                                      const Fac& fac, double cc, double alpha, const double* Ash,
+                                                      double (&y)[KI<KIND>::NEN]) {
   constexpr int NEN = KI<KIND>::NEN, NQ = KQ<KIND>::NQ;
   double acc[NEN];
 #pragma unroll
@@ -100,6 +110,79 @@ __device__ __forceinline__ void fem_conv_element(const FemQuadTab& T, const doub
       for (int b = 0; b < NEN; ++b) sh += Ash[a * NEN + b] * xl[b];
     }
     y[a] = alpha * sh + cc * acc[a];
+  }
+}
+
+// The same product for Q2 by sum factorisation over the tensor-product basis
+// (the factors in T.nx / T.ny / T.ddx / T.ddy): x is interpolated along x for
+// each node row (values and x-derivatives), then along y at each Gauss point,
+// and the test functions are applied along x and then y. 216 FMAs per element
+// row instead of 351, and a few table reads instead of ~320; the order of the
+// sums differs from fem_conv_element's, the values agree to rounding.
+template <class Fac>
+__device__ __forceinline__ void fem_conv_element_q2(const FemQuadTab& T, const double (&xl)[9], const Fac& fac,
+                                                    double cc, double alpha, const double* Ash, double (&y)[9]) {
+#pragma unroll
+  for (int a = 0; a < 9; ++a) {
+    double sh = 0.0;
+    if (Ash) {
+#pragma unroll
+      for (int b = 0; b < 9; ++b) sh += Ash[a * 9 + b] * xl[b];
+    }
+    y[a] = alpha * sh;
+  }
+  double U[3][3], V[3][3];  // [node row j][Gauss column qx]: values and x-derivatives
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    double X[3];
+#pragma unroll
+    for (int b = 0; b < 9; ++b)
+      if (kdj<FEM_Q2_2D>(b) == j) X[kdi<FEM_Q2_2D>(b)] = xl[b];
+#pragma unroll
+    for (int qx = 0; qx < 3; ++qx) {
+      U[j][qx] = (T.nx[qx][0] * X[0] + T.nx[qx][1] * X[1]) + T.nx[qx][2] * X[2];
+      V[j][qx] = (T.ddx[qx][0] * X[0] + T.ddx[qx][1] * X[1]) + T.ddx[qx][2] * X[2];
+    }
+  }
+  double acc[3][3];  // [i][j]
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc[i][j] = 0.0;
+#pragma unroll 1
+  for (int qy = 0; qy < 3; ++qy) {
+    const double y0 = T.ny[qy][0], y1 = T.ny[qy][1], y2 = T.ny[qy][2];
+    const double e0 = T.ddy[qy][0], e1 = T.ddy[qy][1], e2 = T.ddy[qy][2];
+    double wv[3] = {0.0, 0.0, 0.0};  // sum over qx of nx[qx][i] s(qx, qy)
+#pragma unroll
+    for (int qx = 0; qx < 3; ++qx) {
+      const double xq = (y0 * U[0][qx] + y1 * U[1][qx]) + y2 * U[2][qx];
+      const double gy = (e0 * U[0][qx] + e1 * U[1][qx]) + e2 * U[2][qx];
+      const double gx = (y0 * V[0][qx] + y1 * V[1][qx]) + y2 * V[2][qx];
+      const int q = T.qi[qy][qx];
+      const double sq = (fac(3 * q) * gx + fac(3 * q + 1) * gy) + fac(3 * q + 2) * xq;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) wv[i] += T.nx[qx][i] * sq;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      acc[i][0] += y0 * wv[i];
+      acc[i][1] += y1 * wv[i];
+      acc[i][2] += y2 * wv[i];
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 9; ++b) y[b] += cc * acc[kdi<FEM_Q2_2D>(b)][kdj<FEM_Q2_2D>(b)];
+}
+
+template <int KIND, class Fac>
+__device__ __forceinline__ void fem_conv_element(const FemQuadTab& T, const double (&xl)[KI<KIND>::NEN],
+                                                 const Fac& fac, double cc, double alpha, const double* Ash,
+                                                 double (&y)[KI<KIND>::NEN]) {
+  if constexpr (KIND == FEM_Q2_2D) {
+    fem_conv_element_q2(T, xl, fac, cc, alpha, Ash, y);
+  } else {
+    fem_conv_element_loop<KIND>(T, xl, fac, cc, alpha, Ash, y);
   }
 }
 
