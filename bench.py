@@ -270,7 +270,9 @@ def whole_job_rate(world, steps, max_total_ms):
 def poisson(n, solves=5):
     """MG-PCG Poisson solve on an n x n Q1 unit square: pinned node 0, seeded
     random rhs, x0 = 0, tol 1e-8, final MG mesh 4x4. Median of `solves` timed
-    solves after 3 warm-up solves, a 256 MiB L2 flush before each."""
+    solves after 3 warm-up solves, a 256 MiB L2 flush before each. The same for
+    the mixed-precision solve (fem_pressure_solve_mixed, same tolerance on the
+    FP64 residual); errors of both against an FP64 solve to 1e-12."""
     import torch
 
     from jax_fem_cfd_b200 import _lib
@@ -304,11 +306,37 @@ def poisson(n, solves=5):
     ms = float(np.median(times))
     iters = int(it.item())
     status = int(stt.item())
+    x64 = x.clone()
     byts = cg_algorithmic_bytes([ctx.level_info(l)[0] for l in range(ctx.nlev)], iters, None)
+    # reference solution for the error figures: FP64 MG-PCG to 1e-12 (untimed)
+    xr = torch.zeros_like(b)
+    _lib.call("fem_pressure_solve", ctx.handle, ptr(b), ptr(xr), 1e-12, 0.0, 1000, 4, 0, 1, ptr(it), ptr(stt),
+              stream())
+    # mixed precision: FP64 refinement around an FP32 MG-PCG (6 inner iterations), same tolerance
+    cyc, res = ctypes.c_int(0), ctypes.c_double(0.0)
+    mtimes = []
+    for k in range(3 + solves):
+        x.zero_()
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.call("fem_pressure_solve_mixed", ctx.handle, ptr(b), ptr(x), 1e-8, 6, 50, ctypes.byref(cyc),
+                  ctypes.byref(res), stream())
+        e.record()
+        torch.cuda.synchronize()
+        if k >= 3:
+            mtimes.append(s.elapsed_time(e))
+    mms = float(np.median(mtimes))
+    nr = float(torch.linalg.norm(xr))
+    err64 = float(torch.linalg.norm(x64 - xr)) / nr
+    errm = float(torch.linalg.norm(x - xr)) / nr
     del ctx
     return {"ms_per_solve": ms, "solves_per_s": 1000.0 / ms, "iterations": iters, "status": status,
             "elements": n * n, "nodes": (n + 1) ** 2, "algorithmic_bytes": byts,
-            "achieved_gbs": byts / ms / 1e6, "frac_of_hbm": byts / ms / 1e6 / hbm}
+            "achieved_gbs": byts / ms / 1e6, "frac_of_hbm": byts / ms / 1e6 / hbm, "rel_err_fp64": err64,
+            "mixed": {"ms_per_solve": mms, "solves_per_s": 1000.0 / mms, "speedup_vs_fp64": ms / mms,
+                      "cycles": cyc.value, "inner_iterations_per_cycle": 6, "fp64_relres": res.value,
+                      "rel_err": errm}}
 
 
 def poisson_sweep():

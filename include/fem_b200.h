@@ -309,6 +309,21 @@ int fem_step4_graph(fem_ctx* ctx, double* U0, double* P0, double* U1, double* P1
 int fem_graph_launch(fem_graph* graph, cudaStream_t stream);
 int fem_graph_destroy(fem_graph* graph);
 
+/* Mixed-precision pressure-Poisson solve of the context's pinned Q1 2D problem
+ * (the system of fem_pressure_solve with FEM_PREC_MG: gamma_p rows zeroed).
+ * FP64 iterative refinement, x += d after each cycle, until
+ * ||b - A x|| <= tol ||b|| or max_cycles cycles. The inner solve is `inner`
+ * iterations of a multigrid-preconditioned CG on FP32 vectors from d = 0; its
+ * coarsest level is solved in FP64. x (FP64, device) holds the initial guess on
+ * entry and is zeroed on gamma_p at the end. *cycles and *relres (host) receive
+ * the cycle count and the final relative FP64 residual; the call waits for the
+ * stream once per cycle to read the residual norm. It needs the context's
+ * multigrid hierarchy (fem_ctx_setup_multigrid) with a coarsest level of at most
+ * 128 nodes (FEM_E_STATE otherwise), and allocates its FP32 work vectors on the
+ * first call. No reference counterpart: the reference solves in FP64 only. */
+int fem_pressure_solve_mixed(fem_ctx* ctx, const double* b, double* x, double tol, int inner, int max_cycles,
+                             int* cycles, double* relres, cudaStream_t stream);
+
 /* Self-test of failure detection (diagnostics, about 2 s on the GPU): one
  * CTA waits at the solvers' grid barrier for a party that never arrives, so
  * the wait ends only by the barrier's time limit, which sets the timeout bit

@@ -62,6 +62,7 @@ SIGNATURES = {
     "fem_ctx_set_trace": (c_int, [P, P, c_int]),
     "fem_ctx_set_max_ctas": (c_int, [P, c_int, P]),
     "fem_selftest_barrier_timeout": (c_int, [P, P, P]),
+    "fem_pressure_solve_mixed": (c_int, [P, P, P, c_double, c_int, c_int, P, P, P]),
     "fem_step4_graph": (c_int, [P, P, P, P, P, c_double, c_double, c_double, P, P, P, c_double, c_int, c_int, P, P,
                                 P]),
     "fem_graph_launch": (c_int, [P, P]),

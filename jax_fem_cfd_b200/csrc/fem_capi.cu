@@ -142,6 +142,8 @@ struct fem_ctx {
   unsigned long long* trace = nullptr;
   int trace_cap = 0;
   cudaStream_t cap_stream = nullptr;  // private stream for graph captures (fem_step4_graph)
+  float* mx32 = nullptr;              // FP32 vectors of the mixed-precision solve (first use)
+  double* mx64 = nullptr;             // its partial sums and scalars
 };
 
 struct fem_graph {
@@ -262,6 +264,8 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   for (int i = 0; i < 16; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  if (c->mx32) cudaFree(c->mx32);
+  if (c->mx64) cudaFree(c->mx64);
   void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
@@ -1160,6 +1164,24 @@ extern "C" int fem_graph_destroy(fem_graph* g) {
   if (g->graph) cudaGraphDestroy(g->graph);
   delete g;
   return FEM_OK;
+}
+
+extern "C" int fem_pressure_solve_mixed(fem_ctx* c, const double* b, double* x, double tol, int inner,
+                                        int max_cycles, int* cycles, double* relres, cudaStream_t s) {
+  const FemRange range("fem_pressure_solve_mixed");
+  if (!c || !b || !x || !(tol > 0.0) || inner < 1 || max_cycles < 1) return FEM_E_ARG;
+  if (c->g.kind != FEM_Q1_2D || !c->set_zeroP || c->nlev < 2) return FEM_E_STATE;
+  if (c->lv[c->nlev - 1].g.nn > 128) return FEM_E_STATE;  // the one-warp coarse CG
+  const int grid = c->sms * 8;
+  if (!c->mx32) {
+    size_t nf = 3 * (size_t)c->lv[0].g.nn;
+    for (int l = 0; l < c->nlev; ++l) nf += 3 * (size_t)c->lv[l].g.nn;
+    FEM_ALLOC(c->mx32, nf);
+    FEM_ALLOC(c->mx64, (size_t)grid + 8);
+  }
+  CgArgs A;
+  fill_cg_args(c, A);
+  return fem_mixed_poisson(A, grid, c->mx32, c->mx64, b, x, tol, inner, max_cycles, cycles, relres, s);
 }
 
 extern "C" int fem_selftest_barrier_timeout(fem_ctx* c, int* status, cudaStream_t s) {

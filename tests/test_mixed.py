@@ -1,0 +1,105 @@
+"""Mixed-precision pressure-Poisson solve (FP64 refinement around an FP32
+MG-PCG): its solution agrees with the FP64 MG-PCG solve and with the oracle
+to 1e-6 (the mixed path's stated bound), its FP64 residual reaches the
+tolerance, it is deterministic, and it refuses a problem it does not cover."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from tests.test_gpu_parity import rel
+
+
+def _poisson(n, seed=5):
+    from jax_fem_cfd_b200.context import Context, Mesh, make_mask
+    from jax_fem_cfd_b200.core import multigrid as gmg
+    ctx = Context(Mesh(0, False, n, n, 1, 1.0, 1.0))
+    ctx.set_bc(None, make_mask(np.array([0]), ctx.nn), True)
+    nlev = int(np.log2(n // 4)) + 1
+    gmg.Hierarchy(ctx, nlev, [np.array([0])] * nlev, 1e-8)
+    b = np.random.default_rng(seed).standard_normal(ctx.nn)
+    b[0] = 0.0
+    return ctx, b
+
+
+def _mixed(ctx, b, tol=1e-10, inner=6):
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import ptr, stream
+    bg = torch.as_tensor(b, device="cuda")
+    x = torch.zeros_like(bg)
+    cyc, res = ctypes.c_int(0), ctypes.c_double(0.0)
+    _lib.call("fem_pressure_solve_mixed", ctx.handle, ptr(bg), ptr(x), tol, inner, 20, ctypes.byref(cyc),
+              ctypes.byref(res), stream())
+    torch.cuda.synchronize()
+    return x.cpu().numpy(), cyc.value, res.value
+
+
+def _fp64(ctx, b):
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import ptr, stream
+    bg = torch.as_tensor(b, device="cuda")
+    x = torch.zeros_like(bg)
+    it = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("fem_pressure_solve", ctx.handle, ptr(bg), ptr(x), 1e-10, 0.0, 1000, _lib.PREC["multigrid"], 0, 1,
+              ptr(it), ptr(st), stream())
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    return x.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [32, 128, 256])
+def test_mixed_matches_fp64_and_is_deterministic(_cuda, n):
+    ctx, b = _poisson(n)
+    xm, cycles, res = _mixed(ctx, b)
+    assert res <= 1e-10 and 1 <= cycles <= 6, (res, cycles)
+    x64 = _fp64(ctx, b)
+    assert rel(xm, x64) < 1e-6, rel(xm, x64)
+    assert xm[0] == 0.0
+    xm2, _, _ = _mixed(ctx, b)
+    np.testing.assert_array_equal(xm, xm2)
+
+
+@pytest.mark.gpu
+def test_mixed_matches_the_oracle(_cuda):
+    from oracle import element as oel, emult as oem, mesh as om, multigrid as omg, shape as osh, solvers as osv
+    n = 64
+    ctx, b = _poisson(n, seed=8)
+    xm, _, _ = _mixed(ctx, b)
+    nc, nconn, *_ = om.create_mesh_2d(n, n, 1.0, 1.0)
+    wq, N, Nd = osh.quad4_shape_functions(nc[nconn[0]])
+    Le = oel.laplacian_element_calc(wq, Nd)
+    data = omg.multigrid_setup([n, n], [4, 4], [1.0, 1.0], [], om.create_mesh_2d, osh.quad4_shape_functions, 1, None)
+
+    def lhs(v):
+        y = oem.laplacian_element_mult(v, Le, nconn, nc.shape[0])
+        y[0] = 0.0
+        return y
+
+    xo, _ = osv.cg(lhs, b, x0=np.zeros_like(b), tol=1e-10, maxiter=1000,
+                   M=lambda r: omg.v_cycle(r, *data, 1e-8, False, True))
+    xo = xo.copy()
+    xo[0] = 0.0
+    assert rel(xm, xo) < 1e-6, rel(xm, xo)
+
+
+@pytest.mark.gpu
+def test_mixed_refuses_a_mean_zero_problem(_cuda):
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import Context, Mesh, make_mask, ptr, stream
+    from jax_fem_cfd_b200.core import multigrid as gmg
+    ctx = Context(Mesh(0, False, 32, 32, 1, 1.0, 1.0))
+    ctx.set_bc(None, make_mask(np.array([0]), ctx.nn), False)  # mean-zero pressure: not covered
+    gmg.Hierarchy(ctx, 4, [np.array([0])] * 4, 1e-8)
+    b = torch.zeros(ctx.nn, dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.FemError):
+        _lib.call("fem_pressure_solve_mixed", ctx.handle, ptr(b), ptr(b), 1e-8, 4, 4, None, None, stream())
