@@ -93,7 +93,7 @@ int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, con
                           double alpha, const double* Ash, const double* x, double* y, int grid, cudaStream_t s);
 
 int fem_launch_selftest_barrier(const FemSync& sync, int* status, cudaStream_t s);
-// mixed-precision pinned Poisson solve (k_mixed.cu); work: 3 sum(nn_l) + 3 nn_0
+// mixed-precision pinned Poisson solve (k_mixed.cu); work: 6 sum(nn_l) + 3 nn_0
 // floats, dwork: grid + 8 doubles
 int fem_mixed_poisson(const CgArgs& A, int grid, float* work, double* dwork, const double* b, double* x, double tol,
                       int inner, int max_cycles, int* cycles, double* relres, cudaStream_t s);

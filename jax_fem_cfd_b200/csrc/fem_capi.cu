@@ -1175,7 +1175,7 @@ extern "C" int fem_pressure_solve_mixed(fem_ctx* c, const double* b, double* x, 
   const int grid = c->sms * 8;
   if (!c->mx32) {
     size_t nf = 3 * (size_t)c->lv[0].g.nn;
-    for (int l = 0; l < c->nlev; ++l) nf += 3 * (size_t)c->lv[l].g.nn;
+    for (int l = 0; l < c->nlev; ++l) nf += 6 * (size_t)c->lv[l].g.nn;
     FEM_ALLOC(c->mx32, nf);
     FEM_ALLOC(c->mx64, (size_t)grid + 8);
   }
