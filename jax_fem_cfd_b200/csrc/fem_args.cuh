@@ -95,8 +95,13 @@ int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, con
 int fem_launch_selftest_barrier(const FemSync& sync, int* status, cudaStream_t s);
 // mixed-precision pinned Poisson solve (k_mixed.cu); work: 6 sum(nn_l) + 3 nn_0
 // floats, dwork: grid + 8 doubles
+struct MxGraphCache {
+  cudaGraphExec_t exec = nullptr;  // captured inner solve of a context
+  int inner = 0;
+};
 int fem_mixed_poisson(const CgArgs& A, int grid, float* work, double* dwork, const double* b, double* x, double tol,
-                      int inner, int max_cycles, int* cycles, double* relres, cudaStream_t s);
+                      int inner, int max_cycles, int* cycles, double* relres, cudaStream_t s, MxGraphCache* gc,
+                      cudaStream_t cap);
 
 int fem_coop_occupancy_cg(int* occ);
 int fem_coop_occupancy_bi(int* occ);

@@ -144,6 +144,7 @@ struct fem_ctx {
   cudaStream_t cap_stream = nullptr;  // private stream for graph captures (fem_step4_graph)
   float* mx32 = nullptr;              // FP32 vectors of the mixed-precision solve (first use)
   double* mx64 = nullptr;             // its partial sums and scalars
+  MxGraphCache mxg;                   // its captured inner solve
 };
 
 struct fem_graph {
@@ -264,6 +265,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   for (int i = 0; i < 16; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  if (c->mxg.exec) cudaGraphExecDestroy(c->mxg.exec);
   if (c->mx32) cudaFree(c->mx32);
   if (c->mx64) cudaFree(c->mx64);
   void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
@@ -536,6 +538,19 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
   if (!c || nlev < 1 || nlev > FEM_MAX_LEVELS || c->g.kind == FEM_HEX8) return FEM_E_ARG;
   FEM_CHECK(cudaSetDevice(c->device));
   FEM_CHECK(cudaStreamSynchronize(s));
+  // a new hierarchy invalidates the mixed-precision solve's buffers and graph
+  if (c->mxg.exec) {
+    cudaGraphExecDestroy(c->mxg.exec);
+    c->mxg.exec = nullptr;
+  }
+  if (c->mx32) {
+    cudaFree(c->mx32);
+    c->mx32 = nullptr;
+  }
+  if (c->mx64) {
+    cudaFree(c->mx64);
+    c->mx64 = nullptr;
+  }
   const FemGrid& g0 = c->g;
   for (int l = 1; l < nlev; ++l)
     if ((g0.nex >> l) < 1 || (g0.ney >> l) < 1) return FEM_E_ARG;
@@ -1179,9 +1194,11 @@ extern "C" int fem_pressure_solve_mixed(fem_ctx* c, const double* b, double* x, 
     FEM_ALLOC(c->mx32, nf);
     FEM_ALLOC(c->mx64, (size_t)grid + 8);
   }
+  if (!c->cap_stream) FEM_CHECK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
   CgArgs A;
   fill_cg_args(c, A);
-  return fem_mixed_poisson(A, grid, c->mx32, c->mx64, b, x, tol, inner, max_cycles, cycles, relres, s);
+  return fem_mixed_poisson(A, grid, c->mx32, c->mx64, b, x, tol, inner, max_cycles, cycles, relres, s, &c->mxg,
+                           c->cap_stream);
 }
 
 extern "C" int fem_selftest_barrier_timeout(fem_ctx* c, int* status, cudaStream_t s) {

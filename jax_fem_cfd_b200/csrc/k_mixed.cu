@@ -404,7 +404,8 @@ static int mx_inner(const MxPlan& P, int inner, cudaStream_t s) {
 }
 
 int fem_mixed_poisson(const CgArgs& A, int grid, float* work, double* dwork, const double* b, double* x, double tol,
-                      int inner, int max_cycles, int* cycles, double* relres, cudaStream_t s) {
+                      int inner, int max_cycles, int* cycles, double* relres, cudaStream_t s, MxGraphCache* gc,
+                      cudaStream_t cap) {
   MxPlan P;
   P.nlev = A.nlev;
   P.grid = grid;
@@ -449,9 +450,28 @@ int fem_mixed_poisson(const CgArgs& A, int grid, float* work, double* dwork, con
     return fem_after_launch("norms");
   const double bb = nrm[1];
   double rr = nrm[0];
+  // the inner solve only touches the context's buffers: captured once into a
+  // CUDA graph (per inner count) and replayed every cycle
+  if (gc && cap && (!gc->exec || gc->inner != inner)) {
+    if (gc->exec) cudaGraphExecDestroy(gc->exec);
+    gc->exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      const int rc = mx_inner(P, inner, cap);
+      const cudaError_t e = cudaStreamEndCapture(cap, &graph);
+      if (rc == 0 && e == cudaSuccess && cudaGraphInstantiate(&gc->exec, graph, 0) == cudaSuccess) gc->inner = inner;
+      else gc->exec = nullptr;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();  // a failed capture falls back to direct launches
+  }
   int k = 0;
   while (rr > tol * tol * bb && k < max_cycles) {
-    if (int rc = mx_inner(P, inner, s)) return rc;
+    if (gc && gc->exec) {
+      if (cudaGraphLaunch(gc->exec, s) != cudaSuccess) return fem_after_launch("cudaGraphLaunch");
+    } else if (int rc = mx_inner(P, inner, s)) {
+      return rc;
+    }
     k_mx_add<<<gb, MX_THREADS, 0, s>>>(n, x, P.d, nullptr);
     mx_res64(L0, gb, b, x, P.part, s);
     k_mx_final<<<1, 256, 0, s>>>(P.part, gb, P.sc, 4, 0);
