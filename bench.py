@@ -481,13 +481,14 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--only", choices=["matvec", "poisson_sweep", "serving"],
-                    help="run one secondary measurement alone and print it")
+    ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving"],
+                    help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=64, help="--only serving: requests in the stream")
     ap.add_argument("--request-steps", type=int, default=200, help="--only serving: steps per request")
     args = ap.parse_args()
     if args.only:
         fn = {"matvec": matvec, "poisson_sweep": poisson_sweep,
+              "poisson": lambda: {f"poisson_{args.size}x{args.size}_q1": poisson(args.size)},
               "serving": lambda: serving(args.requests, args.request_steps)}[args.only]
         print(json.dumps(fn()))
         return
