@@ -1,0 +1,66 @@
+"""Adjoint of the projection stage (jax_fem_cfd_b200.solvers.adjoint.Projection)
+against central finite differences of the forward stage on a wall-bounded
+cavity: the stage is affine in U*, so the difference quotient is exact up to
+the pressure solve's tolerance."""
+import numpy as np
+import pytest
+import torch
+
+
+@pytest.fixture(scope="module")
+def cavity():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    from jax_fem_cfd_b200.serving import cavity_config
+    from jax_fem_cfd_b200.setup import simulation as sim
+    _, timestep, *rest = sim.setup(cavity_config(16))
+    solver = timestep.solver
+    return solver, solver.u_full(rest[-1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 1])
+def test_projection_vjp_matches_finite_differences(cavity, seed):
+    from jax_fem_cfd_b200.solvers.adjoint import Projection
+    solver, ud = cavity
+    n2, n = solver.ndim * solver.nn, solver.nn
+    rng = np.random.default_rng(seed)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
+    Us, gU, gP, dlt = t(rng.standard_normal(n2)), t(rng.standard_normal(n2)), t(rng.standard_normal(n)), \
+        t(rng.standard_normal(n2))
+    dt, rho = 0.01, 1.0
+
+    def loss(u):
+        U, P = Projection.apply(u, solver, dt, rho, ud, None, 1e-13)
+        return float((gU * U).sum() + (gP * P).sum())
+
+    x = Us.clone().requires_grad_(True)
+    U, P = Projection.apply(x, solver, dt, rho, ud, None, 1e-13)
+    ((gU * U).sum() + (gP * P).sum()).backward()
+    g = x.grad.clone()
+    eps = 1e-2
+    fd = (loss(Us + eps * dlt) - loss(Us - eps * dlt)) / (2 * eps)
+    vjp = float((g * dlt).sum())
+    assert abs(vjp - fd) <= 1e-7 * max(abs(fd), 1.0), (vjp, fd)
+    # U is U_d on the Dirichlet rows whatever U* is: an output gradient carried
+    # only there pulls back to zero
+    dm = solver.dmask.to(torch.bool)
+    x2 = Us.clone().requires_grad_(True)
+    U2, P2 = Projection.apply(x2, solver, dt, rho, ud, None, 1e-13)
+    (torch.where(dm, gU, torch.zeros_like(gU)) * U2).sum().backward()
+    assert float(x2.grad.abs().max()) == 0.0
+
+
+@pytest.mark.gpu
+def test_projection_refuses_mean_zero_pressure():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from bench import tg_config
+    from jax_fem_cfd_b200.setup import simulation as sim
+    from jax_fem_cfd_b200.solvers.adjoint import Projection
+    _, timestep, *rest = sim.setup(tg_config(sim, 8))
+    solver = timestep.solver
+    u = torch.zeros(solver.ndim * solver.nn, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        Projection.apply(u, solver, 0.01, 1.0, None, None)
