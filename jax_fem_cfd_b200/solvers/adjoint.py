@@ -1,6 +1,7 @@
-"""Adjoint of the pressure-projection stage of the 4-step time step.
+"""Adjoints of the two linear stages of the 4-step time step: the pressure
+projection and the momentum solve (for a fixed convection operator).
 
-The stage (solvers/standard.py:156-163, steps 5-7 of fem_step4) maps the
+The projection (solvers/standard.py:156-163, steps 5-7 of fem_step4) maps the
 intermediate velocity U* to
 
     P = A+ k (D U* - F_p)                   k = rho / dt, A+ the pinned pressure solve
@@ -17,11 +18,18 @@ affine in U*, and its reverse (vector-Jacobian product) for output gradients
     lam  = A+ w                     (the adjoint solve: the same pinned MG-PCG)
     g_U* = g_U' + k G lam
 
-`Projection` puts this behind torch.autograd (the analogue of jax.custom_vjp).
-It covers the projection stage only: the momentum solve (transposed BiCGSTAB
-with Ce(U_n)^T and the linearisation of Ce in U_n) is not part of it. Pinned
-pressure (set_zeroP) only. No reference counterpart: the reference
-differentiates with jax.grad.
+`Projection` puts this behind torch.autograd (the analogue of jax.custom_vjp);
+pinned pressure (set_zeroP) only.
+
+`MomentumSolve` is the momentum solve of solvers/standard.py:14-43 for a fixed
+operator A = (rho/dt) Me + theta (rho Ce(U_n) + mu Le) with identity rows on
+gamma_d (A_m = P_f A + P_d), as a function of its right-hand side. Its reverse
+is the adjoint solve A_m^T lam = g: A^T = (rho/dt) Me + theta (rho Ce^T + mu Le)
+(Me, Le symmetric, Ce^T element by element), and the identity rows become
+identity columns, so lam_f solves the masked transposed system with rhs
+(g_f, 0) and lam_d = g_d - (A^T lam_f)_d. The dependence of Ce on U_n (the
+linearisation of convection), step checkpointing and the transport adjoint are
+not built. No reference counterpart: the reference differentiates with jax.grad.
 """
 import torch
 
@@ -97,3 +105,47 @@ class Projection(torch.autograd.Function):
         w[pm] = 0.0
         lam = _pressure(solver, w, tol)
         return gU + k * _grad(solver, lam), None, None, None, None, None, None
+
+
+def _bicgstab(solver, Ksh, beta, B, mask, rhs, tol):
+    ctx = solver.ctx
+    x = torch.zeros_like(rhs)
+    it = torch.zeros(1, dtype=torch.int32, device=rhs.device)
+    st = torch.zeros(1, dtype=torch.int32, device=rhs.device)
+    _lib.call("fem_bicgstab_solve", ctx.handle, solver.ndim, 1.0, ptr(Ksh), float(beta), ptr(B), 0.0, None, ptr(mask),
+              ptr(rhs), ptr(x), float(tol), 0.0, 0, ptr(it), ptr(st), stream())
+    if int(st.item()) != 0:
+        raise _lib.FemError(f"BiCGSTAB status {int(st.item())}")
+    return x
+
+
+class MomentumSolve(torch.autograd.Function):
+    """rhs -> U_hat = A_m^-1 rhs for a fixed Ce(U_n); backward is the adjoint solve."""
+
+    @staticmethod
+    def forward(fctx, rhs, solver, Ce_all, rho, mu, dt, theta=0.5, tol=1e-13):
+        ctx = solver.ctx
+        Me, Le = ctx.element_data()[3], ctx.element_data()[4]
+        Ksh = ((rho / dt) * Me + (theta * mu) * Le).reshape(-1).contiguous()
+        Ce = Ce_all.to(torch.float64).contiguous()
+        x = _bicgstab(solver, Ksh, theta * rho, Ce, solver.dmask, rhs.detach().to(torch.float64).contiguous(), tol)
+        fctx.solver, fctx.Ksh, fctx.Ce, fctx.beta, fctx.tol = solver, Ksh, Ce, theta * rho, tol
+        return x
+
+    @staticmethod
+    def backward(fctx, g):
+        solver, Ksh, Ce, beta, tol = fctx.solver, fctx.Ksh, fctx.Ce, fctx.beta, fctx.tol
+        nen = int(round(Ksh.numel() ** 0.5))
+        CeT = Ce.reshape(-1, nen, nen).transpose(1, 2).contiguous()
+        g = g.contiguous()
+        dm = solver.dmask.to(torch.bool) if solver.dmask is not None else None
+        b = g.clone()
+        if dm is not None:
+            b[dm] = 0.0
+        lam = _bicgstab(solver, Ksh, beta, CeT, solver.dmask, b, tol)
+        if dm is not None:
+            y = torch.empty_like(lam)
+            _lib.call("fem_ebe_apply", solver.ctx.handle, solver.ndim, ptr(lam), ptr(y), 1.0, ptr(Ksh), float(beta),
+                      ptr(CeT), 0, 0.0, None, stream())
+            lam[dm] = g[dm] - y[dm]
+        return lam, None, None, None, None, None, None, None

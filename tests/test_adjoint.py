@@ -64,3 +64,33 @@ def test_projection_refuses_mean_zero_pressure():
     u = torch.zeros(solver.ndim * solver.nn, dtype=torch.float64, device="cuda")
     with pytest.raises(ValueError):
         Projection.apply(u, solver, 0.01, 1.0, None, None)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 1])
+def test_momentum_solve_vjp_matches_finite_differences(cavity, seed):
+    """The adjoint BiCGSTAB solve (transposed, non-symmetric Ce, Dirichlet
+    identity rows turned into columns) against central differences."""
+    from jax_fem_cfd_b200.core import element_calc as ec
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from jax_fem_cfd_b200.solvers.adjoint import MomentumSolve
+    solver, _ = cavity
+    n2 = solver.ndim * solver.nn
+    rng = np.random.default_rng(10 + seed)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
+    _, nconn, *_ = rm.create_mesh_2d(16, 16, 1.0, 1.0)
+    wq, N, Nd = solver.ctx.element_data()[:3]
+    Un = t(rng.standard_normal(n2))
+    Ce = ec.conservative_convec_elem_calc(nconn, Un, wq, N, Nd, solver.nn, solver.ndim, 0.5)
+    rhs, g, dlt = t(rng.standard_normal(n2)), t(rng.standard_normal(n2)), t(rng.standard_normal(n2))
+    args = (solver, Ce, 1.0, 0.05, 0.01)
+
+    def loss(r):
+        return float((g * MomentumSolve.apply(r, *args)).sum())
+
+    x = rhs.clone().requires_grad_(True)
+    (g * MomentumSolve.apply(x, *args)).sum().backward()
+    eps = 1e-2
+    fd = (loss(rhs + eps * dlt) - loss(rhs - eps * dlt)) / (2 * eps)
+    vjp = float((x.grad * dlt).sum())
+    assert abs(vjp - fd) <= 1e-7 * max(abs(fd), 1.0), (vjp, fd)
