@@ -28,8 +28,20 @@ is the adjoint solve A_m^T lam = g: A^T = (rho/dt) Me + theta (rho Ce^T + mu Le)
 (Me, Le symmetric, Ce^T element by element), and the identity rows become
 identity columns, so lam_f solves the masked transposed system with rhs
 (g_f, 0) and lam_d = g_d - (A^T lam_f)_d. The dependence of Ce on U_n (the
-linearisation of convection), step checkpointing and the transport adjoint are
-not built. No reference counterpart: the reference differentiates with jax.grad.
+linearisation of convection) enters through `Step`, below; the transport
+adjoint is not built. No reference counterpart: the
+reference differentiates with jax.grad.
+
+`rollout` chains Steps with checkpoints every `ckpt` steps (recomputation in
+the backward pass). `Step` is one whole 4-step time step (U_n, P_n) -> (U_{n+1}, P_{n+1}) of a
+wall-bounded pinned-pressure problem (solvers/standard.py:148-165, theta = 1/2,
+Ce(U_n) with beta = 1/2, F = 0, F_p = 0): the rhs
+(rho/dt) Me U_n - (1 - theta)(rho Ce(U_n) + mu Le) U_n - G P_n (U_d on gamma_d),
+the momentum solve, U* = U_hat + (dt/rho) G P_n / M, the projection. Its
+reverse chains the adjoints above with the velocity side of the convection
+operator: Ce(U) is linear in U, and d/dU <a, Ce(U) b> (conv_vjp_u) is a sum
+over elements and Gauss points of w A_c (N_k d_d B_c + beta d_d N_k B_c), where
+A_c, B_c are a_c, b_c interpolated at the Gauss point.
 """
 import torch
 
@@ -107,6 +119,34 @@ class Projection(torch.autograd.Function):
         return gU + k * _grad(solver, lam), None, None, None, None, None, None
 
 
+def _ebe(solver, x, alpha, A, beta=0.0, B=None, transB=0):
+    """(alpha A + beta B_e) x per velocity component (fem_ebe_apply)."""
+    y = torch.empty_like(x)
+    _lib.call("fem_ebe_apply", solver.ctx.handle, solver.ndim, ptr(x), ptr(y), float(alpha), ptr(A), float(beta),
+              ptr(B), int(transB), 0.0, None, stream())
+    return y
+
+
+def conv_vjp_u(solver, nconn, a, b, beta):
+    """d/dU <a, Ce(U) b> (a, b: ndim*nn vectors, Ce acting on each component)."""
+    wq, N, Nd = solver.ctx.element_data()[:3]
+    nd, nn = solver.ndim, solver.nn
+    w = wq.reshape(-1)
+    ae = a.view(nd, nn)[:, nconn]  # (c, e, i)
+    be = b.view(nd, nn)[:, nconn]
+    A = torch.einsum("qi,cei->ceq", N, ae)
+    B = torch.einsum("qi,cei->ceq", N, be)
+    dB = torch.einsum("qdi,cei->ceqd", Nd, be)
+    s_ = torch.einsum("ceq,ceqd->eqd", A, dB)
+    t_ = torch.einsum("ceq,ceq->eq", A, B)
+    ge = torch.einsum("q,qk,eqd->edk", w, N, s_) + beta * torch.einsum("q,qdk,eq->edk", w, Nd, t_)
+    out = torch.zeros(nd, nn, dtype=torch.float64, device=a.device)
+    idx = nconn.reshape(-1)
+    for d in range(nd):
+        out[d].index_add_(0, idx, ge[:, d, :].reshape(-1))
+    return out.reshape(-1)
+
+
 def _bicgstab(solver, Ksh, beta, B, mask, rhs, tol):
     ctx = solver.ctx
     x = torch.zeros_like(rhs)
@@ -149,3 +189,95 @@ class MomentumSolve(torch.autograd.Function):
                       ptr(CeT), 0, 0.0, None, stream())
             lam[dm] = g[dm] - y[dm]
         return lam, None, None, None, None, None, None, None
+
+
+def _projection_vjp(solver, gU, gP, k, c, tol):
+    ctx, pm, dm = _solver_masks(solver)
+    M = ctx.element_data()[6]
+    gU = gU.contiguous().clone()
+    if dm is not None:
+        gU[dm] = 0.0
+    w = gP.contiguous().clone() - c * _div(solver, (gU / M).contiguous())
+    w[pm] = 0.0
+    return gU + k * _grad(solver, _pressure(solver, w, tol))
+
+
+class Step(torch.autograd.Function):
+    """(U_n, P_n) -> (U_{n+1}, P_{n+1}) of one 4-step time step; backward is its adjoint."""
+
+    @staticmethod
+    def forward(fctx, U_n, P_n, solver, nconn, dt, rho, mu, U_d_full, tol=1e-13):
+        if not solver.cfg.set_zeroP:
+            raise ValueError("Step covers the pinned-pressure (set_zeroP) form only")
+        theta, beta = 0.5, 0.5
+        ctx, pm, dm = _solver_masks(solver)
+        Me, Le, M = ctx.element_data()[3].reshape(-1), ctx.element_data()[4].reshape(-1), ctx.element_data()[6]
+        Un = U_n.detach().to(torch.float64).contiguous()
+        Pn = P_n.detach().to(torch.float64).contiguous()
+        Ce = torch.empty(solver.ctx.ne * Me.numel(), dtype=torch.float64, device=Un.device)
+        _lib.call("fem_convection_build", ctx.handle, ptr(Un), beta, None, None, None, ptr(Ce), stream())
+        rhs = (_ebe(solver, Un, rho / dt, Me) - (1 - theta) * _ebe(solver, Un, mu, Le, rho, Ce)
+               - _grad(solver, Pn))
+        if dm is not None:
+            rhs[dm] = U_d_full[dm]
+        Ksh = ((rho / dt) * Me + (theta * mu) * Le).contiguous()
+        Uh = _bicgstab(solver, Ksh, theta * rho, Ce, solver.dmask, rhs, tol)
+        c, k = dt / rho, rho / dt
+        Us = Uh + c * _grad(solver, Pn) / M
+        P = _pressure(solver, k * _div(solver, Us), tol)
+        U = Us - c * _grad(solver, P) / M
+        if dm is not None:
+            U[dm] = U_d_full[dm]
+        fctx.save = (solver, nconn, Un, Ce, Ksh, Uh, dt, rho, mu, tol)
+        return U, P
+
+    @staticmethod
+    def backward(fctx, gU, gP):
+        solver, nconn, Un, Ce, Ksh, Uh, dt, rho, mu, tol = fctx.save
+        theta, beta = 0.5, 0.5
+        ctx, pm, dm = _solver_masks(solver)
+        Me, Le, M = ctx.element_data()[3].reshape(-1), ctx.element_data()[4].reshape(-1), ctx.element_data()[6]
+        nd, nn = solver.ndim, solver.nn
+        c, k = dt / rho, rho / dt
+        gU = gU if gU is not None else torch.zeros(nd * nn, dtype=torch.float64, device=Un.device)
+        gP = gP if gP is not None else torch.zeros(nn, dtype=torch.float64, device=Un.device)
+        gUs = _projection_vjp(solver, gU, gP, k, c, tol)            # through the projection
+        gPn = c * _div(solver, (gUs / M).contiguous())              # U* = U_hat + c G P_n / M
+        # the adjoint momentum solve (identity rows become identity columns)
+        nen = int(round(Ksh.numel() ** 0.5))
+        CeT = Ce.view(-1, nen, nen).transpose(1, 2).contiguous()
+        b = gUs.clone()
+        if dm is not None:
+            b[dm] = 0.0
+        lam = _bicgstab(solver, Ksh, theta * rho, CeT, solver.dmask, b, tol)  # = lam_f (0 on gamma_d)
+        # rhs = (rho/dt) Me U_n - (1 - theta)(rho Ce(U_n) + mu Le) U_n - G P_n, U_d on gamma_d
+        gUn = (_ebe(solver, lam, rho / dt, Me) - (1 - theta) * _ebe(solver, lam, mu, Le, rho, Ce, 1)
+               - (1 - theta) * rho * conv_vjp_u(solver, nconn, lam, Un, beta))
+        gPn = gPn - _div(solver, lam)
+        # the operator's dependence on U_n: U_hat = A(U_n)^-1 rhs, dA = theta rho Ce(dU) on the free rows
+        gUn = gUn - theta * rho * conv_vjp_u(solver, nconn, lam, Uh, beta)
+        return gUn, gPn, None, None, None, None, None, None, None
+
+
+def rollout(solver, nconn, U0, P0, steps, dt, rho, mu, U_d_full, ckpt=10, tol=1e-13):
+    """`steps` time steps of Step from (U0, P0), differentiable end to end. With
+    gradients enabled and ckpt > 0, every chunk of `ckpt` steps is a checkpoint
+    (torch.utils.checkpoint): only the chunk boundaries are kept, and a chunk's
+    steps are recomputed when the backward pass reaches it."""
+    from torch.utils.checkpoint import checkpoint
+
+    def chunk(u, p, n):
+        for _ in range(n):
+            u, p = Step.apply(u, p, solver, nconn, dt, rho, mu, U_d_full, tol)
+        return u, p
+
+    u, p = U0, P0
+    done = 0
+    while done < steps:
+        n = min(ckpt, steps - done) if ckpt > 0 else steps - done
+        if ckpt > 0 and torch.is_grad_enabled():
+            u, p = checkpoint(chunk, u, p, n, use_reentrant=False)
+        else:
+            u, p = chunk(u, p, n)
+        done += n
+    return u, p
