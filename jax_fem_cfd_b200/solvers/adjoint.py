@@ -28,9 +28,9 @@ is the adjoint solve A_m^T lam = g: A^T = (rho/dt) Me + theta (rho Ce^T + mu Le)
 (Me, Le symmetric, Ce^T element by element), and the identity rows become
 identity columns, so lam_f solves the masked transposed system with rhs
 (g_f, 0) and lam_d = g_d - (A^T lam_f)_d. The dependence of Ce on U_n (the
-linearisation of convection) enters through `Step`, below; the transport
-adjoint is not built. No reference counterpart: the
-reference differentiates with jax.grad.
+linearisation of convection) enters through `Step`, below, and the passive
+scalar's step through `Transport`. No reference counterpart: the reference
+differentiates with jax.grad.
 
 `rollout` chains Steps with checkpoints every `ckpt` steps (recomputation in
 the backward pass). `Step` is one whole 4-step time step (U_n, P_n) -> (U_{n+1}, P_{n+1}) of a
@@ -119,11 +119,12 @@ class Projection(torch.autograd.Function):
         return gU + k * _grad(solver, lam), None, None, None, None, None, None
 
 
-def _ebe(solver, x, alpha, A, beta=0.0, B=None, transB=0):
-    """(alpha A + beta B_e) x per velocity component (fem_ebe_apply)."""
+def _ebe(solver, x, alpha, A, beta=0.0, B=None, transB=0, ncomp=None):
+    """(alpha A + beta B_e) x per component (fem_ebe_apply); ncomp defaults to the
+    velocity's."""
     y = torch.empty_like(x)
-    _lib.call("fem_ebe_apply", solver.ctx.handle, solver.ndim, ptr(x), ptr(y), float(alpha), ptr(A), float(beta),
-              ptr(B), int(transB), 0.0, None, stream())
+    _lib.call("fem_ebe_apply", solver.ctx.handle, ncomp or solver.ndim, ptr(x), ptr(y), float(alpha), ptr(A),
+              float(beta), ptr(B), int(transB), 0.0, None, stream())
     return y
 
 
@@ -147,13 +148,13 @@ def conv_vjp_u(solver, nconn, a, b, beta):
     return out.reshape(-1)
 
 
-def _bicgstab(solver, Ksh, beta, B, mask, rhs, tol):
+def _bicgstab(solver, Ksh, beta, B, mask, rhs, tol, ncomp=None):
     ctx = solver.ctx
     x = torch.zeros_like(rhs)
     it = torch.zeros(1, dtype=torch.int32, device=rhs.device)
     st = torch.zeros(1, dtype=torch.int32, device=rhs.device)
-    _lib.call("fem_bicgstab_solve", ctx.handle, solver.ndim, 1.0, ptr(Ksh), float(beta), ptr(B), 0.0, None, ptr(mask),
-              ptr(rhs), ptr(x), float(tol), 0.0, 0, ptr(it), ptr(st), stream())
+    _lib.call("fem_bicgstab_solve", ctx.handle, ncomp or solver.ndim, 1.0, ptr(Ksh), float(beta), ptr(B), 0.0, None,
+              ptr(mask), ptr(rhs), ptr(x), float(tol), 0.0, 0, ptr(it), ptr(st), stream())
     if int(st.item()) != 0:
         raise _lib.FemError(f"BiCGSTAB status {int(st.item())}")
     return x
@@ -259,25 +260,128 @@ class Step(torch.autograd.Function):
         return gUn, gPn, None, None, None, None, None, None, None
 
 
-def rollout(solver, nconn, U0, P0, steps, dt, rho, mu, U_d_full, ckpt=10, tol=1e-13):
-    """`steps` time steps of Step from (U0, P0), differentiable end to end. With
-    gradients enabled and ckpt > 0, every chunk of `ckpt` steps is a checkpoint
+def transport_elements(solver, nconn, Un, U, dt, D, supg):
+    """(E_k, B_k): the per-element parts of the transport step's operators as
+    differentiable torch functions of U_n and U (solvers/passive_transport.py:
+    14-62 with the matrices of :80-88). The lhs is A = K_A + E_k and the rhs
+    operator B = K_B + B_k, with the shared K_A = Me/dt + (D/2) Le and
+    K_B = Me/dt - (D/2) Le. With SUPG:
+        E_k = Mtau/dt + (Ce(U) + Ctau)/2,   B_k = Mtau/dt - (Ce(U_n) + Ctau)/2,
+        Ctau = tau Ct(U_n),  Mtau = tau Ce(U_n)^T,  tau = tau(U_n, Ce(U), Ct(U_n)),
+    without it E_k = Ce(U)/2 and B_k = -Ce(U_n)/2; Ce has beta = 1
+    (core/element_calc.py:165-185), Ct = sum_q w dN^T (u u^T) dN (:188-200),
+    tau the r = 2 blend of :202-229."""
+    wq, N, Nd = solver.ctx.element_data()[:3]
+    nd, nn = solver.ndim, solver.nn
+    w = wq.reshape(-1)
+
+    def interp(V):
+        return torch.einsum("qi,dei->eqd", N, V.view(nd, nn)[:, nconn])
+
+    def conv(V):
+        Ve = V.view(nd, nn)[:, nconn]
+        adv = torch.einsum("q,qa,eqd,qdb->eab", w, N, interp(V), Nd)
+        div = torch.einsum("qdi,dei->eq", Nd, Ve)
+        return adv + torch.einsum("q,qa,eq,qb->eab", w, N, div, N)
+
+    Ce_new, Ce_n = conv(U), conv(Un)
+    if not supg:
+        return 0.5 * Ce_new, -0.5 * Ce_n
+    Uq = interp(Un)
+    Ct = torch.einsum("q,qda,eqd,eqk,qkb->eab", w, Nd, Uq, Uq, Nd)
+    ce = torch.sqrt((Ce_new ** 2).sum((1, 2)))
+    kt = torch.sqrt((Ct ** 2).sum((1, 2)))
+    un2 = (Uq ** 2).sum(2).mean(1)
+    tau1 = ce / kt
+    tau3 = tau1 * (un2 * ce) / ((D + 1e-6) * kt)
+    tau = (tau1 ** -2 + (dt / 2) ** -2 + tau3 ** -2) ** -0.5
+    Ctau = tau[:, None, None] * Ct
+    Mtau = tau[:, None, None] * Ce_n.transpose(1, 2)
+    return Mtau / dt + 0.5 * (Ce_new + Ctau), Mtau / dt - 0.5 * (Ce_n + Ctau)
+
+
+class Transport(torch.autograd.Function):
+    """(U_n, U, phi_n[, phi_d]) -> phi_{n+1}: the passive-scalar step of
+    solvers/passive_transport.py:64-97 (fem_transport_phi); backward is its
+    adjoint. phi solves A_m phi = r with A_m = P_f A + P_d (identity rows on
+    gamma_d_phi), r_f = (B phi_n)_f, r_d = phi_d. For an output gradient g:
+        A_m^T lam = g        (masked transposed BiCGSTAB, as in MomentumSolve)
+        g_phi_n = B^T (P_f lam),   g_phi_d = lam on gamma_d_phi,
+        g_U_n, g_U = d/dU <P_f lam, B(U_n, U) phi_n - A(U_n, U) phi>
+    the last by torch autograd over transport_elements (the shared parts of A
+    and B do not depend on the velocity)."""
+
+    @staticmethod
+    def forward(fctx, U_n, U, phi_n, phid_full, solver, nconn, dt, D, supg=False, phi_mask=None, tol=1e-13):
+        if (phi_mask is None) != (phid_full is None):
+            raise ValueError("phi_mask and phid_full go together")
+        ctx = solver.ctx
+        Un, Uc, pn = (t.detach().to(torch.float64).contiguous() for t in (U_n, U, phi_n))
+        pd = phid_full.detach().to(torch.float64).contiguous() if phid_full is not None else None
+        phi = torch.empty_like(pn)
+        it = torch.zeros(1, dtype=torch.int32, device=pn.device)
+        st = torch.zeros(1, dtype=torch.int32, device=pn.device)
+        _lib.call("fem_transport_phi", ctx.handle, ptr(Un), ptr(Uc), ptr(pn), float(dt), float(D), int(bool(supg)),
+                  ptr(phi_mask), ptr(pd), float(tol), ptr(phi), ptr(it), ptr(st), stream())
+        if int(st.item()) != 0:
+            raise _lib.FemError(f"transport BiCGSTAB status {int(st.item())}")
+        fctx.save = (solver, nconn, Un, Uc, pn, phi, dt, D, supg, phi_mask, tol)
+        return phi
+
+    @staticmethod
+    def backward(fctx, g):
+        solver, nconn, Un, Uc, pn, phi, dt, D, supg, phi_mask, tol = fctx.save
+        Me, Le = solver.ctx.element_data()[3], solver.ctx.element_data()[4]
+        with torch.enable_grad():
+            un, uc = Un.clone().requires_grad_(True), Uc.clone().requires_grad_(True)
+            Ek, Bk = transport_elements(solver, nconn, un, uc, dt, D, supg)
+        KA = (Me / dt + 0.5 * D * Le).reshape(-1).contiguous()
+        KB = (Me / dt - 0.5 * D * Le).reshape(-1).contiguous()
+        EkT = Ek.detach().transpose(1, 2).contiguous()
+        m = phi_mask.to(torch.bool) if phi_mask is not None else None
+        g = g.contiguous()
+        b = g.clone()
+        if m is not None:
+            b[m] = 0.0
+        lam = _bicgstab(solver, KA, 1.0, EkT, phi_mask, b, tol, ncomp=1)   # lam_f, 0 on gamma_d_phi
+        g_phid = None
+        if m is not None:
+            lam_d = g - _ebe(solver, lam, 1.0, KA, 1.0, EkT, ncomp=1)
+            g_phid = torch.where(m, lam_d, torch.zeros_like(lam_d))
+        g_phin = _ebe(solver, lam, 1.0, KB, 1.0, Bk.detach().transpose(1, 2).contiguous(), ncomp=1)
+        le, pe, fe = lam[nconn], pn[nconn], phi[nconn]
+        with torch.enable_grad():
+            s = torch.einsum("ea,eab,eb->", le, Bk, pe) - torch.einsum("ea,eab,eb->", le, Ek, fe)
+            gUn, gU = torch.autograd.grad(s, (un, uc))
+        return gUn, gU, g_phin, g_phid, None, None, None, None, None, None, None
+
+
+def rollout(solver, nconn, U0, P0, steps, dt, rho, mu, U_d_full, ckpt=10, tol=1e-13, phi0=None, D=0.0, supg=False,
+            phi_mask=None, phid_full=None):
+    """`steps` time steps of Step from (U0, P0), differentiable end to end, and
+    with phi0 given the passive scalar carried along by Transport (the order of
+    solvers/passive_transport.py:64-97: the flow step, then phi from U_n and
+    U_{n+1}); returns (U, P) or (U, P, phi). With gradients enabled and
+    ckpt > 0, every chunk of `ckpt` steps is a checkpoint
     (torch.utils.checkpoint): only the chunk boundaries are kept, and a chunk's
     steps are recomputed when the backward pass reaches it."""
     from torch.utils.checkpoint import checkpoint
 
-    def chunk(u, p, n):
+    def chunk(n, u, p, *phi):
         for _ in range(n):
-            u, p = Step.apply(u, p, solver, nconn, dt, rho, mu, U_d_full, tol)
-        return u, p
+            u1, p = Step.apply(u, p, solver, nconn, dt, rho, mu, U_d_full, tol)
+            if phi:
+                phi = (Transport.apply(u, u1, phi[0], phid_full, solver, nconn, dt, D, supg, phi_mask, tol),)
+            u = u1
+        return (u, p) + phi
 
-    u, p = U0, P0
+    state = (U0, P0) + ((phi0,) if phi0 is not None else ())
     done = 0
     while done < steps:
         n = min(ckpt, steps - done) if ckpt > 0 else steps - done
         if ckpt > 0 and torch.is_grad_enabled():
-            u, p = checkpoint(chunk, u, p, n, use_reentrant=False)
+            state = checkpoint(chunk, n, *state, use_reentrant=False)
         else:
-            u, p = chunk(u, p, n)
+            state = chunk(n, *state)
         done += n
-    return u, p
+    return state

@@ -179,3 +179,117 @@ def test_checkpointed_rollout_gradient(cavity):
     fd = (lp - lm) / (2 * eps)
     vjp = float((g_plain * d).sum())
     assert abs(vjp - fd) <= 1e-6 * max(abs(fd), 1.0), (vjp, fd)
+
+
+def _transport_case(solver, supg, seed=40):
+    from jax_fem_cfd_b200.context import make_mask
+    n2, n = solver.ndim * solver.nn, solver.nn
+    rng = np.random.default_rng(seed)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
+    Un = t(0.5 * rng.standard_normal(n2))
+    U = Un + t(0.1 * rng.standard_normal(n2))
+    phin = t(rng.standard_normal(n))
+    bottom = np.arange(17)  # the y = 0 row of the 17 x 17 node lattice
+    mask = make_mask(bottom, n)
+    phid = torch.zeros(n, dtype=torch.float64, device="cuda")
+    phid[bottom] = t(rng.standard_normal(bottom.size))
+    return Un, U, phin, phid, mask, rng
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("supg", [False, True])
+def test_transport_elements_reproduce_the_product_step(cavity, supg):
+    """transport_elements (the torch restatement the adjoint differentiates)
+    describes the system fem_transport_phi solves: the product's phi leaves a
+    relative residual at the solver's tolerance in the restated system."""
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from jax_fem_cfd_b200.solvers.adjoint import Transport, transport_elements
+    solver, _ = cavity
+    _, nconn, *_ = rm.create_mesh_2d(16, 16, 1.0, 1.0)
+    Un, U, phin, phid, mask, _ = _transport_case(solver, supg)
+    dt, D = 0.01, 1e-3
+    phi = Transport.apply(Un, U, phin, phid, solver, nconn, dt, D, supg, mask)
+    Ek, Bk = transport_elements(solver, nconn, Un, U, dt, D, supg)
+    Me, Le = solver.ctx.element_data()[3], solver.ctx.element_data()[4]
+    n = solver.nn
+
+    def apply(Kel, x):
+        y = torch.zeros(n, dtype=torch.float64, device="cuda")
+        y.index_add_(0, nconn.reshape(-1), torch.einsum("eab,eb->ea", Kel, x[nconn]).reshape(-1))
+        return y
+
+    m = mask.to(torch.bool)
+    r = apply(Me / dt - 0.5 * D * Le + Bk, phin)
+    r[m] = phid[m]
+    Aphi = apply(Me / dt + 0.5 * D * Le + Ek, phi)
+    Aphi[m] = phi[m]
+    rel = float(torch.linalg.norm(Aphi - r) / torch.linalg.norm(r))
+    assert rel < 1e-11, rel
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("supg", [False, True])
+@pytest.mark.parametrize("which", ["phi_n", "U_n", "U", "phi_d"])
+def test_transport_vjp_matches_finite_differences(cavity, supg, which):
+    """The transport adjoint (masked transposed BiCGSTAB, B^T, and the velocity
+    dependence of Ce, Ctau, Mtau and tau) against central differences."""
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from jax_fem_cfd_b200.solvers.adjoint import Transport
+    solver, _ = cavity
+    _, nconn, *_ = rm.create_mesh_2d(16, 16, 1.0, 1.0)
+    Un, U, phin, phid, mask, rng = _transport_case(solver, supg)
+    dt, D = 0.01, 1e-3
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
+    g = t(rng.standard_normal(solver.nn))
+    xs = dict(U_n=Un, U=U, phi_n=phin, phi_d=phid)
+    d = t(rng.standard_normal(xs[which].numel()))
+    if which == "phi_d":
+        d = torch.where(mask.to(torch.bool), d, torch.zeros_like(d))
+
+    def loss(**kw):
+        a = {**xs, **kw}
+        return float((g * Transport.apply(a["U_n"], a["U"], a["phi_n"], a["phi_d"], solver, nconn, dt, D, supg,
+                                          mask)).sum())
+
+    leaves = {k: v.clone().requires_grad_(True) for k, v in xs.items()}
+    phi = Transport.apply(leaves["U_n"], leaves["U"], leaves["phi_n"], leaves["phi_d"], solver, nconn, dt, D, supg,
+                          mask)
+    (g * phi).sum().backward()
+    eps = 1e-5
+    fd = (loss(**{which: xs[which] + eps * d}) - loss(**{which: xs[which] - eps * d})) / (2 * eps)
+    vjp = float((leaves[which].grad * d).sum())
+    assert abs(vjp - fd) <= 1e-6 * max(abs(fd), 1.0), (vjp, fd)
+
+
+@pytest.mark.gpu
+def test_transport_rollout_gradient(cavity):
+    """Flow and SUPG passive scalar over 4 steps: the checkpointed gradient in
+    (U0, phi0) equals the plain one and matches central differences."""
+    from jax_fem_cfd_b200.setup import regular_mesh as rm
+    from jax_fem_cfd_b200.solvers.adjoint import rollout
+    solver, ud = cavity
+    _, nconn, *_ = rm.create_mesh_2d(16, 16, 1.0, 1.0)
+    Un, _, phin, phid, mask, rng = _transport_case(solver, True, seed=41)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
+    P0 = torch.zeros(solver.nn, dtype=torch.float64, device="cuda")
+    gphi = t(rng.standard_normal(solver.nn))
+    kw = dict(phi_mask=mask, phid_full=phid, D=1e-3, supg=True)
+
+    def run(u, phi, ckpt):
+        return rollout(solver, nconn, u, P0, 4, 0.01, 1.0, 0.05, ud, ckpt=ckpt, phi0=phi, **kw)[2]
+
+    def grads(ckpt):
+        u, phi = Un.clone().requires_grad_(True), phin.clone().requires_grad_(True)
+        (gphi * run(u, phi, ckpt)).sum().backward()
+        return u.grad, phi.grad
+
+    (gu0, gp0), (gu2, gp2) = grads(0), grads(2)
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    assert rel(gu2, gu0) < 1e-12 and rel(gp2, gp0) < 1e-12
+    du, dp, eps = t(rng.standard_normal(Un.numel())), t(rng.standard_normal(phin.numel())), 1e-5
+    with torch.no_grad():
+        lp = float((gphi * run(Un + eps * du, phin + eps * dp, 0)).sum())
+        lm = float((gphi * run(Un - eps * du, phin - eps * dp, 0)).sum())
+    fd = (lp - lm) / (2 * eps)
+    vjp = float((gu0 * du).sum() + (gp0 * dp).sum())
+    assert abs(vjp - fd) <= 1e-6 * max(abs(fd), 1.0), (vjp, fd)
