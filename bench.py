@@ -374,6 +374,64 @@ def serving(count, steps):
     return out
 
 
+def inverse(reps=3, adam_iters=5):
+    """Differentiable inverse transport (128^2 Q1 unit square, all walls,
+    nu 1e-3, scalar diffusivity 1e-4 with SUPG, dt 0.01, 150 steps, learnable
+    FP32 initial velocity, adjoint gradient with a checkpoint every 10 steps):
+    device time of the loss alone and of loss + gradient (CUDA events on the
+    launching stream; the working set is L2-resident, so no flush), the
+    gradient against a central difference along a seeded direction, and the
+    loss over a few Adam iterations."""
+    import torch
+
+    from jax_fem_cfd_b200.solvers.inverse_transport import InverseTransport
+    prob = InverseTransport()
+    u0 = prob.initial_velocity()
+    prob.value_and_grad(u0)
+
+    def timed(fn):
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    with torch.no_grad():
+        fwd_ms = timed(lambda: prob.loss(u0))
+    grad_ms = timed(lambda: prob.value_and_grad(u0))
+    u64 = u0.to(torch.float64)
+    L, g = prob.value_and_grad(u64)
+    d = torch.randn(u64.numel(), generator=torch.Generator().manual_seed(7), dtype=torch.float64).to(u64.device)
+    eps = 3e-4
+    with torch.no_grad():
+        fd = (float(prob.loss(u64 + eps * d)) - float(prob.loss(u64 - eps * d))) / (2 * eps)
+    vjp = float((g * d).sum())
+    p = u0.clone().requires_grad_(True)
+    opt = torch.optim.Adam([p], lr=0.01)
+    hist = []
+    for _ in range(adam_iters):
+        opt.zero_grad()
+        Lk = prob.loss(p)
+        Lk.backward()
+        opt.step()
+        hist.append(float(Lk.detach()))
+    with torch.no_grad():
+        hist.append(float(prob.loss(p)))
+    return {"inverse_transport_128x128_q1": {
+        "workload": "128^2 Q1 unit square, all walls, nu 1e-3, D 1e-4 (SUPG), dt 0.01, 150 steps, "
+                    "checkpoint every 10 steps, FP32 initial velocity N(0, 0.1) seed 0, FP64 solves at tol 1e-10",
+        "forward_ms": fwd_ms, "loss_and_gradient_ms": grad_ms, "gradients_per_s": 1e3 / grad_ms,
+        "gradient_over_forward": grad_ms / fwd_ms,
+        "fd_check": {"direction": "N(0,1) seed 7", "eps": eps, "adjoint": vjp, "central_difference": fd,
+                     "rel_err": abs(vjp - fd) / abs(fd)},
+        "adam_lr_0.01_loss": hist}}
+
+
 def poisson_and_matvec(args):
     """Reference-published GPU figures on their own sizes (README.md:28-41):
     MG-PCG Poisson solve on 1024x1024 Q1 elements and the EBE matvec on
@@ -481,7 +539,7 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving"],
+    ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=64, help="--only serving: requests in the stream")
     ap.add_argument("--request-steps", type=int, default=200, help="--only serving: steps per request")
@@ -489,7 +547,7 @@ def main():
     if args.only:
         fn = {"matvec": matvec, "poisson_sweep": poisson_sweep,
               "poisson": lambda: {f"poisson_{args.size}x{args.size}_q1": poisson(args.size)},
-              "serving": lambda: serving(args.requests, args.request_steps)}[args.only]
+              "serving": lambda: serving(args.requests, args.request_steps), "inverse": inverse}[args.only]
         print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
