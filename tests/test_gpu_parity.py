@@ -251,6 +251,12 @@ STEP_CASES = {
                        0.01, 0.01),
     "tg64_q2p_mg": (([64, 64], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]), None, 3,
                     1e-3, 0.01),
+    # the lid-driven cavity at its full size and length: 64^2 Q1, Re 100, dt 0.01, 200 steps
+    "cavity64_q1_mg_200_steps": (([64, 64], [1, 1], 1, False, [0, 1, 2, 3], "multigrid", True, 1e-8, [4, 4]),
+                                 "corners", 200, 0.01, 0.01),
+    # the periodic Taylor-Green workload at full size (256^2 Q2, 263,169 nodes), first 2 steps
+    "tg256_q2p_mg": (([256, 256], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]), None, 2,
+                     1e-3, 0.01),
 }
 
 
@@ -286,6 +292,35 @@ def test_ns_step_parity(case):
     assert ig == io, (ig, io)
     assert rel(Ug, Uo) < SOLVE_TOL, rel(Ug, Uo)
     assert rel(Pg, Po) < SOLVE_TOL, rel(Pg, Po)
+
+
+def test_taylor_green_256_q2_decay():
+    """The Taylor-Green workload at full size and length (256^2 Q2, nu 0.01,
+    dt 1e-3, 500 steps) against its analytic solution: velocity
+    u_0 exp(-2 nu t) and pressure P_0 exp(-4 nu t) (examples/taylor_green.py:
+    6-14), with mean-zero pressure throughout."""
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    args = ([256, 256], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4])
+    compute, timestep, nc, *_ = gsim.setup(_ns_cfg(gsim, *args))
+    ncn = nc.detach().cpu().numpy()
+    x, y = ncn[:, 0], ncn[:, 1]
+    U0 = np.concatenate([np.sin(x) * np.cos(y), -np.cos(x) * np.sin(y)])
+    P0 = 0.25 * (np.cos(2 * x) + np.cos(2 * y))
+    P0 = P0 - P0.mean()
+    nu, dt, steps = 0.01, 1e-3, 500
+    U, P = torch.as_tensor(U0, device="cuda"), torch.as_tensor(P0, device="cuda")
+    for s in range(steps):
+        Fp, F = compute(None, None, s * dt, (s + 1) * dt)
+        U, P, ui, pi = timestep(U, P, dt, 1.0, nu, None, Fp, F)
+    U, P, t = np_(U), np_(P), steps * dt
+    amp = float(U @ U0 / (U0 @ U0))
+    print("TG 256^2 Q2 after 500 steps: amplitude/exp(-2 nu t) - 1 =", amp / np.exp(-2 * nu * t) - 1,
+          "rel U err", rel(U, U0 * np.exp(-2 * nu * t)), "rel P err", rel(P, P0 * np.exp(-4 * nu * t)))
+    # measured on a B200: 3.0e-8, 9.9e-8 and 2.9e-5 (the pressure lags by one step in the scheme)
+    assert abs(amp / np.exp(-2 * nu * t) - 1) < 1e-6, amp
+    assert rel(U, U0 * np.exp(-2 * nu * t)) < 1e-6, rel(U, U0 * np.exp(-2 * nu * t))
+    assert abs(P.mean()) < 1e-12
+    assert rel(P, P0 * np.exp(-4 * nu * t)) < 1e-4, rel(P, P0 * np.exp(-4 * nu * t))
 
 
 @pytest.mark.parametrize("supg", [True, False])
