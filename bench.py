@@ -432,6 +432,64 @@ def inverse(reps=3, adam_iters=5):
         "adam_lr_0.01_loss": hist}}
 
 
+def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv")):
+    """3D channel: hex8 256 x 64 x 64 on [0,4] x [0,1] x [0,1] (1,048,576
+    elements, 1,090,625 nodes), parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
+    zero-traction outlet (P = 0) on x = 4, no-slip walls, Re 200 (mu = 1/200,
+    rho = 1), dt 2e-3, zero initial fields, FP64 at tol 1e-8. Pressure
+    preconditioners the 3D path accepts (multigrid is 2D only, as in
+    setup/simulation.py:81-82). One step = the boundary integral plus fem_step4;
+    device time with CUDA events, working set beyond L2 (Ce alone is 537 MB)."""
+    import torch
+
+    from jax_fem_cfd_b200.setup import simulation as sim
+    out = {}
+    for pc in preconds:
+        cfg = sim.Config(mesh="simple", solver="standard",
+                         mesh_config=sim.SimpleMeshConfig(num_elem=[256, 64, 64], domain_size=[4.0, 1.0, 1.0],
+                                                          shape_func_ord=1, periodic=False),
+                         solver_config=sim.StandardSolverConfig(dirichlet_faces=[0, 2, 3, 4, 5], symmetry_faces=[],
+                                                                outlet_faces=[1], streamline_diff=False,
+                                                                solver_tol=1e-8, set_zeroP=True, pressure_precond=pc,
+                                                                final_multigrid_mesh=None))
+        compute, timestep, nc, sn, h, nn, gd, Ud = sim.setup(cfg)
+        y, z = nc[sn[3], 1], nc[sn[3], 2]
+        Ud = sim.set_face_velocity(Ud, sn[3], gd, 16 * y * (1 - y) * z * (1 - z), nn, var=1)
+        solver = timestep.solver
+        dt, mu = 2e-3, 1.0 / 200
+        bufs = [(torch.zeros(3 * nn, dtype=torch.float64, device="cuda"),
+                 torch.zeros(nn, dtype=torch.float64, device="cuda")) for _ in range(2)]
+        its = []
+
+        def run(k, t0):
+            for s in range(k):
+                (U, P), o = bufs[(t0 + s) % 2], bufs[(t0 + s + 1) % 2]
+                Fp, F = compute(Ud, None, (t0 + s) * dt, (t0 + s + 1) * dt)
+                _, _, ui, pi = solver.step(U, P, dt, 1.0, mu, Ud, Fp, F, out=o)
+                its.append((ui, pi))
+
+        run(warmup, 0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run(steps, warmup)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        it = np.array([(int(a), int(b)) for a, b in its[warmup:]])
+        st = int(solver.status.max())
+        U = bufs[(warmup + steps) % 2][0]
+        out[pc] = {"steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps, "status": st,
+                   "momentum_iters_mean": float(it[:, 0].mean()), "pressure_iters_mean": float(it[:, 1].mean()),
+                   "pressure_iters_first_last": [int(it[0, 1]), int(it[-1, 1])],
+                   "u_max_after": float(U[:nn].max()), "finite": bool(torch.isfinite(U).all())}
+        del compute, timestep, solver, bufs, nc, sn, gd, Ud
+        torch.cuda.empty_cache()
+    return {"channel3d_hex8_256x64x64": {
+        "workload": "hex8 256x64x64 channel, parabolic inflow, outlet, Re 200, dt 2e-3, FP64 tol 1e-8, zero start",
+        "timed_steps": steps, "warmup": warmup, **out}}
+
+
 def poisson_and_matvec(args):
     """Reference-published GPU figures on their own sizes (README.md:28-41):
     MG-PCG Poisson solve on 1024x1024 Q1 elements and the EBE matvec on
@@ -539,7 +597,7 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse"],
+    ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse", "channel3d"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=64, help="--only serving: requests in the stream")
     ap.add_argument("--request-steps", type=int, default=200, help="--only serving: steps per request")
@@ -547,7 +605,8 @@ def main():
     if args.only:
         fn = {"matvec": matvec, "poisson_sweep": poisson_sweep,
               "poisson": lambda: {f"poisson_{args.size}x{args.size}_q1": poisson(args.size)},
-              "serving": lambda: serving(args.requests, args.request_steps), "inverse": inverse}[args.only]
+              "serving": lambda: serving(args.requests, args.request_steps), "inverse": inverse,
+              "channel3d": lambda: channel3d(args.steps)}[args.only]
         print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup

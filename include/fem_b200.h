@@ -222,7 +222,11 @@ int fem_transport_phi(fem_ctx* ctx, const double* U_n, const double* U, const do
 /* F_p = int_Gamma_d q (u_d . n) over the boundary edges/faces listed in bconn
  * (nb x I, int32, I = 2 lin2, 3 lin3, 4 quad4 faces) with outward normals nvec
  * (nb x dim) and Dirichlet values at their nodes U_b (ndim*nn, full vector)
- * (core/element_calc.py:111 u_dot_n_boundary_integral_1d, :137 _2d). */
+ * (core/element_calc.py:111 u_dot_n_boundary_integral_1d, :137 _2d). The
+ * assembly runs node-parallel: a node -> face-entry table is built on the
+ * device on every call, and each node sums its entries in face order. The
+ * result is bitwise that of a serial scatter in face order (the reference's
+ * segment_sum order). */
 int fem_boundary_flux(fem_ctx* ctx, const int32_t* bconn, const double* nvec, int nb, int nodes_per_face,
                       const double* U_full, double* F_p, cudaStream_t stream);
 
@@ -230,8 +234,8 @@ int fem_boundary_flux(fem_ctx* ctx, const int32_t* bconn, const double* nvec, in
  * device memory. No counterpart in the reference: the reference has one
  * boundary integral and leaves device memory to XLA.
  *
- * fem_boundary_flux keeps its per-face scratch (nb * nodes_per_face doubles) in
- * the context. When a larger boundary arrives, it grows that scratch with a
+ * fem_boundary_flux keeps its scratch in the context: nb * nodes_per_face
+ * doubles and as many ints per face entry, plus 2 nn + 1 ints for the node table. When a larger boundary arrives, it grows that scratch with a
  * stream synchronize, cudaFree and cudaMalloc, and cudaFree synchronizes the
  * whole device. Some callers cannot do that: a host framework whose handlers
  * must take every device byte from the framework's own allocator, or a

@@ -82,6 +82,11 @@ int fem_launch_interp(const FemLattice& H, const FemLattice& h, const double* xH
 int fem_launch_restrict(const FemLattice& h, const FemLattice& H, const double* xh, double* xH, cudaStream_t s);
 int fem_launch_boundary(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
                         const double* U, int nn, double* Fe, double* Fp, cudaStream_t s);
+// fem_launch_boundary with the scatter as a node-centric gather over a CSR
+// built in cnt (nn ints), off (nn + 1) and list (nb * npf); same result.
+int fem_launch_boundary_csr(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
+                            const double* U, int nn, double* Fe, int* cnt, int* off, int* list, double* Fp,
+                            cudaStream_t s);
 int fem_launch_dot(const double* x, const double* y, int n, double* part, double* out, cudaStream_t s);
 int fem_launch_axpby(double a, const double* x, double b, double* y, int n, cudaStream_t s);
 int fem_launch_scatter(const int64_t* idx, const double* vals, double value, int n, double* out, cudaStream_t s);

@@ -135,6 +135,7 @@ struct fem_ctx {
   FemQuadTab qt{};         // Gauss table of the mesh (2D), for on-the-fly convection
   int conv_otf = 0;        // fem_step4 applies Ce without building it (2D kinds)
   int Fe_cap = 0;
+  int *bs_cnt = nullptr, *bs_off = nullptr, *bs_list = nullptr;  // boundary scatter CSR (nn, nn + 1, Fe_cap)
   int* flags = nullptr;  // device scratch ints
   // optional stage timing
   int timing = 0, nev = 0;
@@ -272,7 +273,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
                   c->rhsU, c->Uhat, c->gPn, c->Ustar, c->rhsP, c->Ce, c->Ce2, c->Ct, c->Mt, c->Ek, c->tau,
-                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab};
+                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab, c->bs_cnt, c->bs_off, c->bs_list};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
@@ -1005,11 +1006,20 @@ extern "C" int fem_boundary_flux(fem_ctx* c, const int32_t* bconn, const double*
   if (nb * npf > c->Fe_cap) {
     FEM_CHECK(cudaStreamSynchronize(s));
     if (c->Fe) cudaFree(c->Fe);
+    if (c->bs_list) cudaFree(c->bs_list);
     c->Fe = nullptr;
+    c->bs_list = nullptr;
+    c->Fe_cap = 0;
     FEM_ALLOC(c->Fe, (size_t)nb * npf);
+    FEM_ALLOC(c->bs_list, (size_t)nb * npf);
     c->Fe_cap = nb * npf;
   }
-  return fem_launch_boundary(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, c->Fe, Fp, s);
+  if (!c->bs_cnt) {
+    FEM_ALLOC(c->bs_cnt, (size_t)c->g.nn);
+    FEM_ALLOC(c->bs_off, (size_t)c->g.nn + 1);
+  }
+  return fem_launch_boundary_csr(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, c->Fe, c->bs_cnt, c->bs_off,
+                                 c->bs_list, Fp, s);
 }
 
 // Fixed per-face scratch of fem_boundary_flux_noalloc: one copy per device in

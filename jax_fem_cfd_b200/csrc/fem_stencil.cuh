@@ -383,32 +383,30 @@ __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid&
   for (int t = tm.cta(); t < ntile; t += tm.ncta()) {
     const int z = t / nt2, rr = t - z * nt2, by = rr / ntx, bx = rr - by * ntx;
     const int x0 = bx * 32 - R, y0 = by * TY - R;
-    auto gidx = [&](int s) -> int {
-      const int lz = D3 ? s / SXY : 0, r2 = s - lz * SXY, ly = r2 / SX, lx = r2 - ly * SX;
-      int gx = x0 + lx, gy = y0 + ly, gz = D3 ? z + lz - 1 : 0;
-      if (g.periodic) {
-        gx = fem_wrap(gx, g.nnx);
-        gy = fem_wrap(gy, g.nny);
-      } else {
-        gx = gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx);
-        gy = gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy);
-      }
-      if (D3) gz = gz < 0 ? 0 : (gz >= g.nnz ? g.nnz - 1 : gz);
-      return (gz * g.nny + gy) * g.nnx + gx;
+    auto rowb = [&](int r) -> int {
+      int gy = y0 + r;
+      gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
+      return gy * g.nnx;
+    };
+    auto colx = [&](int c) -> int {
+      const int gx = x0 + c;
+      return g.periodic ? fem_wrap(gx, g.nnx) : (gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx));
     };
     if constexpr (D3) {
+      // planes z-1, z, z+1 (clamped) one after another, each staged row-wise:
+      // sm[k * NS + lz * SXY + ly * SX + lx]
+      const size_t plane = (size_t)g.nnx * g.nny;
 #pragma unroll
-      for (int k = 0; k < NSRC; ++k) fem_stage(sm + k * NS, src[k], NS, gidx);
+      for (int k = 0; k < NSRC; ++k) {
+        if (src[k] == nullptr) continue;
+#pragma unroll
+        for (int lz = 0; lz < 3; ++lz) {
+          int gz = z + lz - 1;
+          gz = gz < 0 ? 0 : (gz >= g.nnz ? g.nnz - 1 : gz);
+          fem_stage_2d(sm + k * NS + lz * SXY, src[k] + gz * plane, SX, SY, rowb, colx);
+        }
+      }
     } else {
-      auto rowb = [&](int r) -> int {
-        int gy = y0 + r;
-        gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
-        return gy * g.nnx;
-      };
-      auto colx = [&](int c) -> int {
-        const int gx = x0 + c;
-        return g.periodic ? fem_wrap(gx, g.nnx) : (gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx));
-      };
 #pragma unroll
       for (int k = 0; k < NSRC; ++k) fem_stage_2d(sm + k * NS, src[k], SX, SY, rowb, colx);
     }

@@ -193,6 +193,65 @@ __global__ void k_boundary_scatter(const int32_t* __restrict__ bconn, int nb, in
     for (int t = 0; t < nb * npf; ++t) F[bconn[t]] += Fe[t];
 }
 
+// Parallel form of k_boundary_scatter with the same result bit for bit: each
+// node sums its entries t (bconn[t] == node) in increasing t, the serial loop's
+// order, through a node -> entry CSR built on the device (count, one-CTA
+// exclusive scan, fill, then an insertion sort of each node's short list).
+__global__ void k_bs_count(const int32_t* __restrict__ bconn, int m, int nn, int* __restrict__ cnt) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    const int n = bconn[t];
+    if ((unsigned)n < (unsigned)nn) atomicAdd(cnt + n, 1);
+  }
+}
+// off[i] = sum_{i' < i} cnt[i'] for i in [0, nn]; one CTA, each thread a contiguous chunk
+__global__ void k_bs_scan(const int* __restrict__ cnt, int nn, int* __restrict__ off) {
+  __shared__ int part[1024];
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int chunk = (nn + T - 1) / T;
+  const int b = min(nn, tid * chunk), e = min(nn, b + chunk);
+  int sum = 0;
+  for (int i = b; i < e; ++i) sum += cnt[i];
+  part[tid] = sum;
+  __syncthreads();
+  for (int d = 1; d < T; d <<= 1) {
+    const int v = tid >= d ? part[tid - d] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  int run = part[tid] - sum;
+  for (int i = b; i < e; ++i) {
+    off[i] = run;
+    run += cnt[i];
+  }
+  if (tid == T - 1) off[nn] = part[T - 1];
+}
+__global__ void k_bs_fill(const int32_t* __restrict__ bconn, int m, int nn, const int* __restrict__ off,
+                          int* __restrict__ cur, int* __restrict__ list) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    const int n = bconn[t];
+    if ((unsigned)n < (unsigned)nn) list[off[n] + atomicAdd(cur + n, 1)] = t;
+  }
+}
+__global__ void k_bs_gather(const int* __restrict__ off, int* __restrict__ list, const double* __restrict__ Fe, int nn,
+                            double* __restrict__ F) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += gridDim.x * blockDim.x) {
+    const int b = off[n], e = off[n + 1];
+    for (int i = b + 1; i < e; ++i) {
+      const int v = list[i];
+      int j = i - 1;
+      while (j >= b && list[j] > v) {
+        list[j + 1] = list[j];
+        --j;
+      }
+      list[j + 1] = v;
+    }
+    double acc = 0.0;
+    for (int i = b; i < e; ++i) acc += Fe[list[i]];
+    F[n] = acc;
+  }
+}
+
 // ---------------------------------------------------------------- blas-1 ----
 __global__ void k_dot_partial(const double* __restrict__ x, const double* __restrict__ y, int n,
                               double* __restrict__ part) {
@@ -444,6 +503,29 @@ int fem_launch_boundary(const double* coords, int dim, const int32_t* bconn, con
   }
   k_boundary_scatter<<<1, 512, 0, s>>>(bconn, nb, npf, Fe, nn, Fp);
   return fem_after_launch("k_boundary_scatter");
+}
+int fem_launch_boundary_csr(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
+                            const double* U, int nn, double* Fe, int* cnt, int* off, int* list, double* Fp,
+                            cudaStream_t s) {
+  const int m = nb * npf;
+  if (nb > 0) {
+    k_boundary_fe<<<fem_nblocks(nb, 128), 128, 0, s>>>(coords, dim, bconn, nvec, nb, npf, U, nn, Fe);
+    if (int rc = fem_after_launch("k_boundary_fe")) return rc;
+  }
+  if (cudaMemsetAsync(cnt, 0, (size_t)nn * sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");
+  if (m > 0) {
+    k_bs_count<<<fem_nblocks(m, 256), 256, 0, s>>>(bconn, m, nn, cnt);
+    if (int rc = fem_after_launch("k_bs_count")) return rc;
+  }
+  k_bs_scan<<<1, 1024, 0, s>>>(cnt, nn, off);
+  if (int rc = fem_after_launch("k_bs_scan")) return rc;
+  if (cudaMemsetAsync(cnt, 0, (size_t)nn * sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");
+  if (m > 0) {
+    k_bs_fill<<<fem_nblocks(m, 256), 256, 0, s>>>(bconn, m, nn, off, cnt, list);
+    if (int rc = fem_after_launch("k_bs_fill")) return rc;
+  }
+  k_bs_gather<<<fem_nblocks(nn, 256), 256, 0, s>>>(off, list, Fe, nn, Fp);
+  return fem_after_launch("k_bs_gather");
 }
 int fem_launch_dot(const double* x, const double* y, int n, double* part, double* out, cudaStream_t s) {
   const int nb = fem_nblocks(n, 256, 1024);
