@@ -366,14 +366,113 @@ struct FemNoHook {
   __device__ __forceinline__ void operator()() const {}
 };
 
+// 3D form of fem_tiled_stencil. A CTA owns a column tile (32 x TY nodes of an
+// x-y plane) and a run of z-planes, and marches up the run. Each step stages
+// plane z+1 of the NSRC sources (halo included) into `stg`, combines it into a
+// ring of three planes (z-1, z, z+1; clamped at the lattice ends) and applies
+// the stencil on plane z. Every source value is staged and combined once per
+// column tile and run (plus two planes at the run's start) instead of once for
+// each of the planes above, at and below it. The stencil sum of a node (terms,
+// order, coefficients) is the one of the plane-by-plane form. The tile is as
+// tall as the cap_doubles of smem at sm allow ((NSRC + 3) * (32+2R) * (TY+2R)
+// doubles), and the CTAs are spread over runs of z.
+template <int KIND, int NSRC, class Team, class Comb, class Body, class Pre>
+__device__ __forceinline__ void fem_tiled_stencil_3d(const Team& tm, const FemGrid& g, const double* tab,
+                                                     double* __restrict__ sm, const double* const (&src)[NSRC],
+                                                     const Comb& comb, const Body& body, const Pre& pre,
+                                                     int cap_doubles) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  const int WR = blockDim.x >> 5;
+  // the tallest tile the smem allows, then the rows split evenly over as many tiles
+  const int TYmax = fem_tile_rows(g.nnx, g.nny, 1, R, 1, cap_doubles, NSRC + 3);
+  const int nty = (g.nny + TYmax - 1) / TYmax, TY = (g.nny + nty - 1) / nty;
+  const int SX = 32 + 2 * R, SY = TY + 2 * R, SXY = SX * SY;
+  const int ntx = (g.nnx + 31) >> 5, nt2 = ntx * nty;
+  int nzc = tm.ncta() / nt2;
+  if (nzc < 1) nzc = 1;
+  if (nzc > g.nnz) nzc = g.nnz;
+  const int zl = (g.nnz + nzc - 1) / nzc;
+  const int nunit = nt2 * ((g.nnz + zl - 1) / zl);
+  const int tx = threadIdx.x & 31, ty0 = threadIdx.x >> 5;
+  const int nc = fem_axis_ncls(KIND, g.periodic);
+  const size_t plane = (size_t)g.nnx * g.nny;
+  double* __restrict__ stg = sm;                // NSRC * SXY: the plane being staged
+  double* __restrict__ ring = sm + NSRC * SXY;  // 3 * SXY: combined planes
+  bool first = true;
+  for (int u = tm.cta(); u < nunit; u += tm.ncta()) {
+    const int zc = u / nt2, rr = u - zc * nt2, by = rr / ntx, bx = rr - by * ntx;
+    const int z0 = zc * zl, z1 = min(g.nnz, z0 + zl);
+    const int x0 = bx * 32 - R, y0 = by * TY - R;
+    auto rowb = [&](int r) -> int {
+      int gy = y0 + r;
+      gy = g.periodic ? fem_wrap(gy, g.nny) : (gy < 0 ? 0 : (gy >= g.nny ? g.nny - 1 : gy));
+      return gy * g.nnx;
+    };
+    auto colx = [&](int c) -> int {
+      const int gx = x0 + c;
+      return g.periodic ? fem_wrap(gx, g.nnx) : (gx < 0 ? 0 : (gx >= g.nnx ? g.nnx - 1 : gx));
+    };
+    for (int q = z0 - 1; q <= z1; ++q) {
+      const int gz = q < 0 ? 0 : (q >= g.nnz ? g.nnz - 1 : q);
+#pragma unroll
+      for (int k = 0; k < NSRC; ++k)
+        if (src[k] != nullptr) fem_stage_2d(stg + k * SXY, src[k] + gz * plane, SX, SY, rowb, colx);
+      if (first) {
+        pre();
+        first = false;
+      }
+      fem_stage_wait();
+      double* __restrict__ slot = ring + ((q - z0 + 1) % 3) * SXY;
+      for (int s = threadIdx.x; s < SXY; s += blockDim.x) {
+        double v[NSRC];
+#pragma unroll
+        for (int k = 0; k < NSRC; ++k) v[k] = stg[k * SXY + s];
+        slot[s] = comb(s, v);
+      }
+      __syncthreads();
+      if (q > z0) {
+        const int z = q - 1;
+        const double* pl[3] = {ring + ((q - z0 - 1) % 3) * SXY, ring + ((q - z0) % 3) * SXY, slot};
+        const int cz = fem_axis_cls(KIND, 0, z, g.nez);
+        for (int ty = ty0; ty < TY; ty += WR) {
+          const int x = bx * 32 + tx, y = by * TY + ty;
+          if (x < g.nnx && y < g.nny) {
+            const int cx = fem_axis_cls(KIND, g.periodic, x, g.nex), cy = fem_axis_cls(KIND, g.periodic, y, g.ney);
+            const double* c = tab + (size_t)((cz * nc + cy) * nc + cx) * NOFF;
+            double acc = 0.0;
+#pragma unroll
+            for (int dz = 0; dz < W; ++dz)
+#pragma unroll
+              for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+                for (int dx = 0; dx < W; ++dx)
+                  acc += c[(dz * W + dy) * W + dx] * pl[dz][(ty + dy) * SX + tx + dx];
+            const int n = (z * g.nny + y) * g.nnx + x;
+            body(n, x, y, z, acc, pl[1][(ty + R) * SX + tx + R]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (first) pre();
+}
+
 // pre() runs once per CTA while its first tile's copies are in flight (every
 // thread, before comb is used; a CTA without a tile runs it after the loop).
+// cap_doubles: the smem at sm (the 3D form sizes its tiles by it; the 2D
+// form uses FEM_TILE_SMEM).
 template <int KIND, int NSRC, class Team, class Comb, class Body, class Pre = FemNoHook>
 __device__ __forceinline__ void fem_tiled_stencil(const Team& tm, const FemGrid& g, const double* tab,
                                                   double* __restrict__ sm, const double* const (&src)[NSRC],
-                                                  const Comb& comb, const Body& body, const Pre& pre = Pre()) {
+                                                  const Comb& comb, const Body& body, const Pre& pre = Pre(),
+                                                  int cap_doubles = FEM_TILE_SMEM) {
   constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
   constexpr bool D3 = (KIND == FEM_HEX8);
+  if constexpr (D3) {
+    fem_tiled_stencil_3d<KIND, NSRC>(tm, g, tab, sm, src, comb, body, pre, cap_doubles);
+    return;
+  }
   const int WR = blockDim.x >> 5;  // warps = rows per pass
   const int TY = fem_tile_rows(g.nnx, g.nny, g.nnz, R, tm.ncta(), FEM_TILE_SMEM, (D3 ? 3 : 1) * NSRC);
   const int SX = 32 + 2 * R, SY = TY + 2 * R, SXY = SX * SY, NS = SXY * (D3 ? 3 : 1);

@@ -299,7 +299,8 @@ __global__ void k_elem_combine(size_t n, double s_m, const double* __restrict__ 
 // 32 x (blockDim/32) nodes per CTA (3D: one plane), x staged in smem by cp.async.
 template <int KIND>
 __global__ void __launch_bounds__(512) k_stencil_apply(FemGrid g, const double* __restrict__ tab, double alpha,
-                                                       const double* __restrict__ x, double* __restrict__ y) {
+                                                       const double* __restrict__ x, double* __restrict__ y,
+                                                       int cap_doubles) {
   extern __shared__ double sm[];
   __shared__ double stab[FEM_TAB_MAX];
   const int nt = fem_stencil_ncls(g) * KI<KIND>::NOFF;
@@ -311,7 +312,8 @@ __global__ void __launch_bounds__(512) k_stencil_apply(FemGrid g, const double* 
   } tm;
   const double* src[1] = {x};
   fem_tiled_stencil<KIND, 1>(tm, g, stab, sm, src, [](int, const double(&v)[1]) { return v[0]; },
-                             [&](int n, int, int, int, double acc, double) { y[n] = alpha * acc; });
+                             [&](int n, int, int, int, double acc, double) { y[n] = alpha * acc; }, FemNoHook(),
+                             cap_doubles);
 }
 
 // Streaming y = alpha S x (2D kinds) in register strips: a warp owns 32 - 2R
@@ -426,8 +428,9 @@ int fem_launch_shared_apply(int ncomp, const FemGrid& g, const double* A, double
     if (g.kind == FEM_HEX8) {
       constexpr int T = 512, TY = T / 32;
       const int grid = ((g.nnx + 31) / 32) * ((g.nny + TY - 1) / TY) * g.nnz;
-      const int dyn = (32 + 2) * (TY + 2) * 3 * (int)sizeof(double);
-      k_stencil_apply<FEM_HEX8><<<grid, T, dyn, s>>>(g, tab, alpha, x + o, y + o);
+      // fem_tiled_stencil_3d with one source: 1 staged plane + a ring of 3
+      const int dyn = (32 + 2) * (TY + 2) * 4 * (int)sizeof(double);
+      k_stencil_apply<FEM_HEX8><<<grid, T, dyn, s>>>(g, tab, alpha, x + o, y + o, dyn / (int)sizeof(double));
     } else {
       constexpr int M = 16;
       const int ow = (g.kind == FEM_Q2_2D) ? 28 : 30;
