@@ -272,7 +272,13 @@ def transport_elements(solver, nconn, Un, U, dt, D, supg):
     (core/element_calc.py:165-185), Ct = sum_q w dN^T (u u^T) dN (:188-200),
     tau the r = 2 blend of :202-229."""
     wq, N, Nd = solver.ctx.element_data()[:3]
-    nd, nn = solver.ndim, solver.nn
+    return transport_element_matrices(wq, N, Nd, solver.ndim, solver.nn, nconn, Un, U, dt, D, supg)
+
+
+def transport_element_matrices(wq, N, Nd, nd, nn, nconn, Un, U, dt, D, supg):
+    """transport_elements on explicit element data: wq (nq[, 1]), N (nq, nen),
+    Nd (nq, nd, nen) of a uniform mesh, nconn (ne, nen) int64, U_n and U
+    (nd * nn, component-major); torch tensors on any device."""
     w = wq.reshape(-1)
 
     def interp(V):
