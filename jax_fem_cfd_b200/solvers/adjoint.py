@@ -131,7 +131,12 @@ def _ebe(solver, x, alpha, A, beta=0.0, B=None, transB=0, ncomp=None):
 def conv_vjp_u(solver, nconn, a, b, beta):
     """d/dU <a, Ce(U) b> (a, b: ndim*nn vectors, Ce acting on each component)."""
     wq, N, Nd = solver.ctx.element_data()[:3]
-    nd, nn = solver.ndim, solver.nn
+    return conv_vjp_u_elements(wq, N, Nd, solver.ndim, solver.nn, nconn, a, b, beta)
+
+
+def conv_vjp_u_elements(wq, N, Nd, nd, nn, nconn, a, b, beta):
+    """conv_vjp_u on explicit element data (wq (nq[, 1]), N (nq, nen), Nd
+    (nq, nd, nen) of a uniform mesh, nconn (ne, nen) int64)."""
     w = wq.reshape(-1)
     ae = a.view(nd, nn)[:, nconn]  # (c, e, i)
     be = b.view(nd, nn)[:, nconn]

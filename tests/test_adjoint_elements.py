@@ -55,3 +55,25 @@ def test_transport_element_matrices_are_differentiable_in_both_velocities():
     un = t(0.5 * rng.standard_normal(2 * nn)).requires_grad_(True)
     u = t(0.5 * rng.standard_normal(2 * nn)).requires_grad_(True)
     assert torch.autograd.gradcheck(f, (un, u), eps=1e-6, atol=1e-7, rtol=1e-6)
+
+
+@pytest.mark.parametrize("beta", [0.5, 1.0])
+def test_convection_vjp_matches_the_oracle(beta):
+    """Ce(U) is linear in U, so <a, Ce(d) b> = conv_vjp_u(a, b) . d exactly,
+    with Ce from the oracle (core/element_calc.py:165-185) acting on each
+    velocity component."""
+    from oracle import element as oe
+    from oracle import mesh as om
+    from oracle import shape as osh
+    from jax_fem_cfd_b200.solvers.adjoint import conv_vjp_u_elements
+    coords, nconn, *_ = om.create_mesh_2d(5, 4, 1.0, 0.8)
+    wq, N, Nd = osh.quad4_shape_functions(coords[nconn[0]])
+    nn, nd = coords.shape[0], 2
+    rng = np.random.default_rng(11)
+    a, b, d = (rng.standard_normal(nd * nn) for _ in range(3))
+    Ce = oe.conservative_convec_elem_calc(nconn, d, wq, N, Nd, nn, nd, beta)
+    ref = sum(np.einsum("ea,eab,eb->", a[c * nn:(c + 1) * nn][nconn], Ce, b[c * nn:(c + 1) * nn][nconn])
+              for c in range(nd))
+    t = torch.as_tensor
+    g = conv_vjp_u_elements(t(wq), t(N), t(Nd), nd, nn, t(nconn), t(a), t(b), beta)
+    assert abs(float(g @ t(d)) - ref) <= 1e-13 * abs(ref), (float(g @ t(d)), ref)
