@@ -43,10 +43,38 @@ operator: Ce(U) is linear in U, and d/dU <a, Ce(U) b> (conv_vjp_u) is a sum
 over elements and Gauss points of w A_c (N_k d_d B_c + beta d_d N_k B_c), where
 A_c, B_c are a_c, b_c interpolated at the Gauss point.
 """
+import contextlib
+
 import torch
 
 from .. import _lib
 from ..context import ptr, stream
+
+_DEFERRED = []  # device int32 flags of the open deferred_status blocks
+
+
+@contextlib.contextmanager
+def deferred_status():
+    """Inside the block, the solves here do not read their status back on the
+    host after each call (which waits for the device). Each status is folded
+    into one device flag instead, read once when the block ends, and a failure
+    anywhere inside raises FemError then."""
+    flag = torch.zeros(1, dtype=torch.int32, device=torch.device("cuda", torch.cuda.current_device()))
+    _DEFERRED.append(flag)
+    try:
+        yield
+    finally:
+        _DEFERRED.pop()
+    if int(flag.item()) != 0:
+        raise _lib.FemError("a solve inside the deferred-status block failed (status flags "
+                            f"{int(flag.item()):#x})")
+
+
+def _check(st, what):
+    if _DEFERRED:
+        _DEFERRED[-1].bitwise_or_(st[:1])
+    elif int(st.item()) != 0:
+        raise _lib.FemError(f"{what} status {int(st.item())}")
 
 
 def _solver_masks(solver):
@@ -60,14 +88,13 @@ def _pressure(solver, rhs, tol):
     """A+ rhs: the pinned MG-PCG pressure solve of the solver's context from 0."""
     ctx, pm, _ = _solver_masks(solver)
     r = rhs.clone()
-    r[pm] = 0.0
+    r.masked_fill_(pm, 0.0)
     x = torch.zeros_like(r)
     it = torch.zeros(1, dtype=torch.int32, device=r.device)
     st = torch.zeros(1, dtype=torch.int32, device=r.device)
     _lib.call("fem_pressure_solve", ctx.handle, ptr(r), ptr(x), float(tol), 0.0, 1000, solver.precond, 0, 1, ptr(it),
               ptr(st), stream())
-    if int(st.item()) != 0:
-        raise _lib.FemError(f"pressure solve status {int(st.item())}")
+    _check(st, "pressure solve")
     return x
 
 
@@ -98,7 +125,7 @@ class Projection(torch.autograd.Function):
         P = _pressure(solver, rhs, tol)
         U = U_star - c * _grad(solver, P) / M
         if dm is not None:
-            U[dm] = U_d_full[dm]
+            U = torch.where(dm, U_d_full, U)
         fctx.solver, fctx.k, fctx.c, fctx.tol = solver, k, c, tol
         return U, P
 
@@ -110,11 +137,11 @@ class Projection(torch.autograd.Function):
         gU = (gU if gU is not None else torch.zeros(solver.ndim * solver.nn, dtype=torch.float64,
                                                      device=M.device)).contiguous().clone()
         if dm is not None:
-            gU[dm] = 0.0
+            gU.masked_fill_(dm, 0.0)
         w = (gP.contiguous().clone() if gP is not None else torch.zeros(solver.nn, dtype=torch.float64,
                                                                         device=M.device))
         w = w - c * _div(solver, (gU / M).contiguous())
-        w[pm] = 0.0
+        w.masked_fill_(pm, 0.0)
         lam = _pressure(solver, w, tol)
         return gU + k * _grad(solver, lam), None, None, None, None, None, None
 
@@ -160,8 +187,7 @@ def _bicgstab(solver, Ksh, beta, B, mask, rhs, tol, ncomp=None):
     st = torch.zeros(1, dtype=torch.int32, device=rhs.device)
     _lib.call("fem_bicgstab_solve", ctx.handle, ncomp or solver.ndim, 1.0, ptr(Ksh), float(beta), ptr(B), 0.0, None,
               ptr(mask), ptr(rhs), ptr(x), float(tol), 0.0, 0, ptr(it), ptr(st), stream())
-    if int(st.item()) != 0:
-        raise _lib.FemError(f"BiCGSTAB status {int(st.item())}")
+    _check(st, "BiCGSTAB")
     return x
 
 
@@ -187,13 +213,13 @@ class MomentumSolve(torch.autograd.Function):
         dm = solver.dmask.to(torch.bool) if solver.dmask is not None else None
         b = g.clone()
         if dm is not None:
-            b[dm] = 0.0
+            b.masked_fill_(dm, 0.0)
         lam = _bicgstab(solver, Ksh, beta, CeT, solver.dmask, b, tol)
         if dm is not None:
             y = torch.empty_like(lam)
             _lib.call("fem_ebe_apply", solver.ctx.handle, solver.ndim, ptr(lam), ptr(y), 1.0, ptr(Ksh), float(beta),
                       ptr(CeT), 0, 0.0, None, stream())
-            lam[dm] = g[dm] - y[dm]
+            lam = torch.where(dm, g - y, lam)
         return lam, None, None, None, None, None, None, None
 
 
@@ -202,9 +228,9 @@ def _projection_vjp(solver, gU, gP, k, c, tol):
     M = ctx.element_data()[6]
     gU = gU.contiguous().clone()
     if dm is not None:
-        gU[dm] = 0.0
+        gU.masked_fill_(dm, 0.0)
     w = gP.contiguous().clone() - c * _div(solver, (gU / M).contiguous())
-    w[pm] = 0.0
+    w.masked_fill_(pm, 0.0)
     return gU + k * _grad(solver, _pressure(solver, w, tol))
 
 
@@ -225,7 +251,7 @@ class Step(torch.autograd.Function):
         rhs = (_ebe(solver, Un, rho / dt, Me) - (1 - theta) * _ebe(solver, Un, mu, Le, rho, Ce)
                - _grad(solver, Pn))
         if dm is not None:
-            rhs[dm] = U_d_full[dm]
+            rhs = torch.where(dm, U_d_full, rhs)
         Ksh = ((rho / dt) * Me + (theta * mu) * Le).contiguous()
         Uh = _bicgstab(solver, Ksh, theta * rho, Ce, solver.dmask, rhs, tol)
         c, k = dt / rho, rho / dt
@@ -233,7 +259,7 @@ class Step(torch.autograd.Function):
         P = _pressure(solver, k * _div(solver, Us), tol)
         U = Us - c * _grad(solver, P) / M
         if dm is not None:
-            U[dm] = U_d_full[dm]
+            U = torch.where(dm, U_d_full, U)
         fctx.save = (solver, nconn, Un, Ce, Ksh, Uh, dt, rho, mu, tol)
         return U, P
 
@@ -254,7 +280,7 @@ class Step(torch.autograd.Function):
         CeT = Ce.view(-1, nen, nen).transpose(1, 2).contiguous()
         b = gUs.clone()
         if dm is not None:
-            b[dm] = 0.0
+            b.masked_fill_(dm, 0.0)
         lam = _bicgstab(solver, Ksh, theta * rho, CeT, solver.dmask, b, tol)  # = lam_f (0 on gamma_d)
         # rhs = (rho/dt) Me U_n - (1 - theta)(rho Ce(U_n) + mu Le) U_n - G P_n, U_d on gamma_d
         gUn = (_ebe(solver, lam, rho / dt, Me) - (1 - theta) * _ebe(solver, lam, mu, Le, rho, Ce, 1)
@@ -334,8 +360,7 @@ class Transport(torch.autograd.Function):
         st = torch.zeros(1, dtype=torch.int32, device=pn.device)
         _lib.call("fem_transport_phi", ctx.handle, ptr(Un), ptr(Uc), ptr(pn), float(dt), float(D), int(bool(supg)),
                   ptr(phi_mask), ptr(pd), float(tol), ptr(phi), ptr(it), ptr(st), stream())
-        if int(st.item()) != 0:
-            raise _lib.FemError(f"transport BiCGSTAB status {int(st.item())}")
+        _check(st, "transport BiCGSTAB")
         fctx.save = (solver, nconn, Un, Uc, pn, phi, dt, D, supg, phi_mask, tol)
         return phi
 
@@ -353,7 +378,7 @@ class Transport(torch.autograd.Function):
         g = g.contiguous()
         b = g.clone()
         if m is not None:
-            b[m] = 0.0
+            b.masked_fill_(m, 0.0)
         lam = _bicgstab(solver, KA, 1.0, EkT, phi_mask, b, tol, ncomp=1)   # lam_f, 0 on gamma_d_phi
         g_phid = None
         if m is not None:

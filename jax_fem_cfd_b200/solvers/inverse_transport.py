@@ -15,7 +15,7 @@ differentiate its JAX time loop with jax.grad.
 import numpy as np
 import torch
 
-from .adjoint import rollout
+from .adjoint import deferred_status, rollout
 
 
 class InverseTransport:
@@ -56,11 +56,15 @@ class InverseTransport:
         return state[2]
 
     def loss(self, U0, ckpt=None):
-        return (self.mass * (self.final_scalar(U0, ckpt) - self.target) ** 2).sum()
+        """The loss as a 0-d tensor (differentiable in U0). The solves' statuses
+        are read once, at the end, unless an enclosing block defers them."""
+        with deferred_status():
+            return (self.mass * (self.final_scalar(U0, ckpt) - self.target) ** 2).sum()
 
     def value_and_grad(self, U0, ckpt=None):
         """(loss, d loss / d U0) with U0's dtype for the gradient."""
         u = U0.detach().clone().requires_grad_(True)
-        L = self.loss(u, ckpt)
-        L.backward()
+        with deferred_status():
+            L = (self.mass * (self.final_scalar(u, ckpt) - self.target) ** 2).sum()
+            L.backward()
         return float(L.detach()), u.grad
