@@ -293,3 +293,23 @@ def test_transport_rollout_gradient(cavity):
     fd = (lp - lm) / (2 * eps)
     vjp = float((gu0 * du).sum() + (gp0 * dp).sum())
     assert abs(vjp - fd) <= 1e-6 * max(abs(fd), 1.0), (vjp, fd)
+
+
+@pytest.mark.gpu
+def test_deferred_status_raises_when_the_block_ends(cavity):
+    """A solve that fails inside deferred_status (here: a non-finite U*, which
+    the pressure solve reports in its status word) raises FemError when the
+    block ends; outside a block the same call raises at once."""
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.solvers.adjoint import Projection, deferred_status
+    solver, ud = cavity
+    bad = torch.full((solver.ndim * solver.nn,), float("nan"), dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.FemError, match="deferred"):
+        with deferred_status():
+            Projection.apply(bad, solver, 0.01, 1.0, ud, None, 1e-13)
+    with pytest.raises(_lib.FemError, match="pressure solve status 2"):
+        Projection.apply(bad, solver, 0.01, 1.0, ud, None, 1e-13)
+    good = torch.zeros(solver.ndim * solver.nn, dtype=torch.float64, device="cuda")
+    with deferred_status():
+        U, P = Projection.apply(good, solver, 0.01, 1.0, ud, None, 1e-13)
+    assert torch.isfinite(U).all() and torch.isfinite(P).all()
