@@ -432,6 +432,80 @@ def inverse(reps=3, adam_iters=5):
         "adam_lr_0.01_loss": hist}}
 
 
+def cavity_config_64(mod):
+    """64^2 Q1 lid-driven cavity on the unit square, all walls Dirichlet, MG-PCG
+    (final mesh 4 x 4) at tol 1e-8, pinned pressure."""
+    return mod.Config(mesh="simple", solver="standard",
+                      mesh_config=mod.SimpleMeshConfig(num_elem=[64, 64], domain_size=[1.0, 1.0], shape_func_ord=1,
+                                                       periodic=False),
+                      solver_config=mod.StandardSolverConfig(dirichlet_faces=[0, 1, 2, 3], symmetry_faces=[],
+                                                             outlet_faces=[], streamline_diff=False, solver_tol=1e-8,
+                                                             set_zeroP=True, pressure_precond="multigrid",
+                                                             final_multigrid_mesh=[4, 4]))
+
+
+def cavity(steps=200, warmup=3, cpu_steps=40):
+    """The lid-driven cavity: 64^2 Q1, Re 100 (lid u = 1 including the corner
+    nodes, mu = 0.01, rho = 1), dt 0.01, zero initial fields, 200 steps. Device
+    time of the 200 steps with CUDA events (each step: the boundary integral
+    and fem_step4), after `warmup` steps from which the fields are reset to
+    zero; the numpy oracle, 1 thread, on the first `cpu_steps` steps beside it.
+    The working set is L2-resident (no flush): this is the latency-bound end of
+    the path."""
+    import torch
+    from threadpoolctl import threadpool_limits
+
+    import oracle.simulation as osim
+    from jax_fem_cfd_b200.setup import simulation as sim
+
+    def prepare(mod):
+        compute, timestep, nc, sn, h, nn, gd, Ud = mod.setup(cavity_config_64(mod))
+        Ud = mod.set_face_velocity(Ud, sn[2], gd, 1.0, nn, var=1)
+        return compute, timestep, nn, Ud
+
+    compute, timestep, nn, Ud = prepare(sim)
+    solver = timestep.solver
+    bufs = [(torch.zeros(2 * nn, dtype=torch.float64, device="cuda"),
+             torch.zeros(nn, dtype=torch.float64, device="cuda")) for _ in range(2)]
+    its = []
+
+    def run(k):
+        for s in range(k):
+            (U, P), o = bufs[s % 2], bufs[(s + 1) % 2]
+            Fp, F = compute(Ud, None, s * 0.01, (s + 1) * 0.01)
+            _, _, ui, pi = solver.step(U, P, 0.01, 1.0, 0.01, Ud, Fp, F, out=o)
+            its.append((ui, pi))
+
+    run(warmup)
+    for U, P in bufs:
+        U.zero_()
+        P.zero_()
+    its.clear()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    it = np.array([(int(a), int(b)) for a, b in its])
+    with threadpool_limits(1):
+        ocompute, otimestep, onn, oUd = prepare(osim)
+        U, P = np.zeros(2 * onn), np.zeros(onn)
+        t0 = time.perf_counter()
+        for s in range(cpu_steps):
+            Fp, F = ocompute(oUd, None, s * 0.01, (s + 1) * 0.01)
+            U, P, _, _ = otimestep(U, P, 0.01, 1.0, 0.01, oUd, Fp, F)
+        cpu_el = time.perf_counter() - t0
+    return {"cavity_64x64_q1_re100": {
+        "workload": "64^2 Q1 lid-driven cavity, Re 100 (corners on the lid), dt 0.01, 200 steps from zero, FP64, "
+                    "MG-PCG tol 1e-8", "steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
+        "status": int(solver.status.max()), "momentum_iters_mean": float(it[:, 0].mean()),
+        "pressure_iters_mean": float(it[:, 1].mean()),
+        "cpu_baseline": {"value": cpu_steps / cpu_el, "unit": "steps/s", "cores": 1, "kind": "port",
+                         "sample": f"first {cpu_steps} steps of the same workload, numpy oracle, 1 thread"}}}
+
+
 def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv")):
     """3D channel: hex8 256 x 64 x 64 on [0,4] x [0,1] x [0,1] (1,048,576
     elements, 1,090,625 nodes), parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
@@ -597,7 +671,8 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse", "channel3d"],
+    ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse", "channel3d",
+                                       "cavity"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=64, help="--only serving: requests in the stream")
     ap.add_argument("--request-steps", type=int, default=200, help="--only serving: steps per request")
@@ -606,7 +681,7 @@ def main():
         fn = {"matvec": matvec, "poisson_sweep": poisson_sweep,
               "poisson": lambda: {f"poisson_{args.size}x{args.size}_q1": poisson(args.size)},
               "serving": lambda: serving(args.requests, args.request_steps), "inverse": inverse,
-              "channel3d": lambda: channel3d(args.steps)}[args.only]
+              "channel3d": lambda: channel3d(args.steps), "cavity": cavity}[args.only]
         print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
