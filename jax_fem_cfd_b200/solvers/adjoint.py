@@ -50,7 +50,11 @@ import torch
 from .. import _lib
 from ..context import ptr, stream
 
-_DEFERRED = []  # device int32 flags of the open deferred_status blocks
+# Device int32 flags of the open deferred_status blocks. Process-wide, not per
+# thread: the autograd engine runs the backward functions of CUDA tensors on its
+# own device thread, which has to see the flag of the block around backward().
+# So deferred blocks are for one thread at a time.
+_DEFERRED = []
 
 
 @contextlib.contextmanager
@@ -58,7 +62,8 @@ def deferred_status():
     """Inside the block, the solves here do not read their status back on the
     host after each call (which waits for the device). Each status is folded
     into one device flag instead, read once when the block ends, and a failure
-    anywhere inside raises FemError then."""
+    anywhere inside raises FemError then. Blocks nest; they are process-wide
+    (see _DEFERRED), so only one thread at a time may use them."""
     flag = torch.zeros(1, dtype=torch.int32, device=torch.device("cuda", torch.cuda.current_device()))
     _DEFERRED.append(flag)
     try:
