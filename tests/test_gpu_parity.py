@@ -400,6 +400,44 @@ def test_hex8_box_step_parity(precond):
     assert rel(Ug, Uo) < SOLVE_TOL and rel(Pg, Po) < SOLVE_TOL, (rel(Ug, Uo), rel(Pg, Po))
 
 
+def _channel3d_cfg(mod, precond, nel):
+    return mod.Config(mesh="simple", solver="standard",
+                      mesh_config=mod.SimpleMeshConfig(num_elem=nel, domain_size=[4.0, 1.0, 1.0], shape_func_ord=1,
+                                                       periodic=False),
+                      solver_config=mod.StandardSolverConfig(dirichlet_faces=[0, 2, 3, 4, 5], symmetry_faces=[],
+                                                             outlet_faces=[1], streamline_diff=False, solver_tol=1e-8,
+                                                             set_zeroP=True, pressure_precond=precond,
+                                                             final_multigrid_mesh=None))
+
+
+@pytest.mark.parametrize("precond", ["jacobi", "approx_inv"])
+def test_hex8_channel_step_parity(precond):
+    """The 3D channel's boundary set at a small size (hex8 16 x 8 x 8 on
+    [0,4] x [0,1] x [0,1]): parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
+    zero-traction outlet (P = 0) on x = 4, no-slip walls, Re 200, dt 2e-3;
+    3 steps of fem_step4 vs the oracle, boundary integral included."""
+    import oracle.simulation as osim
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    out = []
+    for mod in (gsim, osim):
+        compute, timestep, nc, sn, h, nn, gd, Ud = mod.setup(_channel3d_cfg(mod, precond, [16, 8, 8]))
+        ncn, face = np_(nc), np_(sn[3])
+        y, z = ncn[face, 1], ncn[face, 2]
+        vals = 16 * y * (1 - y) * z * (1 - z)
+        Ud = mod.set_face_velocity(Ud, sn[3], gd, torch.as_tensor(vals) if mod is gsim else vals, nn, var=1)
+        U, P = np.zeros(3 * nn), np.zeros(nn)
+        its = []
+        for s in range(3):
+            Fp, F = compute(Ud, None, s * 2e-3, (s + 1) * 2e-3)
+            U, P, ui, pi = timestep(U, P, 2e-3, 1.0, 1.0 / 200, Ud, Fp, F)
+            its.append((int(ui), int(pi)))
+        out.append((np_(U), np_(P), its, np_(Fp)))
+    (Ug, Pg, ig, Fg), (Uo, Po, io, Fo) = out
+    assert ig == io, (ig, io)
+    assert rel(Fg, Fo) < OPS_TOL, rel(Fg, Fo)
+    assert rel(Ug, Uo) < SOLVE_TOL and rel(Pg, Po) < SOLVE_TOL, (rel(Ug, Uo), rel(Pg, Po))
+
+
 @pytest.mark.parametrize("dim,order", [(2, 2), (3, 1)])
 def test_boundary_flux_faces(dim, order):
     """u.n boundary integral on lin3 edges (Q2) and quad4 faces (hex8) with a
