@@ -344,6 +344,42 @@ def test_passive_transport_step(supg):
     assert rel(U, g["U"]) < SOLVE_TOL and rel(P, g["P"]) < SOLVE_TOL and rel(phi, g["phi"]) < SOLVE_TOL
 
 
+def test_inverse_transport_forward_full_size():
+    """The forward path of the inverse transport workload at its full size and
+    length: 128^2 Q1 unit square, all walls, nu 1e-3, scalar diffusivity 1e-4
+    with SUPG, phi_0 the indicator of [0.4,0.6] x [0.2,0.4], U_0 seeded
+    N(0, 0.1), dt 0.01, 150 steps of the product NS + transport step against the
+    oracle: equal iteration counts every step, fields to 1e-10 at the end."""
+    import oracle.simulation as osim
+    import jax_fem_cfd_b200.setup.simulation as gsim
+
+    def run(mod):
+        cfg = mod.Config(mesh="simple", solver="passive_transport",
+                         mesh_config=mod.SimpleMeshConfig(num_elem=[128, 128], domain_size=[1, 1], shape_func_ord=1,
+                                                          periodic=False),
+                         solver_config=mod.PassiveTransportConfig(
+                             mod.StandardSolverConfig(dirichlet_faces=[0, 1, 2, 3], symmetry_faces=[], outlet_faces=[],
+                                                      streamline_diff=False, solver_tol=1e-8, set_zeroP=True,
+                                                      pressure_precond="multigrid", final_multigrid_mesh=[4, 4]),
+                             mod.ADEConfig(phi_dirichlet_faces=[], phi_SUPG=True)))
+        compute, timestep, nc, sn, h, nn, nnx, nny, gd, Ud, gdp = mod.setup(cfg)
+        x, y = np_(nc)[:, 0], np_(nc)[:, 1]
+        phi = ((x >= 0.4) & (x <= 0.6) & (y >= 0.2) & (y <= 0.4)).astype(np.float64)
+        U, P = 0.1 * np.random.default_rng(0).standard_normal(2 * nn), np.zeros(nn)
+        its = []
+        for _ in range(150):
+            Fp, F = compute(Ud, None, 0, 0)
+            U, P, phi, ui, pi, fi = timestep(U, P, phi, 0.01, 1.0, 1e-3, 1e-4, Ud, None, Fp, F, None)
+            its.append((int(ui), int(pi), int(fi)))
+        return np_(U), np_(P), np_(phi), its
+
+    Ug, Pg, fg, ig = run(gsim)
+    Uo, Po, fo, io = run(osim)
+    assert ig == io, [(k, a, b) for k, (a, b) in enumerate(zip(ig, io)) if a != b][:5]
+    assert rel(Ug, Uo) < SOLVE_TOL and rel(Pg, Po) < SOLVE_TOL and rel(fg, fo) < SOLVE_TOL, (
+        rel(Ug, Uo), rel(Pg, Po), rel(fg, fo))
+
+
 def test_channel_outlet_step():
     import jax_fem_cfd_b200.setup.simulation as gsim
     g = load_golden("step_channel_q1_outlet")
