@@ -52,7 +52,7 @@ extern "C" {
 #define FEM_PREC_NONE 0
 #define FEM_PREC_JACOBI 1
 #define FEM_PREC_APPROX_INV 2
-#define FEM_PREC_APPROX_INV_PT 3 /* passive_transport.py:409-418 variant */
+#define FEM_PREC_APPROX_INV_PT 3 /* solvers/passive_transport.py:141-150 variant */
 #define FEM_PREC_MG 4
 
 /* solver status bits written to the device status word */
@@ -116,7 +116,14 @@ int fem_ctx_set_bc(fem_ctx* ctx, const uint8_t* dmask, const uint8_t* pmask, int
 /* Multigrid hierarchy (core/multigrid.py:9-88): nlev levels obtained by halving
  * nex, ney; level_pmasks is the concatenation over levels of the uint8 gamma_p
  * masks of each level mesh (NULL: node 0 of every level). coarse_tol is the
- * coarsest-level CG tolerance (the reference passes solver_tol). */
+ * coarsest-level CG tolerance (the reference passes solver_tol).
+ * hex8 meshes (an extension: the reference refuses 3D multigrid,
+ * setup/simulation.py:75-76) get the 3D form of the scheme: every axis halved
+ * per level (nex, ney, nez divisible by 2^(nlev-1)), trilinear prolongation
+ * and R = P^T, a degree-3 Chebyshev smoother on D^-1 A with its interval from
+ * a power-iteration estimate of lambda_max, and the coarsest level (at most
+ * 4096 nodes) solved exactly by its inverse, formed on the device here;
+ * coarse_tol is then unused. Pinned pressure only. */
 int fem_ctx_setup_multigrid(fem_ctx* ctx, int nlev, const uint8_t* level_pmasks, double coarse_tol,
                             cudaStream_t stream);
 
@@ -188,7 +195,11 @@ int fem_mg_vcycle(fem_ctx* ctx, const double* r, double* z, cudaStream_t stream)
  * jax_iterative_solvers.py:214 cg). Pinned rows (set_zeroP) or mean-zero
  * handling follow the context's boundary setup. center_rhs subtracts mean(b)
  * first; post applies the final pin/mean fix of solve_pressure. x holds x0 on
- * entry and the solution on exit. iters/status: device int32. */
+ * entry and the solution on exit. iters/status: device int32.
+ * On hex8 with FEM_PREC_MG the solve is the same CG (stop rule, iteration
+ * count) preconditioned by the hex8 V-cycle, run as one CUDA graph whose loop
+ * condition is evaluated on the device; pinned pressure only, and the stream
+ * must not be capturing (FEM_E_STATE). */
 int fem_pressure_solve(fem_ctx* ctx, const double* b, double* x, double tol, double atol, int maxiter, int precond,
                        int center_rhs, int post, int* iters, int* status, cudaStream_t stream);
 
@@ -201,6 +212,16 @@ int fem_pressure_solve(fem_ctx* ctx, const double* b, double* x, double tol, dou
 int fem_bicgstab_solve(fem_ctx* ctx, int ncomp, double alpha, const double* Ash, double beta, const double* B,
                        double gamma, const double* C, const uint8_t* mask, const double* b, double* x, double tol,
                        double atol, int maxiter, int* iters, int* status, cudaStream_t stream);
+
+/* Precision of fem_step4's pressure solve on a hex8 multigrid context:
+ * FEM_PRECISION_FP64 (default, the reference's FP64 CG) or FEM_PRECISION_MIXED
+ * (fem_pressure_solve_mixed's scheme: FP64 refinement, `inner` FP32
+ * multigrid-PCG iterations per cycle, at most max_cycles cycles; iters[1] of
+ * fem_step4 then receives the cycle count). No reference counterpart: the
+ * reference solves in FP64 only. */
+#define FEM_PRECISION_FP64 0
+#define FEM_PRECISION_MIXED 1
+int fem_ctx_set_precision(fem_ctx* ctx, int precision, int inner, int max_cycles);
 
 /* One 4-step projection time step (solvers/standard.py:148 four_step_timestep
  * as called by setup_solver.timestep_loaded :264): Ce(U_n), momentum
@@ -222,37 +243,52 @@ int fem_transport_phi(fem_ctx* ctx, const double* U_n, const double* U, const do
 /* F_p = int_Gamma_d q (u_d . n) over the boundary edges/faces listed in bconn
  * (nb x I, int32, I = 2 lin2, 3 lin3, 4 quad4 faces) with outward normals nvec
  * (nb x dim) and Dirichlet values at their nodes U_b (ndim*nn, full vector)
- * (core/element_calc.py:111 u_dot_n_boundary_integral_1d, :137 _2d). The
- * assembly runs node-parallel: a node -> face-entry table is built on the
- * device on every call, and each node sums its entries in face order. The
- * result is bitwise that of a serial scatter in face order (the reference's
- * segment_sum order). */
+ * (core/element_calc.py:111 u_dot_n_boundary_integral_1d, :137 _2d). quad4
+ * faces belong to the axis-aligned hex8 lattice: their in-plane axes are the
+ * two other than the normal's largest component. The assembly runs
+ * node-parallel: a node -> face-entry table is built on the device on every
+ * call, and each node sums its entries in face order. The result is bitwise
+ * that of a serial scatter in face order (the reference's segment_sum order).
+ * A face that names a node outside [0, nn) is skipped (nothing of it is read
+ * or written); fem_boundary_flux_skipped reports how many were. */
 int fem_boundary_flux(fem_ctx* ctx, const int32_t* bconn, const double* nvec, int nb, int nodes_per_face,
                       const double* U_full, double* F_p, cudaStream_t stream);
+
+/* Number of faces the last fem_boundary_flux / fem_boundary_flux_noalloc call
+ * on ctx skipped because they named a node outside [0, nn); 0 for valid input.
+ * Waits for `stream` (the stream of that call). No reference counterpart: the
+ * reference's segment_sum drops out-of-range segment ids without a report. */
+int fem_boundary_flux_skipped(fem_ctx* ctx, int* count, cudaStream_t stream);
 
 /* Same result as fem_boundary_flux, but the call never allocates or frees
  * device memory. No counterpart in the reference: the reference has one
  * boundary integral and leaves device memory to XLA.
  *
  * fem_boundary_flux keeps its scratch in the context: nb * nodes_per_face
- * doubles and as many ints per face entry, plus 2 nn + 1 ints for the node table. When a larger boundary arrives, it grows that scratch with a
- * stream synchronize, cudaFree and cudaMalloc, and cudaFree synchronizes the
- * whole device. Some callers cannot do that: a host framework whose handlers
- * must take every device byte from the framework's own allocator, or a
+ * doubles and as many ints per face entry, plus 2 nn + 1 ints for the node
+ * table. When a larger boundary arrives, it grows that scratch with a stream
+ * synchronize, cudaFree and cudaMalloc, and cudaFree synchronizes the whole
+ * device. Some callers cannot do that: a host framework whose handlers must
+ * take every device byte from the framework's own allocator, or a
  * time-stepping loop that must not stall the device when its set of boundary
- * faces changes. This entry point is for them. Its scratch is one fixed array
- * of FEM_NOALLOC_FACE_VALUES doubles inside this library, one copy per device,
- * held by every GPU that loads the library until the process exits.
+ * faces changes. This entry point is for them. Its scratch is one fixed
+ * structure inside this library (the face values plus the tables of the
+ * node-parallel assembly, whose node table is a hash table of
+ * 2 * FEM_NOALLOC_FACE_VALUES slots rather than nn entries; 2.9 MB), one copy
+ * per device, held by every GPU that loads the library until the process
+ * exits. The work is the same node-parallel gather as fem_boundary_flux's, and
+ * the flux is bitwise the same.
  *  - nb * nodes_per_face must be <= FEM_NOALLOC_FACE_VALUES (for example 32768
  *    lin2 edges or 16384 quad4 faces). Larger requests return FEM_E_ARG with
  *    the limit in fem_last_error(), and nothing is launched.
  *  - The calling thread's current device must be ctx's device (else
  *    FEM_E_STATE). The first call on each device looks up that device's copy
- *    of the array (cudaGetSymbolAddress, which may load the library's device
- *    code). Make that first call before any stream capture begins.
- *  - Nothing has to start at zero: each call writes every scratch value it
- *    reads, on `stream`, before reading it.
- *  - All calls on one device share the one array, and it keeps the last
+ *    of the structure (cudaGetSymbolAddress, which may load the library's
+ *    device code). Make that first call before any stream capture begins.
+ *  - Nothing has to start at zero: each call clears the tables it counts in
+ *    and writes every other scratch value it reads, on `stream`, before
+ *    reading it.
+ *  - All calls on one device share the one structure, and it keeps the last
  *    call's contents. Two calls that can overlap on the GPU (different streams
  *    with no event between them, or different host threads) race on it and
  *    may return wrong fluxes: order them on one stream. */
@@ -313,7 +349,7 @@ int fem_step4_graph(fem_ctx* ctx, double* U0, double* P0, double* U1, double* P1
 int fem_graph_launch(fem_graph* graph, cudaStream_t stream);
 int fem_graph_destroy(fem_graph* graph);
 
-/* Mixed-precision pressure-Poisson solve of the context's pinned Q1 2D problem
+/* Mixed-precision pressure-Poisson solve of the context's pinned Q1 2D or hex8 problem
  * (the system of fem_pressure_solve with FEM_PREC_MG: gamma_p rows zeroed).
  * FP64 iterative refinement, x += d after each cycle, until
  * ||b - A x|| <= tol ||b|| or max_cycles cycles. The inner solve is `inner`
@@ -324,7 +360,11 @@ int fem_graph_destroy(fem_graph* graph);
  * stream once per cycle to read the residual norm. It needs the context's
  * multigrid hierarchy (fem_ctx_setup_multigrid) with a coarsest level of at most
  * 128 nodes (FEM_E_STATE otherwise), and allocates its FP32 work vectors on the
- * first call. No reference counterpart: the reference solves in FP64 only. */
+ * first call. On hex8 the inner solve uses the hex8 V-cycle (Chebyshev
+ * smoother, FP32 vectors, FP64 sums and FP64 coarsest solve) and the whole
+ * refinement loop is one CUDA graph with a device-side loop condition; the
+ * call then waits for the stream once, at the end. No reference counterpart:
+ * the reference solves in FP64 only. */
 int fem_pressure_solve_mixed(fem_ctx* ctx, const double* b, double* x, double tol, int inner, int max_cycles,
                              int* cycles, double* relres, cudaStream_t stream);
 

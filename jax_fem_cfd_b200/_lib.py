@@ -16,6 +16,7 @@ FEM_KIND_Q1_2D, FEM_KIND_Q2_2D, FEM_KIND_HEX8 = 0, 1, 2
 SHAPE_QUAD4, SHAPE_QUAD9, SHAPE_HEX8, SHAPE_LIN2, SHAPE_LIN3 = 0, 1, 2, 3, 4
 PREC = {None: 0, "none": 0, "jacobi": 1, "approx_inv": 2, "approx_inv_pt": 3, "multigrid": 4}
 STATUS_BARRIER_TIMEOUT, STATUS_NONFINITE, STATUS_MAXITER, STATUS_BREAKDOWN = 1, 2, 4, 8
+PRECISION = {"fp64": 0, "mixed": 1}
 
 
 class MeshDesc(ctypes.Structure):
@@ -53,6 +54,7 @@ SIGNATURES = {
     "fem_transport_phi": (c_int, [P, P, P, P, c_double, c_double, c_int, P, P, c_double, P, P, P, P]),
     "fem_boundary_flux": (c_int, [P, P, P, c_int, c_int, P, P, P]),
     "fem_boundary_flux_noalloc": (c_int, [P, P, P, c_int, c_int, P, P, P]),
+    "fem_boundary_flux_skipped": (c_int, [P, P, P]),
     "fem_scatter": (c_int, [P, P, c_double, c_int, P, P]),
     "fem_make_mask": (c_int, [P, c_int, c_int, P, P]),
     "fem_dot": (c_int, [P, P, P, c_int, P, P]),
@@ -61,6 +63,7 @@ SIGNATURES = {
     "fem_ctx_stage_times": (c_int, [P, P, c_int]),
     "fem_ctx_set_trace": (c_int, [P, P, c_int]),
     "fem_ctx_set_max_ctas": (c_int, [P, c_int, P]),
+    "fem_ctx_set_precision": (c_int, [P, c_int, c_int, c_int]),
     "fem_selftest_barrier_timeout": (c_int, [P, P, P]),
     "fem_pressure_solve_mixed": (c_int, [P, P, P, c_double, c_int, c_int, P, P, P]),
     "fem_step4_graph": (c_int, [P, P, P, P, P, c_double, c_double, c_double, P, P, P, c_double, c_int, c_int, P, P,

@@ -14,7 +14,21 @@ from ..setup.regular_mesh import mesh_of
 
 
 def level_meshes(mesh: Mesh, nlev):
+    if mesh.ndim == 3:
+        return [Mesh(mesh.kind, False, mesh.nex >> l, mesh.ney >> l, mesh.nez >> l, mesh.lx, mesh.ly, mesh.lz)
+                for l in range(nlev)]
     return [Mesh(mesh.kind, mesh.periodic, mesh.nex >> l, mesh.ney >> l, 1, mesh.lx, mesh.ly) for l in range(nlev)]
+
+
+def _face_nodes_3d(m: Mesh):
+    """Node lists of the hex8 faces [D, R, T, L, F, B] (setup/regular_mesh.py:80-96)."""
+    nnx, nny, nnz = m.nex + 1, m.ney + 1, m.nez + 1
+    zoff = np.arange(nnz) * nnx * nny
+    return [np.tile(np.arange(nnx), nnz) + np.repeat(zoff, nnx),
+            np.tile(nnx * np.arange(1, nny + 1) - 1, nnz) + np.repeat(zoff, nny),
+            np.tile(nnx * (nny - 1) + np.arange(nnx), nnz) + np.repeat(zoff, nnx),
+            np.tile(nnx * np.arange(nny), nnz) + np.repeat(zoff, nny),
+            np.arange(nnx * nny), nnx * nny * (nnz - 1) + np.arange(nnx * nny)]
 
 
 def _face_nodes_2d(m: Mesh):
@@ -25,11 +39,12 @@ def _face_nodes_2d(m: Mesh):
 
 def level_pin_sets(mesh: Mesh, nlev, outlet_faces, partial_dirichlet, shape_func_ord):
     """gamma_p of every level (core/multigrid.py:35-62): outlet face nodes plus
-    partial-Dirichlet remainders; [0] when there are none."""
+    partial-Dirichlet remainders; [0] when there are none. hex8 meshes (the 3D
+    extension) take the outlet faces of each level's box."""
     out = []
     for m in level_meshes(mesh, nlev):
         nodes = []
-        surf = None if m.periodic else _face_nodes_2d(m)
+        surf = None if m.periodic else (_face_nodes_3d(m) if m.ndim == 3 else _face_nodes_2d(m))
         if outlet_faces:
             for f in outlet_faces:
                 nodes.append(surf[f])

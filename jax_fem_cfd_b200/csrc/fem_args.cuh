@@ -50,6 +50,8 @@ struct StepArgs {
 // Host launchers (one translation unit per kernel family; fem_capi.cu drives them)
 // ----------------------------------------------------------------------------
 int fem_after_launch(const char* what);  // records launch count / error; 0 or FEM_E_CUDA
+int fem_cuda_error(const char* where, cudaError_t e);  // records e for fem_last_error; FEM_E_CUDA
+char* fem_err_buf();  // the calling thread's fem_last_error buffer (256 bytes)
 
 int fem_launch_mesh_generate(const FemGrid& g, double dx, double dy, double dz, double* coords, int64_t* nconn,
                              cudaStream_t s);
@@ -80,13 +82,28 @@ int fem_launch_elem_combine(size_t n, double s_m, const double* Mt, double s_c, 
 int fem_launch_lincomb(int n, double a, const double* X, double b, const double* Y, double* out, cudaStream_t s);
 int fem_launch_interp(const FemLattice& H, const FemLattice& h, const double* xH, double* xh, cudaStream_t s);
 int fem_launch_restrict(const FemLattice& h, const FemLattice& H, const double* xh, double* xH, cudaStream_t s);
-int fem_launch_boundary(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
-                        const double* U, int nn, double* Fe, double* Fp, cudaStream_t s);
-// fem_launch_boundary with the scatter as a node-centric gather over a CSR
-// built in cnt (nn ints), off (nn + 1) and list (nb * npf); same result.
+// Boundary flux (core/element_calc.py:111-163) assembled per node in face
+// order through a node -> entry CSR in cnt (nn ints), off (nn + 1) and list
+// (nb * npf); faces naming a node outside [0, nn) are skipped and counted in
+// *skipped.
 int fem_launch_boundary_csr(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
-                            const double* U, int nn, double* Fe, int* cnt, int* off, int* list, double* Fp,
-                            cudaStream_t s);
+                            const double* U, int nn, double* Fe, int* cnt, int* off, int* list, int* skipped,
+                            double* Fp, cudaStream_t s);
+// The same result with tables of a fixed size: the CSR is indexed by the slots
+// of a hash table of `cap` node ids (a power of two >= 2 nb npf) instead of by
+// node, so nothing depends on nn.
+struct FemBoundaryHash {
+  int cap;
+  double* Fe;    // nb * npf
+  int* keys;     // cap
+  int* cnt;      // cap
+  int* off;      // cap + 1
+  int* slot;     // nb * npf
+  int* list;     // nb * npf
+  int* skipped;  // 1
+};
+int fem_launch_boundary_hash(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
+                             const double* U, int nn, const FemBoundaryHash& H, double* Fp, cudaStream_t s);
 int fem_launch_dot(const double* x, const double* y, int n, double* part, double* out, cudaStream_t s);
 int fem_launch_axpby(double a, const double* x, double b, double* y, int n, cudaStream_t s);
 int fem_launch_scatter(const int64_t* idx, const double* vals, double value, int n, double* out, cudaStream_t s);

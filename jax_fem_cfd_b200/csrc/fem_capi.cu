@@ -1,6 +1,7 @@
 // Host side of libfemb200: contexts, workspace, cooperative launches and the
 // extern "C" entry points declared in include/fem_b200.h.
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -13,6 +14,7 @@
 
 #include "fem_b200.h"
 #include "fem_args.cuh"
+#include "fem_mg3.cuh"
 
 // NVTX range over one host entry point (a no-op unless a profiler is attached)
 struct FemRange {
@@ -32,6 +34,8 @@ static int set_err(const char* where, cudaError_t e) {
     cudaError_t _e = (call);                        \
     if (_e != cudaSuccess) return set_err(#call, _e); \
   } while (0)
+int fem_cuda_error(const char* where, cudaError_t e) { return set_err(where, e); }
+char* fem_err_buf() { return g_err; }
 int fem_after_launch(const char* what) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaError_t e = cudaGetLastError();
@@ -91,6 +95,8 @@ static FemLattice lattice_of(const FemGrid& g) {
 }
 
 
+#define FEM_FLAG_BOUNDARY_SKIPPED 0
+
 struct CtxLevel {
   FemGrid g;
   double *Le = nullptr, *Leoff = nullptr, *diag = nullptr, *x = nullptr, *r = nullptr, *t = nullptr;
@@ -134,9 +140,10 @@ struct fem_ctx {
   double* ebe_tab = nullptr;  // stencil table of the shared matrix of fem_ebe_apply
   FemQuadTab qt{};         // Gauss table of the mesh (2D), for on-the-fly convection
   int conv_otf = 0;        // fem_step4 applies Ce without building it (2D kinds)
-  int Fe_cap = 0;
+  size_t Fe_cap = 0;       // face entries the boundary-flux scratch holds
   int *bs_cnt = nullptr, *bs_off = nullptr, *bs_list = nullptr;  // boundary scatter CSR (nn, nn + 1, Fe_cap)
-  int* flags = nullptr;  // device scratch ints
+  int* flags = nullptr;  // device ints: [FEM_FLAG_BOUNDARY_SKIPPED] faces skipped by the last flux call,
+                         // [1], [2] cycles and status of the last hex8 mixed solve
   // optional stage timing
   int timing = 0, nev = 0;
   cudaEvent_t ev[16] = {};
@@ -146,6 +153,9 @@ struct fem_ctx {
   float* mx32 = nullptr;              // FP32 vectors of the mixed-precision solve (first use)
   double* mx64 = nullptr;             // its partial sums and scalars
   MxGraphCache mxg;                   // its captured inner solve
+  Mg3* mg3 = nullptr;                 // hex8 multigrid hierarchy and its solve graphs
+  int precision = FEM_PRECISION_FP64; // pressure solve of fem_step4
+  int mx_inner = 6, mx_cycles = 10;   // its mixed-precision parameters
 };
 
 struct fem_graph {
@@ -269,6 +279,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   if (c->mxg.exec) cudaGraphExecDestroy(c->mxg.exec);
   if (c->mx32) cudaFree(c->mx32);
   if (c->mx64) cudaFree(c->mx64);
+  mg3_destroy(c->mg3);
   void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
@@ -416,6 +427,7 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   cudaStream_t s = 0;
   FEM_CHECK(cudaMemset(c->bar, 0, 2 * sizeof(unsigned int)));
   FEM_CHECK(cudaMemset(c->err, 0, sizeof(int)));
+  FEM_CHECK(cudaMemset(c->flags, 0, 16 * sizeof(int)));
   FEM_CHECK(cudaMemset(c->dmask, 0, vn));
   FEM_CHECK(cudaMemset(c->pmask, 0, nn));
   FEM_CHECK(cudaMemset(c->aipin, 0, nn));
@@ -536,9 +548,20 @@ extern "C" int fem_ctx_set_bc(fem_ctx* c, const uint8_t* dmask, const uint8_t* p
 
 extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* level_pmasks, double coarse_tol,
                                        cudaStream_t s) {
-  if (!c || nlev < 1 || nlev > FEM_MAX_LEVELS || c->g.kind == FEM_HEX8) return FEM_E_ARG;
+  if (!c || nlev < 1 || nlev > FEM_MAX_LEVELS) return FEM_E_ARG;
   FEM_CHECK(cudaSetDevice(c->device));
   FEM_CHECK(cudaStreamSynchronize(s));
+  if (c->g.kind == FEM_HEX8) {
+    // hex8: the Chebyshev-smoothed hierarchy of k_mg3.cu (coarse_tol is unused:
+    // its coarsest level is solved exactly)
+    mg3_destroy(c->mg3);
+    c->mg3 = nullptr;
+    c->nlev = 1;
+    FEM_TRY(mg3_setup(&c->mg3, c->g.nex, c->g.ney, c->g.nez, c->lx, c->ly, c->lz, nlev, level_pmasks, c->sms, s));
+    c->nlev = nlev;
+    c->coarse_tol = coarse_tol;
+    return FEM_OK;
+  }
   // a new hierarchy invalidates the mixed-precision solve's buffers and graph
   if (c->mxg.exec) {
     cudaGraphExecDestroy(c->mxg.exec);
@@ -663,6 +686,16 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
 
 extern "C" int fem_ctx_level_info(const fem_ctx* c, int level, int* nn, int* nnx, int* nny, int* nex, int* ney) {
   if (!c || level < 0 || level >= c->nlev) return FEM_E_ARG;
+  if (c->g.kind == FEM_HEX8) {
+    if (!c->mg3) return FEM_E_STATE;
+    const Mg3Geo& G = c->mg3->geo[level];
+    if (nn) *nn = c->mg3->nn[level];
+    if (nnx) *nnx = G.nx;
+    if (nny) *nny = G.ny;
+    if (nex) *nex = G.nx - 1;
+    if (ney) *ney = G.ny - 1;
+    return FEM_OK;
+  }
   const FemGrid& g = c->lv[level].g;
   FemLattice L = lattice_of(g);
   if (nn) *nn = g.nn;
@@ -836,16 +869,45 @@ static int run_cg(fem_ctx* c, const double* b, double* x, double tol, double ato
   return fem_launch_cg(A, grid, cr, cp, cq, s);
 }
 
+// hex8 multigrid-preconditioned CG (k_mg3.cu): pinned pressure only; one graph
+// launch, so the stream must not be capturing
+static int mg3_ready(fem_ctx* c, int center_rhs, cudaStream_t s) {
+  if (!c->mg3 || !c->set_zeroP || center_rhs) {
+    snprintf(g_err, sizeof(g_err), "hex8 multigrid needs a hierarchy and pinned pressure (set_zeroP)");
+    return FEM_E_STATE;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  FEM_CHECK(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    snprintf(g_err, sizeof(g_err), "hex8 multigrid solves launch their own graph and cannot be captured");
+    return FEM_E_STATE;
+  }
+  if (!c->cap_stream) FEM_CHECK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  return FEM_OK;
+}
+
+static int run_mg3(fem_ctx* c, const double* b, double* x, double tol, double atol, int maxiter, int center_rhs,
+                   int* iters, int* status, cudaStream_t s) {
+  FEM_TRY(mg3_ready(c, center_rhs, s));
+  return mg3_pcg(c->mg3, b, x, tol, atol, maxiter, iters, status, s, c->cap_stream);
+}
+
 extern "C" int fem_pressure_solve(fem_ctx* c, const double* b, double* x, double tol, double atol, int maxiter,
                                   int precond, int center_rhs, int post, int* iters, int* status, cudaStream_t s) {
   const FemRange range("fem_pressure_solve");
   if (!c || !b || !x || !iters || !status || precond < 0 || precond > 4 || maxiter < 0) return FEM_E_ARG;
   if (precond == FEM_PREC_MG && c->nlev < 2) return FEM_E_STATE;
+  if (precond == FEM_PREC_MG && c->g.kind == FEM_HEX8) return run_mg3(c, b, x, tol, atol, maxiter, center_rhs,
+                                                                       iters, status, s);
   return run_cg(c, b, x, tol, atol, maxiter, precond, center_rhs, post, iters, status, s);
 }
 
 extern "C" int fem_mg_vcycle(fem_ctx* c, const double* r, double* z, cudaStream_t s) {
   if (!c || !r || !z || c->nlev < 2) return FEM_E_ARG;
+  if (c->g.kind == FEM_HEX8) {
+    if (!c->mg3) return FEM_E_STATE;
+    return mg3_vcycle64(c->mg3, r, z, s);
+  }
   CgArgs A;
   fill_cg_args(c, A);
   FEM_CHECK(cudaMemcpyAsync(c->pr, r, sizeof(double) * c->g.nn, cudaMemcpyDeviceToDevice, s));
@@ -954,8 +1016,18 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   // 5. PPE rhs and x0 (:97-107)
   FEM_TRY(fem_launch_p_rhs(S, c->Ustar, Fp, Pn, c->rhsP, Po, s));
   stage_mark(c, s);
-  // 6. pressure (P)CG, maxiter 1000 (:115-123)
-  FEM_TRY(run_cg(c, c->rhsP, Po, tol, 0.0, 1000, precond, c->set_zeroP ? 0 : 1, 1, iters + 1, status + 1, s));
+  // 6. pressure (P)CG, maxiter 1000 (:115-123); hex8 multigrid runs the k_mg3.cu
+  // solve, in mixed precision when the context asks for it
+  if (precond == FEM_PREC_MG && g.kind == FEM_HEX8) {
+    FEM_TRY(mg3_ready(c, c->set_zeroP ? 0 : 1, s));
+    if (c->precision == FEM_PRECISION_MIXED)
+      FEM_TRY(mg3_mixed(c->mg3, c->rhsP, Po, tol, c->mx_inner, c->mx_cycles, iters + 1, status + 1, s,
+                        c->cap_stream));
+    else
+      FEM_TRY(mg3_pcg(c->mg3, c->rhsP, Po, tol, 0.0, 1000, iters + 1, status + 1, s, c->cap_stream));
+  } else {
+    FEM_TRY(run_cg(c, c->rhsP, Po, tol, 0.0, 1000, precond, c->set_zeroP ? 0 : 1, 1, iters + 1, status + 1, s));
+  }
   stage_mark(c, s);
   // 7. projection and Dirichlet values (:160-163)
   FEM_TRY(fem_launch_ufinal(S, c->Ustar, Po, Ud, Uo, s));
@@ -991,7 +1063,7 @@ extern "C" int fem_transport_phi(fem_ctx* c, const double* Un, const double* U, 
     FEM_CHECK(cudaMemsetAsync(c->Ct, 0, ntot * sizeof(double), s));
     FEM_CHECK(cudaMemsetAsync(c->Mt, 0, ntot * sizeof(double), s));
   }
-  // rhs and x0 (:294-301 / :318-325)
+  // rhs and x0 (solvers/passive_transport.py:26-33 / :50-57)
   FEM_TRY(fem_launch_phi_rhs(g, c->Me, c->Le, dt, D, c->Mt, c->Ce, c->Ct, phin, phi_mask, phid, c->rhsP, phio, s));
   // lhs: [(1/dt) Me + 0.5 D Le] + [(1/dt) Mtau + 0.5 (Ce + Ctau)]
   FEM_TRY(fem_launch_lincomb(g.nen * g.nen, 1.0 / dt, c->Me, 0.5 * D, c->Le, c->Kd, s));
@@ -1003,52 +1075,75 @@ extern "C" int fem_transport_phi(fem_ctx* c, const double* Un, const double* U, 
 extern "C" int fem_boundary_flux(fem_ctx* c, const int32_t* bconn, const double* nvec, int nb, int npf,
                                  const double* U, double* Fp, cudaStream_t s) {
   if (!c || !bconn || !nvec || !U || !Fp || nb < 0 || npf < 2 || npf > 4) return FEM_E_ARG;
-  if (nb * npf > c->Fe_cap) {
+  const long long need = (long long)nb * npf;
+  if (need > INT_MAX) {
+    snprintf(g_err, sizeof(g_err), "fem_boundary_flux: nb * nodes_per_face = %lld exceeds INT_MAX", need);
+    return FEM_E_ARG;
+  }
+  if (need > (long long)c->Fe_cap) {
     FEM_CHECK(cudaStreamSynchronize(s));
     if (c->Fe) cudaFree(c->Fe);
     if (c->bs_list) cudaFree(c->bs_list);
     c->Fe = nullptr;
     c->bs_list = nullptr;
     c->Fe_cap = 0;
-    FEM_ALLOC(c->Fe, (size_t)nb * npf);
-    FEM_ALLOC(c->bs_list, (size_t)nb * npf);
-    c->Fe_cap = nb * npf;
+    FEM_ALLOC(c->Fe, (size_t)need);
+    FEM_ALLOC(c->bs_list, (size_t)need);
+    c->Fe_cap = (size_t)need;
   }
   if (!c->bs_cnt) {
     FEM_ALLOC(c->bs_cnt, (size_t)c->g.nn);
     FEM_ALLOC(c->bs_off, (size_t)c->g.nn + 1);
   }
   return fem_launch_boundary_csr(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, c->Fe, c->bs_cnt, c->bs_off,
-                                 c->bs_list, Fp, s);
+                                 c->bs_list, c->flags + FEM_FLAG_BOUNDARY_SKIPPED, Fp, s);
 }
 
-// Fixed per-face scratch of fem_boundary_flux_noalloc: one copy per device in
-// this library's device image, shared by every call on that device. Each call
-// writes all nb * npf values it later reads (k_boundary_fe before
-// k_boundary_scatter, same stream), so no value has to start at zero.
-static __device__ __align__(256) double g_noalloc_fe[FEM_NOALLOC_FACE_VALUES];
+extern "C" int fem_boundary_flux_skipped(fem_ctx* c, int* count, cudaStream_t s) {
+  if (!c || !count) return FEM_E_ARG;
+  FEM_CHECK(cudaMemcpyAsync(count, c->flags + FEM_FLAG_BOUNDARY_SKIPPED, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FEM_CHECK(cudaStreamSynchronize(s));
+  return FEM_OK;
+}
+
+// Fixed scratch of fem_boundary_flux_noalloc: one copy per device in this
+// library's device image, shared by every call on that device. The tables of
+// the node-parallel assembly are sized by the face-entry limit alone (a hash
+// table of 2 FEM_NOALLOC_FACE_VALUES node slots replaces the per-node table),
+// 44 bytes per face entry, 2.9 MB in all. Each call clears the tables it
+// counts in and writes every other value before reading it, on its stream.
+#define FEM_NOALLOC_SLOTS (2 * FEM_NOALLOC_FACE_VALUES)
+struct NoallocScratch {
+  double fe[FEM_NOALLOC_FACE_VALUES];
+  int keys[FEM_NOALLOC_SLOTS];
+  int cnt[FEM_NOALLOC_SLOTS];
+  int off[FEM_NOALLOC_SLOTS + 1];
+  int slot[FEM_NOALLOC_FACE_VALUES];
+  int list[FEM_NOALLOC_FACE_VALUES];
+};
+static __device__ __align__(256) NoallocScratch g_noalloc;
 
 #define FEM_NOALLOC_MAX_DEVICES 64
 static std::mutex g_noalloc_mu;
-static double* g_noalloc_fe_ptr[FEM_NOALLOC_MAX_DEVICES] = {};
+static NoallocScratch* g_noalloc_ptr[FEM_NOALLOC_MAX_DEVICES] = {};
 
-// Device address of `device`'s copy of g_noalloc_fe (host code cannot use the
+// Device address of `device`'s copy of g_noalloc (host code cannot use the
 // symbol itself). Looked up once per device on its first call, with that
 // device current; later calls read the cached value.
-static int noalloc_fe_scratch(int device, double** out) {
+static int noalloc_scratch(int device, NoallocScratch** out) {
   if (device < 0 || device >= FEM_NOALLOC_MAX_DEVICES) {
     snprintf(g_err, sizeof(g_err), "fem_boundary_flux_noalloc: device %d beyond the %d supported", device,
              FEM_NOALLOC_MAX_DEVICES);
     return FEM_E_ARG;
   }
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_fe_ptr[device]) {
-    double* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_fe);
-    if (e != cudaSuccess) return set_err("cudaGetSymbolAddress(g_noalloc_fe)", e);
-    g_noalloc_fe_ptr[device] = p;
+  if (!g_noalloc_ptr[device]) {
+    NoallocScratch* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc);
+    if (e != cudaSuccess) return set_err("cudaGetSymbolAddress(g_noalloc)", e);
+    g_noalloc_ptr[device] = p;
   }
-  *out = g_noalloc_fe_ptr[device];
+  *out = g_noalloc_ptr[device];
   return FEM_OK;
 }
 
@@ -1070,9 +1165,11 @@ extern "C" int fem_boundary_flux_noalloc(fem_ctx* c, const int32_t* bconn, const
              cur, c->device);
     return FEM_E_STATE;
   }
-  double* fe = nullptr;
-  FEM_TRY(noalloc_fe_scratch(cur, &fe));
-  return fem_launch_boundary(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, fe, Fp, s);
+  NoallocScratch* sc = nullptr;
+  FEM_TRY(noalloc_scratch(cur, &sc));
+  const FemBoundaryHash H{FEM_NOALLOC_SLOTS, sc->fe,   sc->keys, sc->cnt,
+                          sc->off,           sc->slot, sc->list, c->flags + FEM_FLAG_BOUNDARY_SKIPPED};
+  return fem_launch_boundary_hash(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, H, Fp, s);
 }
 
 extern "C" int fem_scatter(const int64_t* idx, const double* vals, double value, int n, double* out,
@@ -1195,6 +1292,19 @@ extern "C" int fem_pressure_solve_mixed(fem_ctx* c, const double* b, double* x, 
                                         int max_cycles, int* cycles, double* relres, cudaStream_t s) {
   const FemRange range("fem_pressure_solve_mixed");
   if (!c || !b || !x || !(tol > 0.0) || inner < 1 || max_cycles < 1) return FEM_E_ARG;
+  if (c->g.kind == FEM_HEX8) {
+    if (c->nlev < 2) return FEM_E_STATE;
+    FEM_TRY(mg3_ready(c, 0, s));
+    int* dev = c->flags + 1;  // cycles, status
+    FEM_TRY(mg3_mixed(c->mg3, b, x, tol, inner, max_cycles, dev, dev + 1, s, c->cap_stream));
+    int h[2] = {0, 0};
+    FEM_CHECK(cudaMemcpyAsync(h, dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    double rr = 0.0;
+    FEM_TRY(mg3_last_relres(c->mg3, &rr, s));
+    if (cycles) *cycles = h[0];
+    if (relres) *relres = rr;
+    return FEM_OK;
+  }
   if (c->g.kind != FEM_Q1_2D || !c->set_zeroP || c->nlev < 2) return FEM_E_STATE;
   if (c->lv[c->nlev - 1].g.nn > 128) return FEM_E_STATE;  // the one-warp coarse CG
   const int grid = c->sms * 8;
@@ -1216,6 +1326,15 @@ extern "C" int fem_selftest_barrier_timeout(fem_ctx* c, int* status, cudaStream_
   FEM_TRY(reset_sync(c, s));
   const FemSync S{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS, nullptr, 0};
   return fem_launch_selftest_barrier(S, status, s);
+}
+
+extern "C" int fem_ctx_set_precision(fem_ctx* c, int precision, int inner, int max_cycles) {
+  if (!c || (precision != FEM_PRECISION_FP64 && precision != FEM_PRECISION_MIXED) || inner < 1 || max_cycles < 1)
+    return FEM_E_ARG;
+  c->precision = precision;
+  c->mx_inner = inner;
+  c->mx_cycles = max_cycles;
+  return FEM_OK;
 }
 
 extern "C" int fem_ctx_set_max_ctas(fem_ctx* c, int ctas, int* capacity) {

@@ -33,7 +33,7 @@
 #define FEM_PREC_NONE 0
 #define FEM_PREC_JACOBI 1
 #define FEM_PREC_APPROX_INV 2     // solvers/standard.py:225-234 (D1L[gp] = 0)
-#define FEM_PREC_APPROX_INV_PT 3  // solvers/passive_transport.py:409-418 (keeps D1x/D1L on gp)
+#define FEM_PREC_APPROX_INV_PT 3  // solvers/passive_transport.py:141-150 (keeps D1x/D1L on gp)
 #define FEM_PREC_MG 4
 
 struct MgLevel {

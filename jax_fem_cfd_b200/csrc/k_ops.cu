@@ -111,14 +111,23 @@ __global__ void k_restrict(FemLattice h, FemLattice H, const double* __restrict_
 }
 
 // ------------------------------------------------------------- boundary flux --
-// Per boundary face: Fe_I = sum_q (N w)[q][I] (n . U_q); then a single-thread
-// scatter in face order (segment_sum order of core/element_calc.py:131-133).
+// Per boundary face: Fe_I = sum_q (N w)[q][I] (n . U_q) (core/element_calc.py:
+// 111-163); the per-node sums in face order follow (the segment_sum order of
+// core/element_calc.py:131-133). A face that names a node outside [0, nn) is
+// skipped: its entries get Fe = 0, nothing of it is read, and *skipped counts it.
 __global__ void k_boundary_fe(const double* __restrict__ coords, int dim, const int32_t* __restrict__ bconn,
                               const double* __restrict__ nvec, int nb, int npf, const double* __restrict__ U, int nn,
-                              double* __restrict__ Fe) {
+                              double* __restrict__ Fe, int* __restrict__ skipped) {
   const double s3 = 1.0 / sqrt(3.0), g35 = sqrt(3.0 / 5.0);
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nb; f += gridDim.x * blockDim.x) {
     const int32_t* nd = bconn + (size_t)f * npf;
+    bool bad = false;
+    for (int I = 0; I < npf; ++I) bad |= (unsigned)nd[I] >= (unsigned)nn;
+    if (bad) {
+      for (int I = 0; I < npf; ++I) Fe[(size_t)f * npf + I] = 0.0;
+      atomicAdd(skipped, 1);
+      continue;
+    }
     double nrm[3] = {nvec[f * dim], nvec[f * dim + 1], dim == 3 ? nvec[f * dim + 2] : 0.0};
     double Ub[4][3];
     for (int I = 0; I < npf; ++I)
@@ -151,10 +160,12 @@ __global__ void k_boundary_fe(const double* __restrict__ coords, int dim, const 
         for (int d = 0; d < 2; ++d) un += nrm[d] * (Nq[0] * Ub[0][d] + Nq[1] * Ub[1][d] + Nq[2] * Ub[2][d]);
         for (int I = 0; I < 3; ++I) out[I] += (Nq[I] * w) * un;
       }
-    } else {  // quad4 face of a hex: in-plane axes are those orthogonal to the normal
-      int ax[2], na = 0;
-      for (int d = 0; d < 3 && na < 2; ++d)
-        if (nrm[d] == 0.0) ax[na++] = d;
+    } else {  // quad4 face of an axis-aligned hex: the in-plane axes are the two
+              // other than the normal's dominant component
+      int dn = 0;
+      for (int d = 1; d < 3; ++d)
+        if (fabs(nrm[d]) > fabs(nrm[dn])) dn = d;
+      const int ax[2] = {dn == 0 ? 1 : 0, dn == 2 ? 1 : 2};
       const double sx[4] = {-1, 1, 1, -1}, sy[4] = {-1, -1, 1, 1};
       for (int q = 0; q < 4; ++q) {
         const double xi = sx[q] * s3, eta = sy[q] * s3;
@@ -184,19 +195,11 @@ __global__ void k_boundary_fe(const double* __restrict__ coords, int dim, const 
   }
 }
 
-__global__ void k_boundary_scatter(const int32_t* __restrict__ bconn, int nb, int npf, const double* __restrict__ Fe,
-                                   int nn, double* __restrict__ F) {
-  // one CTA: zero, then a serial scatter in face order (deterministic)
-  for (int i = threadIdx.x; i < nn; i += blockDim.x) F[i] = 0.0;
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int t = 0; t < nb * npf; ++t) F[bconn[t]] += Fe[t];
-}
-
-// Parallel form of k_boundary_scatter with the same result bit for bit: each
-// node sums its entries t (bconn[t] == node) in increasing t, the serial loop's
-// order, through a node -> entry CSR built on the device (count, one-CTA
-// exclusive scan, fill, then an insertion sort of each node's short list).
+// Node-parallel assembly with the result of a serial scatter in face order,
+// bit for bit: each node sums its entries t (bconn[t] == node) in increasing t,
+// through a node -> entry CSR built on the device (count, one-CTA exclusive
+// scan, fill, then an insertion sort of each node's short list). Entries whose
+// node is outside [0, nn) are left out.
 __global__ void k_bs_count(const int32_t* __restrict__ bconn, int m, int nn, int* __restrict__ cnt) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
     const int n = bconn[t];
@@ -250,6 +253,64 @@ __global__ void k_bs_gather(const int* __restrict__ off, int* __restrict__ list,
     for (int i = b; i < e; ++i) acc += Fe[list[i]];
     F[n] = acc;
   }
+}
+
+// The same assembly with tables of a fixed size, independent of nn (the
+// no-allocation entry point): the CSR is indexed by slots of an open-addressing
+// hash table of `cap` (a power of two, at least twice the entry count) node ids
+// instead of by node. Slot assignment depends on the order of the atomics, but
+// every slot holds one node and sums its entries in increasing t, so F is the
+// same as the per-node CSR's. keys must be -1 and cnt, cur zero on entry.
+__global__ void k_bh_count(const int32_t* __restrict__ bconn, int m, int nn, int cap, int* __restrict__ keys,
+                           int* __restrict__ slot, int* __restrict__ cnt) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    const int n = bconn[t];
+    int h = -1;
+    if ((unsigned)n < (unsigned)nn) {
+      // linear probing; the table is at most half full, so a free slot or the
+      // node's own slot is met within cap probes
+      unsigned p = ((unsigned)n * 2654435761u) & (unsigned)(cap - 1);
+      for (int k = 0; k < cap; ++k, p = (p + 1) & (unsigned)(cap - 1)) {
+        const int prev = atomicCAS(keys + p, -1, n);
+        if (prev == -1 || prev == n) {
+          h = (int)p;
+          break;
+        }
+      }
+      if (h >= 0) atomicAdd(cnt + h, 1);
+    }
+    slot[t] = h;
+  }
+}
+__global__ void k_bh_fill(const int* __restrict__ slot, int m, const int* __restrict__ off, int* __restrict__ cur,
+                          int* __restrict__ list) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    const int h = slot[t];
+    if (h >= 0) list[off[h] + atomicAdd(cur + h, 1)] = t;
+  }
+}
+__global__ void k_bh_gather(const int* __restrict__ keys, int cap, const int* __restrict__ off, int* __restrict__ list,
+                            const double* __restrict__ Fe, double* __restrict__ F) {
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < cap; h += gridDim.x * blockDim.x) {
+    const int n = keys[h];
+    if (n < 0) continue;
+    const int b = off[h], e = off[h + 1];
+    for (int i = b + 1; i < e; ++i) {
+      const int v = list[i];
+      int j = i - 1;
+      while (j >= b && list[j] > v) {
+        list[j + 1] = list[j];
+        --j;
+      }
+      list[j + 1] = v;
+    }
+    double acc = 0.0;
+    for (int i = b; i < e; ++i) acc += Fe[list[i]];
+    F[n] = acc;
+  }
+}
+__global__ void k_fill_zero(double* __restrict__ F, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F[i] = 0.0;
 }
 
 // ---------------------------------------------------------------- blas-1 ----
@@ -498,21 +559,37 @@ int fem_launch_restrict(const FemLattice& h, const FemLattice& H, const double* 
   k_restrict<<<fem_nblocks((long long)H.nx * H.ny, 256), 256, 0, s>>>(h, H, xh, xH);
   return fem_after_launch("k_restrict");
 }
-int fem_launch_boundary(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
-                        const double* U, int nn, double* Fe, double* Fp, cudaStream_t s) {
+int fem_launch_boundary_hash(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
+                             const double* U, int nn, const FemBoundaryHash& H, double* Fp, cudaStream_t s) {
+  const int m = nb * npf;
+  if (cudaMemsetAsync(H.skipped, 0, sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");
   if (nb > 0) {
-    k_boundary_fe<<<fem_nblocks(nb, 128), 128, 0, s>>>(coords, dim, bconn, nvec, nb, npf, U, nn, Fe);
+    k_boundary_fe<<<fem_nblocks(nb, 128), 128, 0, s>>>(coords, dim, bconn, nvec, nb, npf, U, nn, H.Fe, H.skipped);
     if (int rc = fem_after_launch("k_boundary_fe")) return rc;
   }
-  k_boundary_scatter<<<1, 512, 0, s>>>(bconn, nb, npf, Fe, nn, Fp);
-  return fem_after_launch("k_boundary_scatter");
+  k_fill_zero<<<fem_nblocks(nn, 256), 256, 0, s>>>(Fp, nn);
+  if (int rc = fem_after_launch("k_fill_zero")) return rc;
+  if (m == 0) return FEM_OK;
+  if (cudaMemsetAsync(H.keys, 0xff, (size_t)H.cap * sizeof(int), s) != cudaSuccess ||
+      cudaMemsetAsync(H.cnt, 0, (size_t)H.cap * sizeof(int), s) != cudaSuccess)
+    return fem_after_launch("memset");
+  k_bh_count<<<fem_nblocks(m, 256), 256, 0, s>>>(bconn, m, nn, H.cap, H.keys, H.slot, H.cnt);
+  if (int rc = fem_after_launch("k_bh_count")) return rc;
+  k_bs_scan<<<1, 1024, 0, s>>>(H.cnt, H.cap, H.off);
+  if (int rc = fem_after_launch("k_bs_scan")) return rc;
+  if (cudaMemsetAsync(H.cnt, 0, (size_t)H.cap * sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");
+  k_bh_fill<<<fem_nblocks(m, 256), 256, 0, s>>>(H.slot, m, H.off, H.cnt, H.list);
+  if (int rc = fem_after_launch("k_bh_fill")) return rc;
+  k_bh_gather<<<fem_nblocks(H.cap, 256), 256, 0, s>>>(H.keys, H.cap, H.off, H.list, H.Fe, Fp);
+  return fem_after_launch("k_bh_gather");
 }
 int fem_launch_boundary_csr(const double* coords, int dim, const int32_t* bconn, const double* nvec, int nb, int npf,
-                            const double* U, int nn, double* Fe, int* cnt, int* off, int* list, double* Fp,
-                            cudaStream_t s) {
+                            const double* U, int nn, double* Fe, int* cnt, int* off, int* list, int* skipped,
+                            double* Fp, cudaStream_t s) {
   const int m = nb * npf;
+  if (cudaMemsetAsync(skipped, 0, sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");
   if (nb > 0) {
-    k_boundary_fe<<<fem_nblocks(nb, 128), 128, 0, s>>>(coords, dim, bconn, nvec, nb, npf, U, nn, Fe);
+    k_boundary_fe<<<fem_nblocks(nb, 128), 128, 0, s>>>(coords, dim, bconn, nvec, nb, npf, U, nn, Fe, skipped);
     if (int rc = fem_after_launch("k_boundary_fe")) return rc;
   }
   if (cudaMemsetAsync(cnt, 0, (size_t)nn * sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_ufinal(StepArgs S, const dou
   }
 }
 
-// Scalar transport rhs (passive_transport.py:294-301 / 318-325):
+// Scalar transport rhs (solvers/passive_transport.py:26-33 / 50-57):
 // rhs = (1/dt)(Me + Mtau_e) phi_n - 0.5 (Ce_n + D Le + Ctau_e) phi_n, with the
 // per-element parts pre-combined into Erhs_e; Dirichlet rows -> phi_d.
 template <int KIND>

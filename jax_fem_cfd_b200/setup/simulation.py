@@ -33,6 +33,9 @@ class StandardSolverConfig:
     set_zeroP: bool
     pressure_precond: Optional[str] = None
     final_multigrid_mesh: Optional[List[int]] = None
+    # Extension (no reference field): "mixed" runs the hex8 multigrid pressure
+    # solve as FP64 refinement around FP32 multigrid-PCG iterations.
+    precision: str = "fp64"
 
 
 @dataclass
@@ -78,10 +81,26 @@ class Config:
         if len(self.mesh_config.num_elem) == 3:
             if self.mesh_config.shape_func_ord == 2:
                 raise ValueError("3D quadratic shape functions not yet implemented")
-            if ns.pressure_precond == "multigrid":
-                raise ValueError("3D multigrid not yet implemented")
             if self.mesh_config.periodic:
                 raise ValueError("3D periodic boundary conditions not yet implemented")
+            # 3D multigrid is this package's extension (the reference raises
+            # "3D multigrid not yet implemented"): all axes coarsen together,
+            # pressure must be pinned
+            if ns.pressure_precond == "multigrid":
+                fm = ns.final_multigrid_mesh
+                if fm is None or len(fm) != 3:
+                    raise ValueError("3D multigrid needs a 3-entry final_multigrid_mesh")
+                ratios = {n // f for n, f in zip(self.mesh_config.num_elem, fm) if f > 0}
+                if len(ratios) != 1 or any(n % f for n, f in zip(self.mesh_config.num_elem, fm)):
+                    raise ValueError("3D multigrid halves every axis together: num_elem / final_multigrid_mesh "
+                                     "must be the same power of two on all axes")
+                if not ns.set_zeroP:
+                    raise ValueError("3D multigrid needs pinned pressure (set_zeroP=True)")
+        if getattr(ns, "precision", "fp64") not in ("fp64", "mixed"):
+            raise ValueError(f"Unknown precision: {ns.precision}")
+        if getattr(ns, "precision", "fp64") == "mixed" and not (len(self.mesh_config.num_elem) == 3
+                                                                and ns.pressure_precond == "multigrid"):
+            raise ValueError("precision='mixed' is implemented for the 3D multigrid pressure solve")
         if ns.pressure_precond == "multigrid":
             num_elemf = ns.final_multigrid_mesh
             if num_elemf is None:
@@ -251,7 +270,7 @@ def timestep_loop(t_final, dt, save_interval, print_interval, compute_func, time
 
 def timestep_loop_scan(dt, num_steps, compute_func, timestep_func, rho, mu, D, U_d, phi_d, U0, P0, phi0, S_func):
     """setup/simulation.py:362-374 with the step's argument order
-    (U_d, phi_d, F_p, F) of solvers/passive_transport.py:445."""
+    (U_d, phi_d, F_p, F) of solvers/passive_transport.py:177-178."""
     F_p, F = compute_func(U_d, S_func, 0, 0)
     U, P, phi = f64(U0), f64(P0), f64(phi0)
     for _ in range(int(num_steps)):

@@ -17,6 +17,11 @@ from ..core import multigrid as mg
 from ..setup.regular_mesh import mesh_of
 
 
+# mixed-precision pressure solve: FP32 multigrid-PCG iterations per FP64
+# refinement cycle, and the cap on cycles
+MIXED_INNER, MIXED_CYCLES = 4, 10
+
+
 class NSSolver:
     """Device-resident state of one NS problem: context, boundary sets,
     multigrid hierarchy, cached Dirichlet vectors."""
@@ -37,6 +42,8 @@ class NSSolver:
             pins = mg.level_pin_sets(mesh, nlev, solver_cfg.outlet_faces, mesh_cfg.partial_dirichlet,
                                      mesh_cfg.shape_func_ord)
             self.hier = mg.Hierarchy(ctx, nlev, pins, solver_cfg.solver_tol)
+        precision = getattr(solver_cfg, "precision", "fp64")
+        _lib.call("fem_ctx_set_precision", ctx.handle, _lib.PRECISION[precision], MIXED_INNER, MIXED_CYCLES)
         self.bconn = bconn.to(torch.int32).contiguous() if bconn is not None else None
         self.nvec = f64(nvec).reshape(-1) if nvec is not None else None
         self.iters = torch.zeros(2, dtype=torch.int32, device=ctx.dev)

@@ -145,6 +145,16 @@ def make_pressure_M_op(NS_config, mesh_config, Le, nconn, nn, gamma_p, mesh_func
             t[gamma_p] = 0
             return 3 * D1x - 3 * D1L + t / L_diag
         return op
+    if prec == "multigrid" and len(mesh_config.num_elem) == 3:
+        # build-defined 3D extension (oracle/multigrid3d.py)
+        from . import multigrid3d as mg3
+        levels = mg3.multigrid3d_setup(mesh_config.num_elem, NS_config.final_multigrid_mesh,
+                                       mesh_config.domain_size, NS_config.outlet_faces)
+
+        def op3(r):
+            return mg3.v_cycle3d(r, levels)
+        op3.levels = levels
+        return op3
     if prec == "multigrid":
         data = mg.multigrid_setup(mesh_config.num_elem, NS_config.final_multigrid_mesh,
                                   mesh_config.domain_size, NS_config.outlet_faces, mesh_func, shape_func,

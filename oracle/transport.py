@@ -100,7 +100,7 @@ def setup_solver(node_coords, nconn, bconn, nvec, gamma_d, gamma_p, nn, gamma_d_
         L_diag = ecalc.laplacian_diag(Le, nconn, nn)
 
         def M_op(r, nconn):
-            # passive_transport.py:412-418 keeps the D1x / D1L values on gamma_p
+            # passive_transport.py:147-149 keeps the D1x / D1L values on gamma_p
             D1x = r / L_diag
             D1L = emult.laplacian_element_mult(D1x, Le, nconn, nn) / L_diag
             D1L[gamma_p] = D1x[gamma_p]

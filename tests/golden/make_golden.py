@@ -1,6 +1,6 @@
 """Generate golden fixtures by executing the reference's own modules.
 
-Run from the repository root:  python tests/golden/make_golden.py [/path/to/reference]
+Run from the repository root:  python tests/golden/make_golden.py <path to the jax-fem-cfd checkout>
 
 The reference (jax_fem_cfd) needs jax 0.4.13, which is not installable here; its
 modules are executed under ``jax_shim`` (a numpy restatement of the JAX API subset
@@ -17,7 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import jax_shim  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: python tests/golden/make_golden.py <path to the jax-fem-cfd checkout>")
+REF = sys.argv[1]
 R = jax_shim.load_reference(REF)
 rm, sf, ec, em = R["regular_mesh"], R["shape_functions"], R["element_calc"], R["element_mult"]
 mg, its, std, pt, sim = R["multigrid"], R["jax_iterative_solvers"], R["standard"], R["passive_transport"], R["simulation"]

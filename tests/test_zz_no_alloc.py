@@ -3,13 +3,16 @@
 The no-allocation entry point serves callers that must not allocate device
 memory during a call, for example a host framework that hands out every device
 byte through its own allocator. It keeps its per-face scratch in a fixed array
-inside the library instead of in the context. Both entry points run the same
-kernels, so on the same inputs they agree to rounding (relative 1e-14 here).
-Two calls in a row check that reusing the shared array, which keeps the first
-call's values, still gives correct results.
+inside the library instead of in the context. Both entry points evaluate the
+faces with the same kernel and sum each node's entries in face order, so on
+the same inputs they agree bit for bit (the test allows relative 1e-14). Two
+calls in a row check that reusing the shared array, which keeps the first
+call's values, still gives correct results; a free-memory reading before and
+after further calls checks that they allocate nothing.
 
 This file is collected last, so a run that stops at the first failure has run
 every other test before it."""
+import ctypes
 import os
 import re
 
@@ -102,3 +105,54 @@ def test_noalloc_flux_rejects_more_faces_than_its_scratch():
     assert b"exceeds the fixed scratch" in lib.fem_last_error()
     torch.cuda.synchronize()
     assert float(F.abs().max()) == 0.0
+
+
+def test_noalloc_calls_allocate_no_device_memory():
+    solver, nn = _channel_solver(1)
+    g = torch.Generator().manual_seed(11)
+    U = torch.randn(solver.ndim * nn, generator=g, dtype=torch.float64).cuda()
+    ref = _flux("fem_boundary_flux", solver, solver.bconn, solver.nvec, U, nn)
+    F = torch.empty(nn, dtype=torch.float64, device="cuda")
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import ptr, stream
+
+    def call():
+        _lib.call("fem_boundary_flux_noalloc", solver.ctx.handle, ptr(solver.bconn), ptr(solver.nvec),
+                  int(solver.bconn.shape[0]), int(solver.bconn.shape[1]), ptr(U), ptr(F), stream())
+
+    call()  # the first call on the device looks up the library's scratch
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        call()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0, (free0, free1)
+    assert _rel(F, ref) < TOL
+
+
+def test_bad_node_index_is_skipped_and_reported_by_both_entry_points():
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import ptr, stream
+    solver, nn = _channel_solver(2)
+    lib = _lib.load()
+    g = torch.Generator().manual_seed(5)
+    U = torch.randn(solver.ndim * nn, generator=g, dtype=torch.float64).cuda()
+    nb = solver.bconn.shape[0]
+    bad = solver.bconn.clone()
+    bad[3, 1] = nn + 5  # one node id past the mesh
+    nv = solver.nvec.view(nb, -1)
+    keep = [f for f in range(nb) if f != 3]
+    b_ok = solver.bconn[keep].contiguous()
+    n_ok = nv[keep].reshape(-1).contiguous()
+    ref = _flux("fem_boundary_flux", solver, b_ok, n_ok, U, nn)
+    for name in ("fem_boundary_flux", "fem_boundary_flux_noalloc"):
+        got = _flux(name, solver, bad, solver.nvec, U, nn)
+        cnt = ctypes.c_int(-1)
+        assert lib.fem_boundary_flux_skipped(solver.ctx.handle, ctypes.byref(cnt), stream()) == 0
+        assert cnt.value == 1, (name, cnt.value)
+        assert torch.equal(got, ref), name
+    _flux("fem_boundary_flux_noalloc", solver, solver.bconn, solver.nvec, U, nn)
+    cnt = ctypes.c_int(-1)
+    assert lib.fem_boundary_flux_skipped(solver.ctx.handle, ctypes.byref(cnt), stream()) == 0
+    assert cnt.value == 0
