@@ -506,26 +506,38 @@ def cavity(steps=200, warmup=3, cpu_steps=40):
                          "sample": f"first {cpu_steps} steps of the same workload, numpy oracle, 1 thread"}}}
 
 
-def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv")):
+def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid", "multigrid_mixed")):
     """3D channel: hex8 256 x 64 x 64 on [0,4] x [0,1] x [0,1] (1,048,576
     elements, 1,090,625 nodes), parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
     zero-traction outlet (P = 0) on x = 4, no-slip walls, Re 200 (mu = 1/200,
-    rho = 1), dt 2e-3, zero initial fields, FP64 at tol 1e-8. Pressure
-    preconditioners the 3D path accepts (multigrid is 2D only, as in
-    setup/simulation.py:81-82). One step = the boundary integral plus fem_step4;
-    device time with CUDA events, working set beyond L2 (Ce alone is 537 MB)."""
+    rho = 1), dt 2e-3, zero initial fields, tol 1e-8. Pressure solves: Jacobi
+    and approx_inv PCG (FP64, the preconditioners the reference's 3D path
+    accepts), the hex8 multigrid PCG (4 levels down to 32 x 8 x 8 elements,
+    Chebyshev degree 3; FP64), and the same multigrid as FP32 inner iterations
+    inside FP64 refinement to 1e-8 ("multigrid_mixed", the configuration the
+    workload names). One step = the boundary integral plus fem_step4; device
+    time with CUDA events, working set beyond L2 (Ce alone is 537 MB). Each
+    arm's final U and P are compared with the Jacobi arm's (FP64, same
+    tolerance)."""
     import torch
 
     from jax_fem_cfd_b200.setup import simulation as sim
     out = {}
+    ref = None
     for pc in preconds:
+        prec, extra = pc, {}
+        if pc.startswith("multigrid"):
+            prec = "multigrid"
+            extra = {"final_multigrid_mesh": [32, 8, 8]}
+            if pc.endswith("mixed"):
+                extra["precision"] = "mixed"
         cfg = sim.Config(mesh="simple", solver="standard",
                          mesh_config=sim.SimpleMeshConfig(num_elem=[256, 64, 64], domain_size=[4.0, 1.0, 1.0],
                                                           shape_func_ord=1, periodic=False),
                          solver_config=sim.StandardSolverConfig(dirichlet_faces=[0, 2, 3, 4, 5], symmetry_faces=[],
                                                                 outlet_faces=[1], streamline_diff=False,
-                                                                solver_tol=1e-8, set_zeroP=True, pressure_precond=pc,
-                                                                final_multigrid_mesh=None))
+                                                                solver_tol=1e-8, set_zeroP=True, pressure_precond=prec,
+                                                                **extra))
         compute, timestep, nc, sn, h, nn, gd, Ud = sim.setup(cfg)
         y, z = nc[sn[3], 1], nc[sn[3], 2]
         Ud = sim.set_face_velocity(Ud, sn[3], gd, 16 * y * (1 - y) * z * (1 - z), nn, var=1)
@@ -552,15 +564,24 @@ def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv")):
         ms = e0.elapsed_time(e1)
         it = np.array([(int(a), int(b)) for a, b in its[warmup:]])
         st = int(solver.status.max())
-        U = bufs[(warmup + steps) % 2][0]
+        U, P = bufs[(warmup + steps) % 2]
         out[pc] = {"steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps, "status": st,
                    "momentum_iters_mean": float(it[:, 0].mean()), "pressure_iters_mean": float(it[:, 1].mean()),
                    "pressure_iters_first_last": [int(it[0, 1]), int(it[-1, 1])],
                    "u_max_after": float(U[:nn].max()), "finite": bool(torch.isfinite(U).all())}
+        if pc.endswith("mixed"):
+            out[pc]["pressure_iters_are"] = "FP64 refinement cycles (4 FP32 multigrid-PCG iterations each)"
+        if ref is None:
+            ref = (U.clone(), P.clone())
+        else:
+            out[pc]["rel_err_vs_" + preconds[0]] = {
+                "U": float(torch.linalg.vector_norm(U - ref[0]) / torch.linalg.vector_norm(ref[0])),
+                "P": float(torch.linalg.vector_norm(P - ref[1]) / torch.linalg.vector_norm(ref[1]))}
         del compute, timestep, solver, bufs, nc, sn, gd, Ud
         torch.cuda.empty_cache()
+    del ref
     return {"channel3d_hex8_256x64x64": {
-        "workload": "hex8 256x64x64 channel, parabolic inflow, outlet, Re 200, dt 2e-3, FP64 tol 1e-8, zero start",
+        "workload": "hex8 256x64x64 channel, parabolic inflow, outlet, Re 200, dt 2e-3, tol 1e-8, zero start",
         "timed_steps": steps, "warmup": warmup, **out}}
 
 

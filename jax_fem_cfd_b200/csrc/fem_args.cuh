@@ -3,6 +3,7 @@
 #include <stdint.h>
 #include "fem_solvers.cuh"
 #include "fem_conv.cuh"
+#include "fem_conv3.cuh"
 
 #define FEM_THREADS 512
 #define FEM_OP_THREADS 256
@@ -113,6 +114,12 @@ int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double
                             cudaStream_t s);
 int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc,
                           double alpha, const double* Ash, const double* x, double* y, int grid, cudaStream_t s);
+// hex8: the Gauss-point factors (32 per element, element-major) and
+// y = alpha Ash x + cc Ce x per component (3 components) from them
+int fem_launch_conv_factors3(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,
+                             cudaStream_t s);
+int fem_launch_conv_apply3(const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc, double alpha,
+                           const double* Ash, const double* x, double* y, int grid, int* err, cudaStream_t s);
 
 int fem_launch_selftest_barrier(const FemSync& sync, int* status, cudaStream_t s);
 // mixed-precision pinned Poisson solve (k_mixed.cu); work: 6 sum(nn_l) + 3 nn_0

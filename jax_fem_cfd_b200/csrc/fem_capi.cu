@@ -139,7 +139,7 @@ struct fem_ctx {
   double* cvf = nullptr;   // Gauss-point factors of Ce(U_n) (3 nq per element, structure of arrays)
   double* ebe_tab = nullptr;  // stencil table of the shared matrix of fem_ebe_apply
   FemQuadTab qt{};         // Gauss table of the mesh (2D), for on-the-fly convection
-  int conv_otf = 0;        // fem_step4 applies Ce without building it (2D kinds)
+  int conv_otf = 0;        // fem_step4 applies Ce without building it
   size_t Fe_cap = 0;       // face entries the boundary-flux scratch holds
   int *bs_cnt = nullptr, *bs_off = nullptr, *bs_list = nullptr;  // boundary scatter CSR (nn, nn + 1, Fe_cap)
   int* flags = nullptr;  // device ints: [FEM_FLAG_BOUNDARY_SKIPPED] faces skipped by the last flux call,
@@ -154,6 +154,7 @@ struct fem_ctx {
   double* mx64 = nullptr;             // its partial sums and scalars
   MxGraphCache mxg;                   // its captured inner solve
   Mg3* mg3 = nullptr;                 // hex8 multigrid hierarchy and its solve graphs
+  Mg3* mg2 = nullptr;                 // 2D hierarchy of the graph-driven mixed-precision solve (first use)
   int precision = FEM_PRECISION_FP64; // pressure solve of fem_step4
   int mx_inner = 6, mx_cycles = 10;   // its mixed-precision parameters
 };
@@ -280,6 +281,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   if (c->mx32) cudaFree(c->mx32);
   if (c->mx64) cudaFree(c->mx64);
   mg3_destroy(c->mg3);
+  mg3_destroy(c->mg2);
   void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
@@ -422,7 +424,7 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   FEM_ALLOC(c->Ce, (size_t)g.ne * per);
   FEM_ALLOC(c->vcv, vn);
   FEM_ALLOC(c->ebe_tab, FEM_TAB_MAX);
-  if (g.kind != FEM_HEX8) FEM_ALLOC(c->cvf, (size_t)3 * c->nq * g.ne);
+  FEM_ALLOC(c->cvf, g.kind == FEM_HEX8 ? (size_t)FEM_C3_NF * g.ne : (size_t)3 * c->nq * g.ne);
   FEM_ALLOC(c->dotpart, 4096);
   cudaStream_t s = 0;
   FEM_CHECK(cudaMemset(c->bar, 0, 2 * sizeof(unsigned int)));
@@ -458,18 +460,19 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   FEM_TRY(fem_launch_invdiag(g.nn, c->Ldiag, c->pmask, L0.invD, L0.winvD, s));
   c->nlev = 1;
   FEM_CHECK(cudaDeviceSynchronize());
-  // Gauss table for the on-the-fly convection of fem_step4 (2D kinds)
-  if (g.kind != FEM_HEX8 && c->nq <= FEM_QT_MAX && nen <= FEM_QT_MAX) {
-    double hw[FEM_QT_MAX], hN[FEM_QT_MAX * FEM_QT_MAX], hdN[2 * FEM_QT_MAX * FEM_QT_MAX];
+  // Gauss table for the on-the-fly convection of fem_step4
+  if (c->nq <= FEM_QT_MAX && nen <= FEM_QT_MAX) {
+    double hw[FEM_QT_MAX], hN[FEM_QT_MAX * FEM_QT_MAX], hdN[3 * FEM_QT_MAX * FEM_QT_MAX];
     FEM_CHECK(cudaMemcpy(hw, c->wq, sizeof(double) * c->nq, cudaMemcpyDeviceToHost));
     FEM_CHECK(cudaMemcpy(hN, c->N, sizeof(double) * c->nq * nen, cudaMemcpyDeviceToHost));
-    FEM_CHECK(cudaMemcpy(hdN, c->dN, sizeof(double) * c->nq * 2 * nen, cudaMemcpyDeviceToHost));
+    FEM_CHECK(cudaMemcpy(hdN, c->dN, sizeof(double) * c->nq * nd * nen, cudaMemcpyDeviceToHost));
     for (int q = 0; q < c->nq; ++q) {
       c->qt.w[q] = hw[q];
       for (int b = 0; b < nen; ++b) {
         c->qt.N[q][b] = hN[q * nen + b];
-        c->qt.dx[q][b] = hdN[(q * 2 + 0) * nen + b];
-        c->qt.dy[q][b] = hdN[(q * 2 + 1) * nen + b];
+        c->qt.dx[q][b] = hdN[(q * nd + 0) * nen + b];
+        c->qt.dy[q][b] = hdN[(q * nd + 1) * nen + b];
+        c->qt.dz[q][b] = nd == 3 ? hdN[(q * nd + 2) * nen + b] : 0.0;
       }
     }
     const char* ev = getenv("FEM_CONV_OTF");
@@ -542,6 +545,11 @@ extern "C" int fem_ctx_set_bc(fem_ctx* c, const uint8_t* dmask, const uint8_t* p
     FEM_CHECK(cudaMemcpyAsync(c->aipin, pmask, nn, cudaMemcpyDeviceToDevice, s));
   }
   c->set_zeroP = set_zeroP ? 1 : 0;
+  if (c->mg2) {  // its pins and mean-zero form follow the boundary sets
+    FEM_CHECK(cudaStreamSynchronize(s));
+    mg3_destroy(c->mg2);
+    c->mg2 = nullptr;
+  }
   FEM_TRY(fem_launch_invdiag(c->g.nn, c->Ldiag, c->pmask, c->lv[0].invD, c->lv[0].winvD, s));
   return FEM_OK;
 }
@@ -575,6 +583,8 @@ extern "C" int fem_ctx_setup_multigrid(fem_ctx* c, int nlev, const uint8_t* leve
     cudaFree(c->mx64);
     c->mx64 = nullptr;
   }
+  mg3_destroy(c->mg2);
+  c->mg2 = nullptr;
   const FemGrid& g0 = c->g;
   for (int l = 1; l < nlev; ++l)
     if ((g0.nex >> l) < 1 || (g0.ney >> l) < 1) return FEM_E_ARG;
@@ -892,6 +902,33 @@ static int run_mg3(fem_ctx* c, const double* b, double* x, double tol, double at
   return mg3_pcg(c->mg3, b, x, tol, atol, maxiter, iters, status, s, c->cap_stream);
 }
 
+// 2D multigrid hierarchy of the graph-driven mixed-precision solve, built on
+// first use from the context's multigrid levels (k_mg3.cu, mg2_setup)
+static int mg2_ready(fem_ctx* c, cudaStream_t s) {
+  if (c->nlev < 2 || c->g.kind == FEM_HEX8) return FEM_E_STATE;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  FEM_CHECK(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    snprintf(g_err, sizeof(g_err), "mixed-precision solves launch their own graph and cannot be captured");
+    return FEM_E_STATE;
+  }
+  if (!c->cap_stream) FEM_CHECK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  if (c->mg2) return FEM_OK;
+  FemGrid grids[FEM_MAX_LEVELS];
+  const double* tabs[FEM_MAX_LEVELS];
+  const double* diags[FEM_MAX_LEVELS];
+  const uint8_t* pins[FEM_MAX_LEVELS];
+  for (int l = 0; l < c->nlev; ++l) {
+    const CtxLevel& L = c->lv[l];
+    grids[l] = L.g;
+    tabs[l] = L.tab;
+    diags[l] = (l == 0) ? c->Ldiag : L.diag;
+    pins[l] = (l == 0 && !L.pin) ? c->pmask : L.pin;
+  }
+  FEM_CHECK(cudaStreamSynchronize(s));
+  return mg2_setup(&c->mg2, c->nlev, grids, tabs, diags, pins, c->set_zeroP ? 0 : 1, c->sms, s);
+}
+
 extern "C" int fem_pressure_solve(fem_ctx* c, const double* b, double* x, double tol, double atol, int maxiter,
                                   int precond, int center_rhs, int post, int* iters, int* status, cudaStream_t s) {
   const FemRange range("fem_pressure_solve");
@@ -971,10 +1008,14 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   const double theta = 0.5;
   c->nev = 0;
   stage_mark(c, s);
-  // 1. Ce(U_n), beta = 1/2 (solvers/standard.py:152). On-the-fly (2D): Ce is
-  // never built; instead (mu Le + rho Ce) U_n of the momentum rhs is applied here.
-  const bool otf = c->conv_otf && c->cvf && g.kind != FEM_HEX8 && nd == 2;
-  if (otf) {
+  // 1. Ce(U_n), beta = 1/2 (solvers/standard.py:152). On the fly: Ce is never
+  // built; its Gauss-point factors are, and (mu Le + rho Ce) U_n of the momentum
+  // rhs is applied here.
+  const bool otf = c->conv_otf && c->cvf;
+  if (otf && g.kind == FEM_HEX8) {
+    FEM_TRY(fem_launch_conv_factors3(g, c->qt, Un, 0.5, c->cvf, s));
+    FEM_TRY(fem_launch_conv_apply3(g, c->qt, c->cvf, rho, mu, c->Le, Un, c->vcv, c->sms, c->err, s));
+  } else if (otf) {
     FEM_TRY(fem_launch_conv_factors(g, c->qt, Un, 0.5, c->cvf, s));
     FEM_TRY(fem_launch_conv_apply(2, g, c->qt, c->cvf, rho, mu, c->Le, Un, c->vcv, c->sms, s));
   } else {
@@ -1025,6 +1066,10 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
                         c->cap_stream));
     else
       FEM_TRY(mg3_pcg(c->mg3, c->rhsP, Po, tol, 0.0, 1000, iters + 1, status + 1, s, c->cap_stream));
+  } else if (precond == FEM_PREC_MG && c->precision == FEM_PRECISION_MIXED) {
+    FEM_TRY(mg2_ready(c, s));
+    FEM_TRY(mg3_mixed(c->mg2, c->rhsP, Po, tol, c->mx_inner, c->mx_cycles, iters + 1, status + 1, s,
+                      c->cap_stream));
   } else {
     FEM_TRY(run_cg(c, c->rhsP, Po, tol, 0.0, 1000, precond, c->set_zeroP ? 0 : 1, 1, iters + 1, status + 1, s));
   }
@@ -1305,7 +1350,20 @@ extern "C" int fem_pressure_solve_mixed(fem_ctx* c, const double* b, double* x, 
     if (relres) *relres = rr;
     return FEM_OK;
   }
-  if (c->g.kind != FEM_Q1_2D || !c->set_zeroP || c->nlev < 2) return FEM_E_STATE;
+  if (c->nlev < 2) return FEM_E_STATE;
+  if (c->g.kind != FEM_Q1_2D || !c->set_zeroP) {
+    // quad9 or mean-zero: the graph-driven solve over the 2D hierarchy
+    FEM_TRY(mg2_ready(c, s));
+    int* dev = c->flags + 1;  // cycles, status
+    FEM_TRY(mg3_mixed(c->mg2, b, x, tol, inner, max_cycles, dev, dev + 1, s, c->cap_stream));
+    int h[2] = {0, 0};
+    FEM_CHECK(cudaMemcpyAsync(h, dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    double rr = 0.0;
+    FEM_TRY(mg3_last_relres(c->mg2, &rr, s));
+    if (cycles) *cycles = h[0];
+    if (relres) *relres = rr;
+    return FEM_OK;
+  }
   if (c->lv[c->nlev - 1].g.nn > 128) return FEM_E_STATE;  // the one-warp coarse CG
   const int grid = c->sms * 8;
   if (!c->mx32) {

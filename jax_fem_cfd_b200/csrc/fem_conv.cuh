@@ -18,6 +18,7 @@ struct FemQuadTab {
   double N[FEM_QT_MAX][FEM_QT_MAX];   // [q][node]
   double dx[FEM_QT_MAX][FEM_QT_MAX];  // d N_node / dx at q
   double dy[FEM_QT_MAX][FEM_QT_MAX];  // d N_node / dy at q
+  double dz[FEM_QT_MAX][FEM_QT_MAX];  // d N_node / dz at q (hex8)
   // Q2 tensor factors (filled and checked on the host): N[q][b] = nx[qx][i] ny[qy][j],
   // dx[q][b] = ddx[qx][i] ny[qy][j], dy[q][b] = nx[qx][i] ddy[qy][j] for node b at
   // element-local lattice offset (i, j) and Gauss point q = qi[qy][qx]

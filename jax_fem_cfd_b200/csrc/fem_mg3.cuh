@@ -31,11 +31,20 @@ struct Mg3Geo {
   double m[3][3][3];
 };
 
+// One 2D lattice level (quad4 / quad9, periodic or not): the grid, its full
+// lattice (transfers) and the assembled stencil table of its Laplacian
+// (fem_stencil.cuh).
+struct Mg2Geo {
+  FemGrid g;
+  FemLattice lat;
+  const double* tab;
+};
+
 // Level vectors of storage type T: rhs r, residual t, iterates xa / xb,
 // Chebyshev direction d; invD = 1/diag(A), 0 on gamma_p.
-template <class T>
+template <class T, class G = Mg3Geo>
 struct Mg3Lev {
-  Mg3Geo geo;
+  G geo;
   const T* invD;
   T *r, *t, *xa, *xb, *d;
 };
@@ -47,6 +56,7 @@ struct Mg3Scal {
   int maxiter, max_cycles;
   double gamma, beta, gamma_i, beta_i;
   double rr, rr0, bb, atol2, relres;
+  double zbar;       // mean of the inner preconditioned residual (mean-zero problems)
   int k, cycles, status, out_iters, out_status, pad;
   unsigned long long t0;
 };
@@ -61,7 +71,10 @@ struct Mg3GraphCache {
 
 struct Mg3 {
   int nlev = 0, sms = 148, cap = 148 * 8;
+  int d2 = 0;   // 2D lattice levels (geo2, m64, m32) instead of hex8 ones (geo, l64, l32)
+  int mz = 0;   // mean-zero (periodic) pressure: no gamma_p, solutions centred
   Mg3Geo geo[FEM_MAX_LEVELS];
+  Mg2Geo geo2[FEM_MAX_LEVELS];
   size_t off[FEM_MAX_LEVELS] = {};
   int nn[FEM_MAX_LEVELS] = {};
   size_t total = 0;
@@ -76,17 +89,24 @@ struct Mg3 {
   float* v32 = nullptr;            // p_old, p_new, Ap, d of the FP32 inner solve
   double *x64 = nullptr, *b64 = nullptr;  // solve input / iterate
   double* Ainv = nullptr;          // coarsest level inverse (n x n)
-  double* parts = nullptr;         // 4 partial-sum slots: p.Ap, r.r, b.b, r.z
+  double* parts = nullptr;         // 6 partial-sum slots: p.Ap, r.r, b.b, r.z, sum z, sum r
   Mg3Scal* sc = nullptr;
   double* gj = nullptr;            // setup scratch
   cudaStream_t s2 = nullptr;       // capture stream of the loop bodies
   Mg3Lev<double> l64[FEM_MAX_LEVELS];
   Mg3Lev<float> l32[FEM_MAX_LEVELS];
+  Mg3Lev<double, Mg2Geo> m64[FEM_MAX_LEVELS];
+  Mg3Lev<float, Mg2Geo> m32[FEM_MAX_LEVELS];
   Mg3GraphCache graphs[MG3_GRAPHS];
 };
 
 int mg3_setup(Mg3** out, int nex, int ney, int nez, double lx, double ly, double lz, int nlev,
               const uint8_t* level_pins, int sms, cudaStream_t s);
+// 2D hierarchy for the mixed-precision solve over the levels of a context's
+// 2D multigrid: grids, stencil tables, diagonals and gamma_p masks per level
+// (pins unused when mean_zero).
+int mg2_setup(Mg3** out, int nlev, const FemGrid* grids, const double* const* tabs, const double* const* diags,
+              const uint8_t* const* pins, int mean_zero, int sms, cudaStream_t s);
 void mg3_destroy(Mg3* M);
 int mg3_vcycle64(Mg3* M, const double* r, double* z, cudaStream_t s);
 int mg3_pcg(Mg3* M, const double* b, double* x, double tol, double atol, int maxiter,

@@ -20,9 +20,12 @@ __device__ __forceinline__ void bi_apply(const BiArgs& A, const MatCombo& op, in
 // comb of the staged sources (Ce never materialised).
 template <int KIND, int NC, bool OTF, int NSRC, class Team, class Load, class Comb, class Body>
 __device__ __forceinline__ void bi_tiled_apply(const Team& tm, const BiArgs& A, const MatCombo& op, double* tsm,
-                                               const Load& load, const double* const (&src)[NSRC],
-                                               const Comb& comb, const Body& body) {
-  if constexpr (OTF) {
+                                               const FemC3Tma& tma, const Load& load,
+                                               const double* const (&src)[NSRC], const Comb& comb,
+                                               const Body& body) {
+  if constexpr (OTF && KIND == FEM_HEX8) {
+    fem_tiled_conv3<NC, NSRC>(tm, A.g, tsm, tma, src, comb, A.cvf, A.qt, A.cv_coef, op.alpha, op.A, body);
+  } else if constexpr (OTF) {
     fem_tiled_conv<KIND, NC, NSRC>(tm, A.g, tsm, src, comb, A.cvf, A.qt, A.cv_coef, op.alpha, op.A, body);
   } else {
     fem_tiled_ebe<KIND, NC>(tm, A.g, tsm, load, op, body);
@@ -33,7 +36,15 @@ template <int KIND, int NC, bool OTF>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_constant__ BiArgs A) {
   __shared__ double smem[128];
   __shared__ double sAsh[81];
-  extern __shared__ double tsm[];  // staging of the tiled operator (dynamic)
+  extern __shared__ __align__(128) double tsm[];  // staging of the tiled operator (dynamic)
+  // hex8 on-the-fly convection: the mbarrier of its TMA factor copies
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ unsigned s_phase;
+  if (OTF && KIND == FEM_HEX8 && threadIdx.x == 0) {
+    fem_mbar_init(&s_bar, 1);
+    s_phase = 0u;
+  }
+  const FemC3Tma tma{&s_bar, &s_phase, A.sync.err};
   MatCombo op = A.op;
   if (op.A) {
     for (int t = threadIdx.x; t < KI<KIND>::NEN * KI<KIND>::NEN; t += blockDim.x) sAsh[t] = op.A[t];
@@ -54,7 +65,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_consta
     {
       double a[2] = {0.0, 0.0};
       const double* sx0[1] = {A.x};
-      bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, [&](int j, int c) { return A.x[j + c * N]; }, sx0,
+      bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, tma, [&](int j, int c) { return A.x[j + c * N]; }, sx0,
                                     [](int, const double(&v)[1]) { return v[0]; },
                               [&](int i, const double(&Ax)[NC], const double(&xc)[NC]) {
 #pragma unroll
@@ -97,7 +108,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_consta
         };
         double a[1] = {0.0};
         const double* spn[3] = {r, pold, qold};
-        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, pn, spn,
+        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, tma, pn, spn,
                                       [&](int, const double(&v)[3]) { return v[0] + beta * (v[1] - omega * v[2]); },
                                       [&](int i, const double(&qv)[NC], const double(&pc)[NC]) {
 #pragma unroll
@@ -122,7 +133,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_bicgstab(const __grid_consta
       {
         double a[3] = {0.0, 0.0, 0.0};
         const double* ssv[2] = {r, qnew};
-        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, sv, ssv,
+        bi_tiled_apply<KIND, NC, OTF>(gt, A, op, tsm, tma, sv, ssv,
                                       [&](int, const double(&v)[2]) { return v[0] - alpha_ * v[1]; }, [&](int i, const double(&tvv)[NC], const double(&sc)[NC]) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
@@ -194,6 +205,7 @@ done:
 
 
 static const void* bi_fn(int kind, int ncomp, bool otf) {
+  if (otf && kind == FEM_HEX8) return (const void*)k_bicgstab<FEM_HEX8, 3, true>;
   if (otf) return kind == FEM_Q1_2D ? (const void*)k_bicgstab<FEM_Q1_2D, 2, true>
                                     : (const void*)k_bicgstab<FEM_Q2_2D, 2, true>;
   if (kind == FEM_Q1_2D)
@@ -205,6 +217,7 @@ static const void* bi_fn(int kind, int ncomp, bool otf) {
 // dynamic smem (doubles) of the tiled operator: the EBE gather of fem_tiled_ebe
 // needs NC (32+2R)(16+2R)(3 in 3D); the on-the-fly convection fem_conv_smem
 static int bi_smem_doubles(int kind, int ncomp, bool otf) {
+  if (otf && kind == FEM_HEX8) return FEM_C3_SMEM_MAX;
   if (otf) return FEM_CONV_SMEM;
   return 3 * 1836;
 }
@@ -213,7 +226,7 @@ int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s) {
   BiArgs a = A;
   void* args[] = {&a};
   const bool otf = A.cvf != nullptr;
-  if (otf && (A.g.kind == FEM_HEX8 || ncomp != 2)) return FEM_E_ARG;
+  if (otf && ncomp != (A.g.kind == FEM_HEX8 ? 3 : 2)) return FEM_E_ARG;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(FEM_THREADS);
@@ -232,8 +245,7 @@ int fem_coop_occupancy_bi(int* occ) {
   for (int kind = 0; kind < 3; ++kind)
     for (int v = 0; v < 3; ++v) {
       const bool otf = (v == 2);
-      if (otf && kind == FEM_HEX8) continue;
-      const int nc = otf ? 2 : v + 1;
+      const int nc = otf ? (kind == FEM_HEX8 ? 3 : 2) : v + 1;
       const void* fn = bi_fn(kind, nc, otf);
       const int dyn = bi_smem_doubles(kind, nc, otf) * (int)sizeof(double);
       if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) return -1;

@@ -105,6 +105,19 @@ __device__ __forceinline__ void mg3_sweep(const Mg3Geo& G, const Src& src, const
   }
 }
 
+// 2D lattice levels: one thread per node, the level's assembled stencil table
+// (fem_stencil_apply, sums in FP64).
+template <class Src, class Epi>
+__device__ __forceinline__ void mg3_sweep(const Mg2Geo& G, const Src& src, const Epi& epi) {
+  const FemGrid& g = G.g;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.nn; i += gridDim.x * blockDim.x) {
+    const int ix = i % g.nnx, iy = i / g.nnx;
+    const double y = g.kind == FEM_Q1_2D ? fem_stencil_apply<FEM_Q1_2D>(g, G.tab, ix, iy, 0, src)
+                                         : fem_stencil_apply<FEM_Q2_2D>(g, G.tab, ix, iy, 0, src);
+    epi(i, y);
+  }
+}
+
 // Block sums of NV doubles (fixed shuffle tree, warps in order); thread 0 writes
 // part[k][blockIdx.x], part[k] = parts + k * MG3_PARTS. Every thread must call it.
 template <int NV>
@@ -157,8 +170,8 @@ __device__ __forceinline__ double ld(const T* p, int i) {
 
 // Chebyshev steps 1 and 2 from x = 0 (pre-smoothing): x1 = b1 D^-1 r is formed
 // on the fly at the neighbours, d2 = a2 x1 + b2 D^-1 (r - A x1), x2 = x1 + d2.
-template <class T>
-__global__ void __launch_bounds__(MG3_THREADS) k_mg3_first(Mg3Lev<T> L, double b1, double a2, double b2) {
+template <class T, class G>
+__global__ void __launch_bounds__(MG3_THREADS) k_mg3_first(Mg3Lev<T, G> L, double b1, double a2, double b2) {
   mg3_sweep(L.geo, [&](int j) { return b1 * ld(L.invD, j) * ld(L.r, j); }, [&](int i, double ax) {
     const double iD = ld(L.invD, i), x1 = b1 * iD * ld(L.r, i);
     const double d = a2 * x1 + b2 * iD * (ld(L.r, i) - ax);
@@ -168,25 +181,32 @@ __global__ void __launch_bounds__(MG3_THREADS) k_mg3_first(Mg3Lev<T> L, double b
 }
 
 // One Chebyshev step d = a d + b D^-1 (r - A x_in), x_out = x_in + d (FIRST: a d
-// is absent, d is not read). DOT adds the block partials of r . x_out.
-template <class T, bool FIRST, bool DOT>
+// is absent, d is not read). NDOT = 1 adds the block partials of r . x_out;
+// NDOT = 3 also those of sum x_out and sum r (mean-zero problems).
+template <class T, class G, bool FIRST, int NDOT>
 __global__ void __launch_bounds__(MG3_THREADS)
-    k_mg3_step(Mg3Lev<T> L, const T* __restrict__ xin, T* __restrict__ xout, double a, double b, double* parts) {
-  double acc[1] = {0.0};
+    k_mg3_step(Mg3Lev<T, G> L, const T* __restrict__ xin, T* __restrict__ xout, double a, double b, double* parts) {
+  double acc[NDOT > 0 ? NDOT : 1];
+#pragma unroll
+  for (int k = 0; k < (NDOT > 0 ? NDOT : 1); ++k) acc[k] = 0.0;
   mg3_sweep(L.geo, [&](int j) { return ld(xin, j); }, [&](int i, double ax) {
     const double res = ld(L.r, i) - ax;
     const double d = (FIRST ? 0.0 : a * ld(L.d, i)) + b * ld(L.invD, i) * res;
     const double x = ld(xin, i) + d;
     L.d[i] = (T)d;
     xout[i] = (T)x;
-    if (DOT) acc[0] += ld(L.r, i) * (double)(T)x;
+    if (NDOT > 0) acc[0] += ld(L.r, i) * (double)(T)x;
+    if (NDOT > 1) {
+      acc[1] += (double)(T)x;
+      acc[2] += ld(L.r, i);
+    }
   });
-  if (DOT) mg3_block_parts<1>(acc, parts);
+  if constexpr (NDOT > 0) mg3_block_parts<NDOT>(acc, parts);
 }
 
 // t = r - A x, zero on gamma_p (D^-1 = 0 marks a gamma_p node)
-template <class T>
-__global__ void __launch_bounds__(MG3_THREADS) k_mg3_resid(Mg3Lev<T> L, const T* __restrict__ x) {
+template <class T, class G>
+__global__ void __launch_bounds__(MG3_THREADS) k_mg3_resid(Mg3Lev<T, G> L, const T* __restrict__ x) {
   mg3_sweep(L.geo, [&](int j) { return ld(x, j); }, [&](int i, double ax) {
     L.t[i] = L.invD[i] == (T)0 ? (T)0 : (T)(ld(L.r, i) - ax);
   });
@@ -194,7 +214,7 @@ __global__ void __launch_bounds__(MG3_THREADS) k_mg3_resid(Mg3Lev<T> L, const T*
 
 // r_C = R t_F with R = P^T of the trilinear prolongation (weights 1, 1/2 per axis)
 template <class T>
-__global__ void k_mg3_restrict(Mg3Lev<T> F, Mg3Lev<T> C) {
+__global__ void k_mg3_restrict(Mg3Lev<T, Mg3Geo> F, Mg3Lev<T, Mg3Geo> C) {
   const int NX = C.geo.nx, NY = C.geo.ny, NZ = C.geo.nz, nx = F.geo.nx, ny = F.geo.ny, nz = F.geo.nz;
   const int n = NX * NY * NZ;
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
@@ -222,8 +242,8 @@ __global__ void k_mg3_restrict(Mg3Lev<T> F, Mg3Lev<T> C) {
 
 // x_out = x_pre + P x_C, zero on gamma_p
 template <class T>
-__global__ void k_mg3_prolong(Mg3Lev<T> F, Mg3Lev<T> C, const T* __restrict__ xpre, const T* __restrict__ xc,
-                              T* __restrict__ xout) {
+__global__ void k_mg3_prolong(Mg3Lev<T, Mg3Geo> F, Mg3Lev<T, Mg3Geo> C, const T* __restrict__ xpre,
+                              const T* __restrict__ xc, T* __restrict__ xout) {
   const int NX = C.geo.nx, NY = C.geo.ny, nx = F.geo.nx, ny = F.geo.ny;
   const int n = F.geo.nx * F.geo.ny * F.geo.nz;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -252,12 +272,57 @@ __global__ void k_mg3_prolong(Mg3Lev<T> F, Mg3Lev<T> C, const T* __restrict__ xp
   }
 }
 
-// Coarsest level: x = Ainv r' in FP64 (r' = r with gamma_p zeroed), one warp per row
+// 2D levels: r_C = P^T t_F on the unique-node lattices (weights 1, 1/2 per
+// axis; periodic neighbours wrap), the transpose of fem_interp_at
 template <class T>
-__global__ void k_mg3_coarse(Mg3Lev<T> C, const double* __restrict__ Ainv, T* __restrict__ xout) {
+__global__ void k_mg2_restrict(Mg3Lev<T, Mg2Geo> F, Mg3Lev<T, Mg2Geo> C) {
+  const FemLattice &h = F.geo.lat, &H = C.geo.lat;
+  const int ux = h.ux(), uy = h.uy(), Ux = H.ux(), n = C.geo.g.nn;
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
+    const int R = I / Ux, Cc = I % Ux;
+    double acc = 0.0;
+    for (int dr = -1; dr <= 1; ++dr) {
+      int r = 2 * R + dr;
+      if (h.periodic) {
+        r = r < 0 ? r + uy : (r >= uy ? r - uy : r);
+      } else if (r < 0 || r >= uy) {
+        continue;
+      }
+      const double wr = dr ? 0.5 : 1.0;
+      for (int dc = -1; dc <= 1; ++dc) {
+        int c = 2 * Cc + dc;
+        if (h.periodic) {
+          c = c < 0 ? c + ux : (c >= ux ? c - ux : c);
+        } else if (c < 0 || c >= ux) {
+          continue;
+        }
+        acc += wr * (dc ? 0.5 : 1.0) * (double)F.t[r * ux + c];
+      }
+    }
+    C.r[I] = (T)acc;
+  }
+}
+// x_out = x_pre + P x_C (lattice-bilinear, fem_interp_at), zero on gamma_p
+template <class T>
+__global__ void k_mg2_prolong(Mg3Lev<T, Mg2Geo> F, Mg3Lev<T, Mg2Geo> C, const T* __restrict__ xpre,
+                              const T* __restrict__ xc, T* __restrict__ xout, int mean_zero) {
+  const int ux = F.geo.lat.ux(), n = F.geo.g.nn;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!mean_zero && F.invD[i] == (T)0) {
+      xout[i] = (T)0;
+      continue;
+    }
+    xout[i] = (T)(ld(xpre, i) + fem_interp_at(C.geo.lat, i / ux, i % ux, [&](int J) { return (double)xc[J]; }));
+  }
+}
+
+// Coarsest level: x = Ainv r' in FP64 (r' = r with gamma_p zeroed), one warp per row
+template <class T, class G>
+__global__ void k_mg3_coarse(Mg3Lev<T, G> C, int n, int mean_zero, const double* __restrict__ Ainv,
+                             T* __restrict__ xout) {
   __shared__ double rs[MG3_COARSE_MAX];
-  const int n = C.geo.nx * C.geo.ny * C.geo.nz;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) rs[j] = C.invD[j] == (T)0 ? 0.0 : (double)C.r[j];
+  for (int j = threadIdx.x; j < n; j += blockDim.x)
+    rs[j] = (!mean_zero && C.invD[j] == (T)0) ? 0.0 : (double)C.r[j];
   __syncthreads();
   const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
@@ -266,22 +331,25 @@ __global__ void k_mg3_coarse(Mg3Lev<T> C, const double* __restrict__ Ainv, T* __
     for (int j = lane; j < n; j += 32) s += row[j] * rs[j];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) xout[i] = C.invD[i] == (T)0 ? (T)0 : (T)s;
+    if (lane == 0) xout[i] = (!mean_zero && C.invD[i] == (T)0) ? (T)0 : (T)s;
   }
 }
 
 // --------------------------------------------------------------- CG pieces ----
 
 // p = z + beta p_old (beta = sc->beta), Ap (zero on gamma_p), block partials of p . Ap
-template <class T>
+// (mean-zero problems: z is taken minus its mean sc->zbar, the projection of
+// the preconditioned residual onto the mean-zero subspace)
+template <class T, class G>
 __global__ void __launch_bounds__(MG3_THREADS)
-    k_mg3_ap(Mg3Lev<T> L, const T* __restrict__ z, const T* __restrict__ pold, T* __restrict__ pnew,
-             T* __restrict__ Ap, const Mg3Scal* sc, int inner, double* parts) {
+    k_mg3_ap(Mg3Lev<T, G> L, const T* __restrict__ z, const T* __restrict__ pold, T* __restrict__ pnew,
+             T* __restrict__ Ap, const Mg3Scal* sc, int inner, int mean_zero, double* parts) {
   const double beta = inner ? sc->beta_i : sc->beta;
+  const double zb = mean_zero ? sc->zbar : 0.0;
   double acc[1] = {0.0};
-  mg3_sweep(L.geo, [&](int j) { return (double)(T)(ld(z, j) + beta * ld(pold, j)); }, [&](int i, double ax) {
-    const T p = (T)(ld(z, i) + beta * ld(pold, i));
-    const T q = L.invD[i] == (T)0 ? (T)0 : (T)ax;
+  mg3_sweep(L.geo, [&](int j) { return (double)(T)((ld(z, j) - zb) + beta * ld(pold, j)); }, [&](int i, double ax) {
+    const T p = (T)((ld(z, i) - zb) + beta * ld(pold, i));
+    const T q = (!mean_zero && L.invD[i] == (T)0) ? (T)0 : (T)ax;
     pnew[i] = p;
     Ap[i] = q;
     acc[0] += (double)p * (double)q;
@@ -310,13 +378,13 @@ __global__ void k_mg3_xr(int n, T* __restrict__ x, T* __restrict__ r, const T* _
 
 // FP64 residual r = b - A x (gamma_p rows of A x zeroed) stored as T, with the
 // block partials of r . r and b . b
-template <class T>
+template <class T, class G>
 __global__ void __launch_bounds__(MG3_THREADS)
-    k_mg3_res64(Mg3Lev<T> L, Mg3Geo G, const uint8_t* __restrict__ pin, const double* __restrict__ b,
-                const double* __restrict__ x, T* __restrict__ r, double* parts) {
+    k_mg3_res64(G geo, const uint8_t* __restrict__ pin, const double* __restrict__ b, const double* __restrict__ x,
+                T* __restrict__ r, double* parts) {
   double acc[2] = {0.0, 0.0};
-  mg3_sweep(G, [&](int j) { return x[j]; }, [&](int i, double ax) {
-    const double ri = b[i] - (pin[i] ? 0.0 : ax);
+  mg3_sweep(geo, [&](int j) { return x[j]; }, [&](int i, double ax) {
+    const double ri = b[i] - ((pin && pin[i]) ? 0.0 : ax);
     r[i] = (T)ri;
     acc[0] += ri * ri;
     acc[1] += b[i] * b[i];
@@ -331,6 +399,18 @@ __global__ void k_mg3_add(int n, double* __restrict__ x, const T* __restrict__ d
     const double v = x[i] + (d ? (double)d[i] : 0.0);
     x[i] = (pin && pin[i]) ? 0.0 : v;
   }
+}
+
+// partials of sum x (FP64), and x -= mean(x) from them (every block sums them
+// in the same order)
+__global__ void k_mg3_sum(int n, const double* __restrict__ x, double* parts) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] += x[i];
+  mg3_block_parts<1>(acc, parts);
+}
+__global__ void k_mg3_center(int n, double* __restrict__ x, const double* __restrict__ parts, int np) {
+  const double m = mg3_sum_parts(parts, np) / n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] -= m;
 }
 
 __device__ __forceinline__ unsigned long long mg3_now() {
@@ -348,9 +428,18 @@ __device__ __forceinline__ unsigned long long mg3_now() {
 // The condition (WHILE node) is set in the modes that carry it; it is false
 // once the cap, the tolerance, a non-finite value or the wall budget stops
 // the loop, and the reason goes to sc->status.
+// inv_n > 0 (mean-zero problems): prz + MG3_PARTS and + 2 MG3_PARTS hold the
+// partials of sum z and sum r; z is projected to mean zero (zbar = sum z / n)
+// and gamma = r . (z - zbar).
 __global__ void k_mg3_ctl(Mg3Scal* sc, int mode, const double* __restrict__ prz, int nrz,
-                          const double* __restrict__ prr, int nrr, cudaGraphConditionalHandle h) {
-  const double rz = prz ? mg3_sum_parts(prz, nrz) : 0.0;
+                          const double* __restrict__ prr, int nrr, double inv_n, cudaGraphConditionalHandle h) {
+  double rz = prz ? mg3_sum_parts(prz, nrz) : 0.0;
+  if (prz && inv_n > 0.0) {
+    const double sz = mg3_sum_parts(prz + MG3_PARTS, nrz), sr = mg3_sum_parts(prz + 2 * MG3_PARTS, nrz);
+    const double zb = sz * inv_n;
+    rz -= zb * sr;
+    if (threadIdx.x == 0) sc->zbar = zb;
+  }
   const double rr = prr ? mg3_sum_parts(prr, nrr) : 0.0;
   const double bb = (mode == MG3_CTL_PCG0 || mode == MG3_CTL_MX0) ? mg3_sum_parts(prr + MG3_PARTS, nrr) : 0.0;
   if (threadIdx.x != 0) return;
@@ -451,11 +540,12 @@ __global__ void k_mg3_pw_init(int n, const double* __restrict__ invD, double* __
     v[i] = invD[i] == 0.0 ? 0.0 : (double)((unsigned)i * 2654435761u) / 4294967296.0 - 0.5;
 }
 // w = D^-1 A v, partials of w . w and v . v
+template <class G>
 __global__ void __launch_bounds__(MG3_THREADS)
-    k_mg3_pw(Mg3Geo G, const double* __restrict__ invD, const double* __restrict__ v, double* __restrict__ w,
+    k_mg3_pw(G geo, const double* __restrict__ invD, const double* __restrict__ v, double* __restrict__ w,
              double* parts) {
   double acc[2] = {0.0, 0.0};
-  mg3_sweep(G, [&](int j) { return v[j]; }, [&](int i, double ax) {
+  mg3_sweep(geo, [&](int j) { return v[j]; }, [&](int i, double ax) {
     const double wi = invD[i] * ax;
     w[i] = wi;
     acc[0] += wi * wi;
@@ -500,6 +590,55 @@ __global__ void k_mg3_dense(Mg3Geo G, const uint8_t* __restrict__ pin, double* _
     A[t] = v;
   }
 }
+// 2D levels: 1/diag(A), 0 on gamma_p (pinned problems)
+__global__ void k_mg2_invdiag(int n, const double* __restrict__ diag, const uint8_t* __restrict__ pin,
+                              double* __restrict__ invD64, float* __restrict__ invD32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = (pin && pin[i]) ? 0.0 : 1.0 / diag[i];
+    invD64[i] = v;
+    invD32[i] = (float)v;
+  }
+}
+// dense coarse matrix of a 2D level from its stencil table: row i gets the
+// coefficient of every offset at the neighbour it names (one thread per row,
+// so coinciding neighbours of a tiny periodic lattice add up as in the
+// stencil apply); the matrix is zeroed before. Then either the gamma_p rows
+// and columns become the identity, or (mean-zero) c 1 1^T is added, which makes
+// it SPD and leaves A^-1 r mean-zero and exact for every mean-zero r.
+template <int KIND>
+__global__ void k_mg2_dense_rows(FemGrid g, const double* __restrict__ tab, double* __restrict__ A) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  const int n = g.nn, nc = fem_axis_ncls(KIND, g.periodic);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int ix = i % g.nnx, iy = i / g.nnx;
+    const double* c = tab + (size_t)(fem_axis_cls(KIND, g.periodic, iy, g.ney) * nc +
+                                     fem_axis_cls(KIND, g.periodic, ix, g.nex)) * NOFF;
+    for (int dy = 0; dy < W; ++dy)
+      for (int dx = 0; dx < W; ++dx) {
+        int v = ix + dx - R, w = iy + dy - R;
+        if (g.periodic) {
+          v = fem_wrap(v, g.nnx);
+          w = fem_wrap(w, g.nny);
+        } else {
+          v = v < 0 ? 0 : (v >= g.nnx ? g.nnx - 1 : v);
+          w = w < 0 ? 0 : (w >= g.nny ? g.nny - 1 : w);
+        }
+        A[(size_t)i * n + w * g.nnx + v] += c[dy * W + dx];
+      }
+  }
+}
+__global__ void k_mg2_dense_fix(int n, const uint8_t* __restrict__ pin, int mean_zero, double shift,
+                                double* __restrict__ A) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / n), j = (int)(t % n);
+    if (mean_zero)
+      A[t] += shift;
+    else if ((pin && pin[i]) || (pin && pin[j]))
+      A[t] = (i == j) ? 1.0 : 0.0;
+  }
+}
+
 // Gauss-Jordan step k of the in-place inversion (no pivoting: A is SPD)
 __global__ void k_mg3_gj_pivot(int n, int k, const double* __restrict__ A, double* __restrict__ rowk,
                                double* __restrict__ colk) {
@@ -523,16 +662,17 @@ __global__ void k_mg3_gj_update(int n, int k, double* __restrict__ A, const doub
 
 // -------------------------------------------------------------------- host ----
 
-#define MG3_TRY(x)        \
-  do {                    \
-    int _r = (x);         \
-    if (_r) return _r;    \
+#define MG3_TRY(...)          \
+  do {                        \
+    int _r = (__VA_ARGS__);   \
+    if (_r) return _r;        \
   } while (0)
 #define MG3_CUDA(call)                                              \
   do {                                                              \
     cudaError_t _e = (call);                                        \
     if (_e != cudaSuccess) return fem_cuda_error(#call, _e);        \
   } while (0)
+#define MG3_NSLOTS 6
 
 static int mg3_blocks_elem(long long n, int cap) { return fem_nblocks(n, MG3_THREADS, cap); }
 static int mg3_items(const Mg3Geo& G) {
@@ -542,6 +682,9 @@ static int mg3_blocks_sweep(const Mg3Geo& G, int cap) {
   const int warps = mg3_items(G), b = (warps + (MG3_THREADS / 32) - 1) / (MG3_THREADS / 32);
   return b < 1 ? 1 : (b > cap ? cap : b);
 }
+static int mg3_blocks_sweep(const Mg2Geo& G, int cap) { return mg3_blocks_elem(G.g.nn, cap); }
+static int mg3_nn(const Mg3Geo& G) { return G.nx * G.ny * G.nz; }
+static int mg3_nn(const Mg2Geo& G) { return G.g.nn; }
 
 // 1D assembled rows of one axis: K = (1/h)[-1 2 -1], M = (h/6)[1 4 1] inside,
 // the one-element halves at the first and last node.
@@ -568,10 +711,10 @@ static Mg3Geo mg3_geo(int nex, int ney, int nez, double lx, double ly, double lz
   return G;
 }
 
-template <class T>
-static void mg3_bind(Mg3Lev<T>& L, const Mg3Geo& G, T* base, const T* invD) {
-  const size_t n = (size_t)G.nx * G.ny * G.nz;
-  L.geo = G;
+template <class T, class G>
+static void mg3_bind(Mg3Lev<T, G>& L, const G& geo, T* base, const T* invD) {
+  const size_t n = (size_t)mg3_nn(geo);
+  L.geo = geo;
   L.invD = invD;
   L.r = base;
   L.t = base + n;
@@ -601,91 +744,46 @@ static int dalloc_t(T** p, size_t n) {
   return FEM_OK;
 }
 
-int mg3_setup(Mg3** out, int nex, int ney, int nez, double lx, double ly, double lz, int nlev,
-              const uint8_t* level_pins, int sms, cudaStream_t s) {
-  *out = nullptr;
-  if (nlev < 2 || nlev > FEM_MAX_LEVELS) return FEM_E_ARG;
-  const int f = 1 << (nlev - 1);
-  if (nex % f || ney % f || nez % f) return FEM_E_ARG;
-  Mg3* M = new Mg3();
-  M->nlev = nlev;
-  M->sms = sms;
-  M->cap = sms * 8;
-  const int cap_warps = sms * 32;
-  size_t tot = 0, maxn = 0;
-  for (int l = 0; l < nlev; ++l) {
-    M->geo[l] = mg3_geo(nex >> l, ney >> l, nez >> l, lx, ly, lz, cap_warps);
-    const size_t n = (size_t)M->geo[l].nx * M->geo[l].ny * M->geo[l].nz;
-    M->off[l] = tot;
-    M->nn[l] = (int)n;
-    tot += n;
-    if (n > maxn) maxn = n;
-  }
-  M->total = tot;
-  const int nc = M->nn[nlev - 1];
-  if (nc > MG3_COARSE_MAX) {
-    snprintf(fem_err_buf(), 256, "hex8 multigrid: coarsest level of %d nodes exceeds %d (add levels)", nc,
-             MG3_COARSE_MAX);
-    mg3_destroy(M);
-    return FEM_E_ARG;
-  }
+// Buffers of a hierarchy whose level sizes (M->nn, M->off, M->total) are set.
+static int mg3_alloc(Mg3* M) {
+  const size_t tot = M->total, n0 = M->nn[0], nc = M->nn[M->nlev - 1];
   int rc = FEM_OK;
   rc = rc ? rc : dalloc_t(&M->pin, tot);
   rc = rc ? rc : dalloc_t(&M->invD64, tot);
   rc = rc ? rc : dalloc_t(&M->invD32, tot);
   rc = rc ? rc : dalloc_t(&M->work64, 5 * tot);
   rc = rc ? rc : dalloc_t(&M->work32, 5 * tot);
-  const size_t n0 = M->nn[0];
   rc = rc ? rc : dalloc_t(&M->v64, 4 * n0);  // p_old, p_new, Ap, spare (FP64 PCG)
   rc = rc ? rc : dalloc_t(&M->v32, 4 * n0);  // p_old, p_new, Ap, d (FP32 inner)
   rc = rc ? rc : dalloc_t(&M->x64, n0);
   rc = rc ? rc : dalloc_t(&M->b64, n0);
-  rc = rc ? rc : dalloc_t(&M->Ainv, (size_t)nc * nc);
-  rc = rc ? rc : dalloc_t(&M->parts, 4 * (size_t)MG3_PARTS);
+  rc = rc ? rc : dalloc_t(&M->Ainv, nc * nc);
+  rc = rc ? rc : dalloc_t(&M->parts, MG3_NSLOTS * (size_t)MG3_PARTS);
   rc = rc ? rc : dalloc_t(&M->sc, 1);
-  rc = rc ? rc : dalloc_t(&M->gj, 2 * (size_t)nc + 2);
+  rc = rc ? rc : dalloc_t(&M->gj, 2 * nc + 2);
   if (rc == FEM_OK && cudaStreamCreateWithFlags(&M->s2, cudaStreamNonBlocking) != cudaSuccess)
     rc = fem_cuda_error("cudaStreamCreateWithFlags", cudaGetLastError());
-  if (rc) {
-    mg3_destroy(M);
-    return rc;
-  }
-  for (int l = 0; l < nlev; ++l) {
-    const size_t o = M->off[l];
-    if (level_pins) {
-      if (cudaMemcpyAsync(M->pin + o, level_pins + o, M->nn[l], cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-        rc = fem_cuda_error("cudaMemcpyAsync", cudaGetLastError());
-    } else {
-      if (cudaMemsetAsync(M->pin + o, 0, M->nn[l], s) != cudaSuccess ||
-          cudaMemsetAsync(M->pin + o, 1, 1, s) != cudaSuccess)
-        rc = fem_cuda_error("cudaMemsetAsync", cudaGetLastError());
-    }
-    if (rc) break;
-    k_mg3_invdiag<<<mg3_blocks_elem(M->nn[l], M->cap), MG3_THREADS, 0, s>>>(M->geo[l], M->pin + o, M->invD64 + o,
-                                                                            M->invD32 + o);
-    if ((rc = fem_after_launch("k_mg3_invdiag"))) break;
-    mg3_bind(M->l64[l], M->geo[l], M->work64 + 5 * o, M->invD64 + o);
-    mg3_bind(M->l32[l], M->geo[l], M->work32 + 5 * o, M->invD32 + o);
-  }
-  // largest eigenvalue of D^-1 A per smoothed level (power iteration, FP64)
+  return rc;
+}
+
+// lambda_max of D^-1 A per smoothed level (power iteration, FP64) and the
+// Chebyshev coefficients over [lo, hi] lambda (Saad, Algorithm 12.1)
+template <class G>
+static int mg3_chebyshev(Mg3* M, const G* geo, cudaStream_t s) {
   double hs[2] = {0.0, 0.0};
-  for (int l = 0; l < nlev - 1 && rc == FEM_OK; ++l) {
-    const int n = M->nn[l], gb = mg3_blocks_sweep(M->geo[l], M->cap), ge = mg3_blocks_elem(n, M->cap);
+  for (int l = 0; l < M->nlev - 1; ++l) {
+    const int n = M->nn[l], gb = mg3_blocks_sweep(geo[l], M->cap), ge = mg3_blocks_elem(n, M->cap);
     double *v = M->work64 + 5 * M->off[l], *w = v + n;  // the level's r and t serve as scratch
     k_mg3_pw_init<<<ge, MG3_THREADS, 0, s>>>(n, M->invD64 + M->off[l], v);
     for (int it = 0; it < MG3_POWER_ITERS; ++it) {
-      k_mg3_pw<<<gb, MG3_THREADS, 0, s>>>(M->geo[l], M->invD64 + M->off[l], v, w, M->parts);
+      k_mg3_pw<G><<<gb, MG3_THREADS, 0, s>>>(geo[l], M->invD64 + M->off[l], v, w, M->parts);
       k_mg3_pw_scale<<<ge, MG3_THREADS, 0, s>>>(n, w, v, M->parts, gb, M->gj);
     }
-    if ((rc = fem_after_launch("k_mg3_pw"))) break;
-    if (cudaMemcpyAsync(hs, M->gj, 2 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-      rc = fem_cuda_error("power iteration", cudaGetLastError());
-      break;
-    }
+    MG3_TRY(fem_after_launch("k_mg3_pw"));
+    MG3_CUDA(cudaMemcpyAsync(hs, M->gj, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MG3_CUDA(cudaStreamSynchronize(s));
     const double lam = std::sqrt(hs[0]) / std::sqrt(hs[1]);
     M->lam[l] = lam;
-    // Chebyshev coefficients over [lo, hi] lambda (Saad, Algorithm 12.1)
     const double lo = MG3_CHEB_LO * lam, hi = MG3_CHEB_HI * lam;
     const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
     double rho_old = 1.0 / sigma;
@@ -698,21 +796,76 @@ int mg3_setup(Mg3** out, int nex, int ney, int nez, double lx, double ly, double
       rho_old = rho;
     }
   }
+  return FEM_OK;
+}
+
+// In-place Gauss-Jordan inversion of the n x n coarse matrix in M->Ainv
+static int mg3_invert(Mg3* M, int n, cudaStream_t s) {
+  const long long nn2 = (long long)n * n;
+  const int gb = (int)std::min<long long>((nn2 + 255) / 256, (long long)M->cap * 4);
+  for (int k = 0; k < n; ++k) {
+    k_mg3_gj_pivot<<<1, 1024, 0, s>>>(n, k, M->Ainv, M->gj, M->gj + n);
+    k_mg3_gj_update<<<gb, 256, 0, s>>>(n, k, M->Ainv, M->gj, M->gj + n);
+    if ((k & 255) == 255 || k == n - 1) MG3_TRY(fem_after_launch("k_mg3_gj"));
+  }
+  MG3_CUDA(cudaStreamSynchronize(s));
+  return FEM_OK;
+}
+
+int mg3_setup(Mg3** out, int nex, int ney, int nez, double lx, double ly, double lz, int nlev,
+              const uint8_t* level_pins, int sms, cudaStream_t s) {
+  *out = nullptr;
+  if (nlev < 2 || nlev > FEM_MAX_LEVELS) return FEM_E_ARG;
+  const int f = 1 << (nlev - 1);
+  if (nex % f || ney % f || nez % f) return FEM_E_ARG;
+  Mg3* M = new Mg3();
+  M->nlev = nlev;
+  M->sms = sms;
+  M->cap = sms * 8;
+  const int cap_warps = sms * 32;
+  size_t tot = 0;
+  for (int l = 0; l < nlev; ++l) {
+    M->geo[l] = mg3_geo(nex >> l, ney >> l, nez >> l, lx, ly, lz, cap_warps);
+    const size_t n = (size_t)mg3_nn(M->geo[l]);
+    M->off[l] = tot;
+    M->nn[l] = (int)n;
+    tot += n;
+  }
+  M->total = tot;
+  const int nc = M->nn[nlev - 1];
+  if (nc > MG3_COARSE_MAX) {
+    snprintf(fem_err_buf(), 256, "hex8 multigrid: coarsest level of %d nodes exceeds %d (add levels)", nc,
+             MG3_COARSE_MAX);
+    mg3_destroy(M);
+    return FEM_E_ARG;
+  }
+  int rc = mg3_alloc(M);
+  for (int l = 0; l < nlev && rc == FEM_OK; ++l) {
+    const size_t o = M->off[l];
+    if (level_pins) {
+      if (cudaMemcpyAsync(M->pin + o, level_pins + o, M->nn[l], cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        rc = fem_cuda_error("cudaMemcpyAsync", cudaGetLastError());
+    } else {
+      if (cudaMemsetAsync(M->pin + o, 0, M->nn[l], s) != cudaSuccess ||
+          cudaMemsetAsync(M->pin + o, 1, 1, s) != cudaSuccess)
+        rc = fem_cuda_error("cudaMemsetAsync", cudaGetLastError());
+    }
+    if (rc) break;
+    k_mg3_invdiag<<<mg3_blocks_elem(M->nn[l], M->cap), MG3_THREADS, 0, s>>>(M->geo[l], M->pin + o, M->invD64 + o,
+                                                                            M->invD32 + o);
+    rc = fem_after_launch("k_mg3_invdiag");
+    mg3_bind(M->l64[l], M->geo[l], M->work64 + 5 * o, (const double*)(M->invD64 + o));
+    mg3_bind(M->l32[l], M->geo[l], M->work32 + 5 * o, (const float*)(M->invD32 + o));
+  }
+  if (rc == FEM_OK) rc = mg3_chebyshev(M, M->geo, s);
   // coarsest level: its dense inverse, in place
   if (rc == FEM_OK) {
-    const Mg3Geo& G = M->geo[nlev - 1];
     const long long nn2 = (long long)nc * nc;
     const int gb = (int)std::min<long long>((nn2 + 255) / 256, (long long)M->cap * 4);
-    k_mg3_dense<<<gb, 256, 0, s>>>(G, M->pin + M->off[nlev - 1], M->Ainv);
+    k_mg3_dense<<<gb, 256, 0, s>>>(M->geo[nlev - 1], M->pin + M->off[nlev - 1], M->Ainv);
     rc = fem_after_launch("k_mg3_dense");
-    for (int k = 0; k < nc && rc == FEM_OK; ++k) {
-      k_mg3_gj_pivot<<<1, 1024, 0, s>>>(nc, k, M->Ainv, M->gj, M->gj + nc);
-      k_mg3_gj_update<<<gb, 256, 0, s>>>(nc, k, M->Ainv, M->gj, M->gj + nc);
-      if (((k & 255) == 255 || k == nc - 1) && (rc = fem_after_launch("k_mg3_gj"))) break;
-    }
-    if (rc == FEM_OK && cudaStreamSynchronize(s) != cudaSuccess)
-      rc = fem_cuda_error("coarse inverse", cudaGetLastError());
   }
+  if (rc == FEM_OK) rc = mg3_invert(M, nc, s);
   if (rc) {
     mg3_destroy(M);
     return rc;
@@ -721,40 +874,143 @@ int mg3_setup(Mg3** out, int nex, int ney, int nez, double lx, double ly, double
   return FEM_OK;
 }
 
-// V-cycle on the level vectors of precision T: input lv[0].r, output lv[0].xb.
-// dot: block partials of r . z into parts (for the CG), written by the last step.
+int mg2_setup(Mg3** out, int nlev, const FemGrid* grids, const double* const* tabs, const double* const* diags,
+              const uint8_t* const* pins, int mean_zero, int sms, cudaStream_t s) {
+  *out = nullptr;
+  if (nlev < 2 || nlev > FEM_MAX_LEVELS) return FEM_E_ARG;
+  Mg3* M = new Mg3();
+  M->nlev = nlev;
+  M->sms = sms;
+  M->cap = sms * 8;
+  M->d2 = 1;
+  M->mz = mean_zero ? 1 : 0;
+  size_t tot = 0;
+  for (int l = 0; l < nlev; ++l) {
+    const FemGrid& g = grids[l];
+    Mg2Geo& G = M->geo2[l];
+    G.g = g;
+    const int sc = (g.kind == FEM_Q2_2D) ? 2 : 1;
+    G.lat = FemLattice{sc * g.nex + 1, sc * g.ney + 1, g.periodic};
+    G.tab = tabs[l];
+    M->off[l] = tot;
+    M->nn[l] = g.nn;
+    tot += g.nn;
+  }
+  M->total = tot;
+  const int nc = M->nn[nlev - 1];
+  if (nc > MG3_COARSE_MAX) {
+    snprintf(fem_err_buf(), 256, "mixed multigrid: coarsest level of %d nodes exceeds %d", nc, MG3_COARSE_MAX);
+    mg3_destroy(M);
+    return FEM_E_ARG;
+  }
+  int rc = mg3_alloc(M);
+  for (int l = 0; l < nlev && rc == FEM_OK; ++l) {
+    const size_t o = M->off[l];
+    const uint8_t* pin = mean_zero ? nullptr : pins[l];
+    if (pin) {
+      if (cudaMemcpyAsync(M->pin + o, pin, M->nn[l], cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        rc = fem_cuda_error("cudaMemcpyAsync", cudaGetLastError());
+    } else if (cudaMemsetAsync(M->pin + o, 0, M->nn[l], s) != cudaSuccess) {
+      rc = fem_cuda_error("cudaMemsetAsync", cudaGetLastError());
+    }
+    if (rc) break;
+    k_mg2_invdiag<<<mg3_blocks_elem(M->nn[l], M->cap), MG3_THREADS, 0, s>>>(M->nn[l], diags[l],
+                                                                            mean_zero ? nullptr : M->pin + o,
+                                                                            M->invD64 + o, M->invD32 + o);
+    rc = fem_after_launch("k_mg2_invdiag");
+    mg3_bind(M->m64[l], M->geo2[l], M->work64 + 5 * o, (const double*)(M->invD64 + o));
+    mg3_bind(M->m32[l], M->geo2[l], M->work32 + 5 * o, (const float*)(M->invD32 + o));
+  }
+  if (rc == FEM_OK) rc = mg3_chebyshev(M, M->geo2, s);
+  if (rc == FEM_OK) {
+    const Mg2Geo& C = M->geo2[nlev - 1];
+    const long long nn2 = (long long)nc * nc;
+    const int gb = (int)std::min<long long>((nn2 + 255) / 256, (long long)M->cap * 4);
+    if (cudaMemsetAsync(M->Ainv, 0, sizeof(double) * nn2, s) != cudaSuccess)
+      rc = fem_cuda_error("cudaMemsetAsync", cudaGetLastError());
+    if (rc == FEM_OK) {
+      if (C.g.kind == FEM_Q1_2D)
+        k_mg2_dense_rows<FEM_Q1_2D><<<mg3_blocks_elem(nc, M->cap), MG3_THREADS, 0, s>>>(C.g, C.tab, M->Ainv);
+      else
+        k_mg2_dense_rows<FEM_Q2_2D><<<mg3_blocks_elem(nc, M->cap), MG3_THREADS, 0, s>>>(C.g, C.tab, M->Ainv);
+      rc = fem_after_launch("k_mg2_dense_rows");
+    }
+    if (rc == FEM_OK) {
+      // the shift of the mean-zero coarse matrix: about its mean diagonal entry / n
+      double d[2] = {0.0, 0.0};
+      if (cudaMemcpyAsync(d, M->Ainv, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        rc = fem_cuda_error("coarse diagonal", cudaGetLastError());
+      if (rc == FEM_OK) {
+        k_mg2_dense_fix<<<gb, 256, 0, s>>>(nc, M->mz ? nullptr : M->pin + M->off[nlev - 1], M->mz, d[0] / nc,
+                                           M->Ainv);
+        rc = fem_after_launch("k_mg2_dense_fix");
+      }
+    }
+  }
+  if (rc == FEM_OK) rc = mg3_invert(M, nc, s);
+  if (rc) {
+    mg3_destroy(M);
+    return rc;
+  }
+  *out = M;
+  return FEM_OK;
+}
+
+// transfers per level geometry
 template <class T>
-static int mg3_vcycle(const Mg3* M, Mg3Lev<T>* lv, double* dot_parts, cudaStream_t s) {
+static void mg3_restrict(const Mg3* M, const Mg3Lev<T, Mg3Geo>& F, const Mg3Lev<T, Mg3Geo>& C, int nC,
+                         cudaStream_t s) {
+  k_mg3_restrict<T><<<mg3_blocks_elem(nC, M->cap), MG3_THREADS, 0, s>>>(F, C);
+}
+template <class T>
+static void mg3_restrict(const Mg3* M, const Mg3Lev<T, Mg2Geo>& F, const Mg3Lev<T, Mg2Geo>& C, int nC,
+                         cudaStream_t s) {
+  k_mg2_restrict<T><<<mg3_blocks_elem(nC, M->cap), MG3_THREADS, 0, s>>>(F, C);
+}
+template <class T>
+static void mg3_prolong(const Mg3* M, const Mg3Lev<T, Mg3Geo>& F, const Mg3Lev<T, Mg3Geo>& C, int nF,
+                        cudaStream_t s) {
+  k_mg3_prolong<T><<<mg3_blocks_elem(nF, M->cap), MG3_THREADS, 0, s>>>(F, C, F.xb, C.xb, F.xa);
+}
+template <class T>
+static void mg3_prolong(const Mg3* M, const Mg3Lev<T, Mg2Geo>& F, const Mg3Lev<T, Mg2Geo>& C, int nF,
+                        cudaStream_t s) {
+  k_mg2_prolong<T><<<mg3_blocks_elem(nF, M->cap), MG3_THREADS, 0, s>>>(F, C, F.xb, C.xb, F.xa, M->mz);
+}
+
+// V-cycle on the level vectors of precision T: input lv[0].r, output lv[0].xb.
+// dot: block partials of r . z (and, mean-zero, sum z and sum r) into
+// dot_parts, written by the last smoothing step.
+template <class T, class G>
+static int mg3_vcycle(const Mg3* M, Mg3Lev<T, G>* lv, double* dot_parts, cudaStream_t s) {
   const int N = M->nlev, cap = M->cap;
   for (int l = 0; l < N - 1; ++l) {
-    const Mg3Lev<T>& L = lv[l];
+    const Mg3Lev<T, G>& L = lv[l];
     const int gb = mg3_blocks_sweep(L.geo, cap);
-    k_mg3_first<T><<<gb, MG3_THREADS, 0, s>>>(L, M->cb[l][0], M->ca[l][1], M->cb[l][1]);
+    k_mg3_first<T, G><<<gb, MG3_THREADS, 0, s>>>(L, M->cb[l][0], M->ca[l][1], M->cb[l][1]);
     const T* x = L.xa;
     T* y = L.xb;
     for (int k = 2; k < MG3_DEGREE; ++k) {  // pre-smoothing steps 3.. (ping-pong ending in xb)
-      k_mg3_step<T, false, false><<<gb, MG3_THREADS, 0, s>>>(L, x, y, M->ca[l][k], M->cb[l][k], nullptr);
+      k_mg3_step<T, G, false, 0><<<gb, MG3_THREADS, 0, s>>>(L, x, y, M->ca[l][k], M->cb[l][k], nullptr);
       const T* tmp = y;
       y = const_cast<T*>(x);
       x = tmp;
     }
     // x holds the pre-smoothed iterate; keep it in xb
-    if (x != L.xb) {
-      if (cudaMemcpyAsync(L.xb, x, sizeof(T) * M->nn[l], cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-        return fem_cuda_error("cudaMemcpyAsync", cudaGetLastError());
-    }
-    k_mg3_resid<T><<<gb, MG3_THREADS, 0, s>>>(L, L.xb);
-    k_mg3_restrict<T><<<mg3_blocks_elem(M->nn[l + 1], cap), MG3_THREADS, 0, s>>>(L, lv[l + 1]);
+    if (x != L.xb) MG3_CUDA(cudaMemcpyAsync(L.xb, x, sizeof(T) * M->nn[l], cudaMemcpyDeviceToDevice, s));
+    k_mg3_resid<T, G><<<gb, MG3_THREADS, 0, s>>>(L, L.xb);
+    mg3_restrict(M, L, lv[l + 1], M->nn[l + 1], s);
     MG3_TRY(fem_after_launch("k_mg3_down"));
   }
-  const Mg3Lev<T>& C = lv[N - 1];
+  const Mg3Lev<T, G>& C = lv[N - 1];
   const int nc = M->nn[N - 1];
-  k_mg3_coarse<T><<<(nc + 7) / 8, 256, 0, s>>>(C, M->Ainv, C.xb);
+  k_mg3_coarse<T, G><<<(nc + 7) / 8, 256, 0, s>>>(C, nc, M->mz, M->Ainv, C.xb);
   MG3_TRY(fem_after_launch("k_mg3_coarse"));
   for (int l = N - 2; l >= 0; --l) {
-    const Mg3Lev<T>& L = lv[l];
+    const Mg3Lev<T, G>& L = lv[l];
     const int gb = mg3_blocks_sweep(L.geo, cap);
-    k_mg3_prolong<T><<<mg3_blocks_elem(M->nn[l], cap), MG3_THREADS, 0, s>>>(L, lv[l + 1], L.xb, lv[l + 1].xb, L.xa);
+    mg3_prolong(M, L, lv[l + 1], M->nn[l], s);
     // post-smoothing: steps xa -> xb -> xa -> xb (degree 3 ends in xb)
     T* bufs[2] = {L.xa, L.xb};
     for (int k = 0; k < MG3_DEGREE; ++k) {
@@ -763,11 +1019,13 @@ static int mg3_vcycle(const Mg3* M, Mg3Lev<T>* lv, double* dot_parts, cudaStream
       const T* xi = bufs[k & 1];
       T* xo = bufs[(k + 1) & 1];
       if (k == 0)
-        k_mg3_step<T, true, false><<<gb, MG3_THREADS, 0, s>>>(L, xi, xo, 0.0, M->cb[l][0], nullptr);
+        k_mg3_step<T, G, true, 0><<<gb, MG3_THREADS, 0, s>>>(L, xi, xo, 0.0, M->cb[l][0], nullptr);
+      else if (dp && M->mz)
+        k_mg3_step<T, G, false, 3><<<gb, MG3_THREADS, 0, s>>>(L, xi, xo, M->ca[l][k], M->cb[l][k], dp);
       else if (dp)
-        k_mg3_step<T, false, true><<<gb, MG3_THREADS, 0, s>>>(L, xi, xo, M->ca[l][k], M->cb[l][k], dp);
+        k_mg3_step<T, G, false, 1><<<gb, MG3_THREADS, 0, s>>>(L, xi, xo, M->ca[l][k], M->cb[l][k], dp);
       else
-        k_mg3_step<T, false, false><<<gb, MG3_THREADS, 0, s>>>(L, xi, xo, M->ca[l][k], M->cb[l][k], nullptr);
+        k_mg3_step<T, G, false, 0><<<gb, MG3_THREADS, 0, s>>>(L, xi, xo, M->ca[l][k], M->cb[l][k], nullptr);
     }
     MG3_TRY(fem_after_launch("k_mg3_up"));
   }
@@ -775,6 +1033,7 @@ static int mg3_vcycle(const Mg3* M, Mg3Lev<T>* lv, double* dot_parts, cudaStream
 }
 
 int mg3_vcycle64(Mg3* M, const double* r, double* z, cudaStream_t s) {
+  if (M->d2) return FEM_E_STATE;
   Mg3Lev<double>& L0 = M->l64[0];
   MG3_CUDA(cudaMemcpyAsync(L0.r, r, sizeof(double) * M->nn[0], cudaMemcpyDeviceToDevice, s));
   MG3_TRY(mg3_vcycle<double>(M, M->l64, nullptr, s));
@@ -839,24 +1098,24 @@ static int mg3_capture(Mg3* M, cudaStream_t cs, Pro pro, Body body, Epi epi, cud
   return rc;
 }
 
-// One FP32-or-FP64 PCG iteration body pieces on level-0 vectors of type T.
+// One PCG iteration's vectors on level 0, of type T.
 template <class T>
 struct Mg3Cg {
   T *x, *r, *z, *pold, *pnew, *Ap;
 };
 
-template <class T>
-static int mg3_cg_iter(const Mg3* M, Mg3Lev<T>* lv, const Mg3Cg<T>& V, int inner, bool vcycle, int ctl_mode,
+template <class T, class G>
+static int mg3_cg_iter(const Mg3* M, Mg3Lev<T, G>* lv, const Mg3Cg<T>& V, int inner, bool vcycle, int ctl_mode,
                        cudaGraphConditionalHandle h, cudaStream_t s) {
-  const Mg3Lev<T>& L0 = lv[0];
+  const Mg3Lev<T, G>& L0 = lv[0];
   const int n = M->nn[0], gb = mg3_blocks_sweep(L0.geo, M->cap), ge = mg3_blocks_elem(n, M->cap);
   double *pA = M->parts, *pB = M->parts + MG3_PARTS, *pC = M->parts + 3 * MG3_PARTS;
-  k_mg3_ap<T><<<gb, MG3_THREADS, 0, s>>>(L0, V.z, V.pold, V.pnew, V.Ap, M->sc, inner, pA);
+  k_mg3_ap<T, G><<<gb, MG3_THREADS, 0, s>>>(L0, V.z, V.pold, V.pnew, V.Ap, M->sc, inner, M->mz, pA);
   k_mg3_xr<T><<<ge, MG3_THREADS, 0, s>>>(n, V.x, V.r, V.pnew, V.pold, V.Ap, M->sc, inner, pA, gb, pB);
   MG3_TRY(fem_after_launch("k_mg3_cg"));
   if (vcycle) {
-    MG3_TRY(mg3_vcycle<T>(M, lv, pC, s));
-    k_mg3_ctl<<<1, 256, 0, s>>>(M->sc, ctl_mode, pC, gb, pB, ge, h);
+    MG3_TRY(mg3_vcycle<T, G>(M, lv, pC, s));
+    k_mg3_ctl<<<1, 256, 0, s>>>(M->sc, ctl_mode, pC, gb, pB, ge, M->mz ? 1.0 / n : 0.0, h);
     MG3_TRY(fem_after_launch("k_mg3_ctl"));
   }
   return FEM_OK;
@@ -880,9 +1139,10 @@ static Mg3GraphCache* mg3_cache_slot(Mg3* M, const Mg3GraphKey& key) {
 }
 
 // FP64 MG-PCG (utils/jax_iterative_solvers.py:87-120 with M = the V-cycle):
-// b, x (x0 in, solution out) device FP64; iters/status device ints.
-int mg3_pcg(Mg3* M, const double* b, double* x, double tol, double atol, int maxiter, int* iters,
-            int* status, cudaStream_t s, cudaStream_t cs) {
+// b, x (x0 in, solution out) device FP64; iters/status device ints. hex8.
+int mg3_pcg(Mg3* M, const double* b, double* x, double tol, double atol, int maxiter, int* iters, int* status,
+            cudaStream_t s, cudaStream_t cs) {
+  if (M->d2) return FEM_E_STATE;
   Mg3GraphKey key;
   memset(&key, 0, sizeof(key));
   key.mode = MG3_MODE_PCG;
@@ -895,17 +1155,18 @@ int mg3_pcg(Mg3* M, const double* b, double* x, double tol, double atol, int max
     double *pB = M->parts + MG3_PARTS, *pC = M->parts + 3 * MG3_PARTS;
     auto pro = [&](cudaStream_t cs_, cudaGraphConditionalHandle h) -> int {
       MG3_CUDA(cudaMemsetAsync(V.pold, 0, sizeof(double) * n, cs_));
-      k_mg3_res64<double><<<gb, MG3_THREADS, 0, cs_>>>(lv[0], lv[0].geo, M->pin, M->b64, M->x64, lv[0].r, pB);
+      k_mg3_res64<double, Mg3Geo><<<gb, MG3_THREADS, 0, cs_>>>(lv[0].geo, M->pin, M->b64, M->x64, lv[0].r, pB);
       MG3_TRY(fem_after_launch("k_mg3_res64"));
       MG3_TRY(mg3_vcycle<double>(M, lv, pC, cs_));
-      k_mg3_ctl<<<1, 256, 0, cs_>>>(M->sc, MG3_CTL_PCG0, pC, gb, pB, gb, h);
+      k_mg3_ctl<<<1, 256, 0, cs_>>>(M->sc, MG3_CTL_PCG0, pC, gb, pB, gb, 0.0, h);
       return fem_after_launch("k_mg3_ctl");
     };
     auto body = [&](cudaStream_t bs, cudaGraphConditionalHandle h) -> int {
       return mg3_cg_iter<double>(M, lv, V, 0, true, MG3_CTL_PCG, h, bs);
     };
     auto epi = [&](cudaStream_t cs_) -> int {
-      k_mg3_add<double><<<mg3_blocks_elem(n, M->cap), MG3_THREADS, 0, cs_>>>(n, M->x64, (const double*)nullptr, M->pin);
+      k_mg3_add<double><<<mg3_blocks_elem(n, M->cap), MG3_THREADS, 0, cs_>>>(n, M->x64, (const double*)nullptr,
+                                                                             M->pin);
       k_mg3_finish<<<1, 32, 0, cs_>>>(M->sc, MG3_MODE_PCG);
       return fem_after_launch("k_mg3_finish");
     };
@@ -923,45 +1184,64 @@ int mg3_pcg(Mg3* M, const double* b, double* x, double tol, double atol, int max
   return FEM_OK;
 }
 
+// The mixed-precision refinement graph for level vectors of geometry G.
+template <class G>
+static int mg3_mixed_graph(Mg3* M, Mg3Lev<float, G>* lv, int inner, cudaStream_t cs, cudaGraphExec_t* exec) {
+  const int n = M->nn[0];
+  float* d32 = M->v32 + 3 * n;
+  const Mg3Cg<float> V{d32, lv[0].r, lv[0].xb, M->v32, M->v32 + n, M->v32 + 2 * n};
+  const int gb = mg3_blocks_sweep(lv[0].geo, M->cap), ge = mg3_blocks_elem(n, M->cap);
+  double *pA = M->parts, *pB = M->parts + MG3_PARTS, *pC = M->parts + 3 * MG3_PARTS;
+  const uint8_t* pin0 = M->mz ? nullptr : M->pin;
+  const double inv_n = M->mz ? 1.0 / n : 0.0;
+  auto pro = [&](cudaStream_t cs_, cudaGraphConditionalHandle h) -> int {
+    if (M->mz) {  // centre b (mean-zero problems solve on the mean-zero subspace)
+      k_mg3_sum<<<ge, MG3_THREADS, 0, cs_>>>(n, M->b64, pA);
+      k_mg3_center<<<ge, MG3_THREADS, 0, cs_>>>(n, M->b64, pA, ge);
+    }
+    k_mg3_res64<float, G><<<gb, MG3_THREADS, 0, cs_>>>(lv[0].geo, pin0, M->b64, M->x64, lv[0].r, pB);
+    k_mg3_ctl<<<1, 256, 0, cs_>>>(M->sc, MG3_CTL_MX0, nullptr, 0, pB, gb, 0.0, h);
+    return fem_after_launch("k_mg3_ctl");
+  };
+  auto body = [&](cudaStream_t bs, cudaGraphConditionalHandle h) -> int {
+    MG3_CUDA(cudaMemsetAsync(d32, 0, sizeof(float) * n, bs));
+    MG3_CUDA(cudaMemsetAsync(V.pold, 0, sizeof(float) * n, bs));
+    MG3_TRY(mg3_vcycle<float, G>(M, lv, pC, bs));
+    k_mg3_ctl<<<1, 256, 0, bs>>>(M->sc, MG3_CTL_IN0, pC, gb, nullptr, 0, inv_n, h);
+    for (int k = 0; k < inner; ++k) MG3_TRY(mg3_cg_iter<float, G>(M, lv, V, 1, k + 1 < inner, MG3_CTL_IN, h, bs));
+    k_mg3_add<float><<<ge, MG3_THREADS, 0, bs>>>(n, M->x64, d32, nullptr);
+    k_mg3_res64<float, G><<<gb, MG3_THREADS, 0, bs>>>(lv[0].geo, pin0, M->b64, M->x64, lv[0].r, pB);
+    k_mg3_ctl<<<1, 256, 0, bs>>>(M->sc, MG3_CTL_MX, nullptr, 0, pB, gb, 0.0, h);
+    return fem_after_launch("k_mg3_mixed");
+  };
+  auto epi = [&](cudaStream_t cs_) -> int {
+    if (M->mz) {
+      k_mg3_sum<<<ge, MG3_THREADS, 0, cs_>>>(n, M->x64, pA);
+      k_mg3_center<<<ge, MG3_THREADS, 0, cs_>>>(n, M->x64, pA, ge);
+    } else {
+      k_mg3_add<float><<<ge, MG3_THREADS, 0, cs_>>>(n, M->x64, (const float*)nullptr, M->pin);
+    }
+    k_mg3_finish<<<1, 32, 0, cs_>>>(M->sc, MG3_MODE_MIXED);
+    return fem_after_launch("k_mg3_finish");
+  };
+  return mg3_capture(M, cs, pro, body, epi, exec);
+}
+
 // Mixed precision: FP64 refinement x += d until ||b - A x|| <= tol ||b|| or
 // max_cycles, d from `inner` FP32 MG-PCG iterations on A d = r from d = 0.
-int mg3_mixed(Mg3* M, const double* b, double* x, double tol, int inner, int max_cycles,
-              int* cycles, int* status, cudaStream_t s, cudaStream_t cs) {
+int mg3_mixed(Mg3* M, const double* b, double* x, double tol, int inner, int max_cycles, int* cycles, int* status,
+              cudaStream_t s, cudaStream_t cs) {
   Mg3GraphKey key;
   memset(&key, 0, sizeof(key));
   key.mode = MG3_MODE_MIXED;
   key.inner = inner;
   Mg3GraphCache* gc = mg3_cache_slot(M, key);
   const int n = M->nn[0];
-  Mg3Lev<float>* lv = M->l32;
   if (!gc->exec) {
-    float* d32 = M->v32 + 3 * n;
-    const Mg3Cg<float> V{d32, lv[0].r, lv[0].xb, M->v32, M->v32 + n, M->v32 + 2 * n};
-    const int gb = mg3_blocks_sweep(lv[0].geo, M->cap), ge = mg3_blocks_elem(n, M->cap);
-    double *pB = M->parts + MG3_PARTS, *pC = M->parts + 3 * MG3_PARTS;
-    auto pro = [&](cudaStream_t cs_, cudaGraphConditionalHandle h) -> int {
-      k_mg3_res64<float><<<gb, MG3_THREADS, 0, cs_>>>(lv[0], lv[0].geo, M->pin, M->b64, M->x64, lv[0].r, pB);
-      k_mg3_ctl<<<1, 256, 0, cs_>>>(M->sc, MG3_CTL_MX0, nullptr, 0, pB, gb, h);
-      return fem_after_launch("k_mg3_ctl");
-    };
-    auto body = [&](cudaStream_t bs, cudaGraphConditionalHandle h) -> int {
-      MG3_CUDA(cudaMemsetAsync(d32, 0, sizeof(float) * n, bs));
-      MG3_CUDA(cudaMemsetAsync(V.pold, 0, sizeof(float) * n, bs));
-      MG3_TRY(mg3_vcycle<float>(M, lv, pC, bs));
-      k_mg3_ctl<<<1, 256, 0, bs>>>(M->sc, MG3_CTL_IN0, pC, gb, nullptr, 0, h);
-      for (int k = 0; k < inner; ++k)
-        MG3_TRY(mg3_cg_iter<float>(M, lv, V, 1, k + 1 < inner, MG3_CTL_IN, h, bs));
-      k_mg3_add<float><<<ge, MG3_THREADS, 0, bs>>>(n, M->x64, d32, nullptr);
-      k_mg3_res64<float><<<gb, MG3_THREADS, 0, bs>>>(lv[0], lv[0].geo, M->pin, M->b64, M->x64, lv[0].r, pB);
-      k_mg3_ctl<<<1, 256, 0, bs>>>(M->sc, MG3_CTL_MX, nullptr, 0, pB, gb, h);
-      return fem_after_launch("k_mg3_mixed");
-    };
-    auto epi = [&](cudaStream_t cs_) -> int {
-      k_mg3_add<float><<<ge, MG3_THREADS, 0, cs_>>>(n, M->x64, (const float*)nullptr, M->pin);
-      k_mg3_finish<<<1, 32, 0, cs_>>>(M->sc, MG3_MODE_MIXED);
-      return fem_after_launch("k_mg3_finish");
-    };
-    MG3_TRY(mg3_capture(M, cs, pro, body, epi, &gc->exec));
+    if (M->d2)
+      MG3_TRY(mg3_mixed_graph<Mg2Geo>(M, M->m32, inner, cs, &gc->exec));
+    else
+      MG3_TRY(mg3_mixed_graph<Mg3Geo>(M, M->l32, inner, cs, &gc->exec));
   }
   k_mg3_set<<<1, 32, 0, s>>>(M->sc, tol, 0.0, 0, max_cycles);
   MG3_TRY(fem_after_launch("k_mg3_set"));

@@ -720,6 +720,74 @@ int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, con
   return fem_after_launch("k_conv_apply");
 }
 
+// hex8: Gauss-point factors of Ce(U), element-major fq[e * 32 + 4 q + k]
+// (fem_conv3_factors), one thread per element
+__global__ void __launch_bounds__(256) k_conv_factors3(FemGrid g, const __grid_constant__ FemQuadTab qt,
+                                                       const double* __restrict__ U, double bd,
+                                                       double* __restrict__ fq) {
+  const size_t nn = g.nn;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.ne; e += gridDim.x * blockDim.x) {
+    const int ex = e % g.nex, eyz = e / g.nex, ey = eyz % g.ney, ez = eyz / g.ney;
+    double u[3][8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const size_t n = fem_enode<FEM_HEX8, 0>(g, ex, ey, ez) + (size_t)kdk<FEM_HEX8>(b) * g.nnx * g.nny +
+                       (size_t)kdj<FEM_HEX8>(b) * g.nnx + kdi<FEM_HEX8>(b);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) u[c][b] = U[n + c * nn];
+    }
+    fem_conv3_factors(qt, u, bd, fq + (size_t)e * FEM_C3_NF);
+  }
+}
+
+// hex8: y = alpha Ash x + cc Ce x (3 components) from the factors, one tile
+// loop per CTA over the lattice
+__global__ void __launch_bounds__(FEM_THREADS, 1) k_conv_apply3(FemGrid g, const __grid_constant__ FemQuadTab qt,
+                                                                const double* __restrict__ fq, double cc,
+                                                                double alpha, const double* __restrict__ Ash,
+                                                                const double* __restrict__ x, double* __restrict__ y,
+                                                                int* err) {
+  extern __shared__ __align__(128) double sm3[];
+  __shared__ double sA[64];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ unsigned phase;
+  if (Ash)
+    for (int t = threadIdx.x; t < 64; t += blockDim.x) sA[t] = Ash[t];
+  if (threadIdx.x == 0) {
+    fem_mbar_init(&bar, 1);
+    phase = 0u;
+  }
+  __syncthreads();
+  const size_t nn = g.nn;
+  struct Tiles {
+    __device__ __forceinline__ int cta() const { return blockIdx.x; }
+    __device__ __forceinline__ int ncta() const { return gridDim.x; }
+  } tm;
+  const double* src[1] = {x};
+  const FemC3Tma tma{&bar, &phase, err};
+  fem_tiled_conv3<3, 1>(tm, g, sm3, tma, src, [](int, const double(&v)[1]) { return v[0]; }, fq, qt, cc, alpha,
+                        Ash ? sA : nullptr, [&](int i, const double(&v)[3], const double(&)[3]) {
+#pragma unroll
+                          for (int c = 0; c < 3; ++c) y[i + c * nn] = v[c];
+                        });
+}
+
+int fem_launch_conv_factors3(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,
+                             cudaStream_t s) {
+  if (g.kind != FEM_HEX8) return FEM_E_ARG;
+  k_conv_factors3<<<fem_nblocks(g.ne, 256), 256, 0, s>>>(g, qt, U, bd, fq);
+  return fem_after_launch("k_conv_factors3");
+}
+
+int fem_launch_conv_apply3(const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc, double alpha,
+                           const double* Ash, const double* x, double* y, int grid, int* err, cudaStream_t s) {
+  if (g.kind != FEM_HEX8 || grid < 1) return FEM_E_ARG;
+  const int dyn = FEM_C3_SMEM(3, 1) * (int)sizeof(double);
+  cudaFuncSetAttribute(k_conv_apply3, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  k_conv_apply3<<<grid, FEM_THREADS, dyn, s>>>(g, qt, fq, cc, alpha, Ash, x, y, err);
+  return fem_after_launch("k_conv_apply3");
+}
+
 // Self-test of the grid barrier's time limit: one CTA waits at a counter
 // barrier for one more party than the launch has, so the wait can only end
 // through the FEM_BARRIER_TIMEOUT_NS limit. It then sets FEM_ERR_BARRIER_TIMEOUT

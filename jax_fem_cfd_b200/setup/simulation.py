@@ -33,8 +33,8 @@ class StandardSolverConfig:
     set_zeroP: bool
     pressure_precond: Optional[str] = None
     final_multigrid_mesh: Optional[List[int]] = None
-    # Extension (no reference field): "mixed" runs the hex8 multigrid pressure
-    # solve as FP64 refinement around FP32 multigrid-PCG iterations.
+    # Extension (no reference field): "mixed" runs the multigrid pressure solve
+    # as FP64 refinement around FP32 multigrid-PCG iterations.
     precision: str = "fp64"
 
 
@@ -98,9 +98,8 @@ class Config:
                     raise ValueError("3D multigrid needs pinned pressure (set_zeroP=True)")
         if getattr(ns, "precision", "fp64") not in ("fp64", "mixed"):
             raise ValueError(f"Unknown precision: {ns.precision}")
-        if getattr(ns, "precision", "fp64") == "mixed" and not (len(self.mesh_config.num_elem) == 3
-                                                                and ns.pressure_precond == "multigrid"):
-            raise ValueError("precision='mixed' is implemented for the 3D multigrid pressure solve")
+        if getattr(ns, "precision", "fp64") == "mixed" and ns.pressure_precond != "multigrid":
+            raise ValueError("precision='mixed' is implemented for the multigrid pressure solve")
         if ns.pressure_precond == "multigrid":
             num_elemf = ns.final_multigrid_mesh
             if num_elemf is None:

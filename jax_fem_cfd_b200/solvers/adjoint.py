@@ -9,17 +9,17 @@ intermediate velocity U* to
 
 with D = G^T (divergence_element_mult is sum_i G_i^T u_i, gradient_element_mult
 is [G_1 p; ...]). A+ solves A P = rhs with the gamma_p rows of A and rhs
-zeroed and P = 0 on gamma_p, which is symmetric on the free nodes. The stage is
-affine in U*, and its reverse (vector-Jacobian product) for output gradients
-(g_U, g_P) is
+zeroed and P = 0 on gamma_p (set_zeroP), or, for mean-zero pressure, is
+C S C with C = I - 1 1^T / n the centring and S the solve on the mean-zero
+subspace; both are symmetric. The stage is affine in U*, and its reverse
+(vector-Jacobian product) for output gradients (g_U, g_P) is
 
     g_U' = g_U with gamma_d rows zeroed
-    w    = g_P - c D (M^-1 g_U'),  w = 0 on gamma_p
-    lam  = A+ w                     (the adjoint solve: the same pinned MG-PCG)
+    w    = g_P - c D (M^-1 g_U'),  w = 0 on gamma_p (pinned)
+    lam  = A+ w                     (the adjoint solve: the same MG-PCG)
     g_U* = g_U' + k G lam
 
-`Projection` puts this behind torch.autograd (the analogue of jax.custom_vjp);
-pinned pressure (set_zeroP) only.
+`Projection` puts this behind torch.autograd (the analogue of jax.custom_vjp).
 
 `MomentumSolve` is the momentum solve of solvers/standard.py:14-43 for a fixed
 operator A = (rho/dt) Me + theta (rho Ce(U_n) + mu Le) with identity rows on
@@ -34,7 +34,7 @@ differentiates with jax.grad.
 
 `rollout` chains Steps with checkpoints every `ckpt` steps (recomputation in
 the backward pass). `Step` is one whole 4-step time step (U_n, P_n) -> (U_{n+1}, P_{n+1}) of a
-wall-bounded pinned-pressure problem (solvers/standard.py:148-165, theta = 1/2,
+wall-bounded pinned-pressure or a periodic mean-zero problem (solvers/standard.py:148-165, theta = 1/2,
 Ce(U_n) with beta = 1/2, F = 0, F_p = 0): the rhs
 (rho/dt) Me U_n - (1 - theta)(rho Ce(U_n) + mu Le) U_n - G P_n (U_d on gamma_d),
 the momentum solve, U* = U_hat + (dt/rho) G P_n / M, the projection. Its
@@ -90,15 +90,20 @@ def _solver_masks(solver):
 
 
 def _pressure(solver, rhs, tol):
-    """A+ rhs: the pinned MG-PCG pressure solve of the solver's context from 0."""
+    """A+ rhs: the pressure solve of the solver's context from 0. Pinned
+    (set_zeroP): gamma_p rows of rhs zeroed and P = 0 there. Mean-zero: rhs
+    centred, the solve on the mean-zero subspace and P centred
+    (solvers/standard.py:104-125), i.e. P = C S C rhs with C = I - 1 1^T / n."""
     ctx, pm, _ = _solver_masks(solver)
+    pinned = bool(solver.cfg.set_zeroP)
     r = rhs.clone()
-    r.masked_fill_(pm, 0.0)
+    if pinned:
+        r.masked_fill_(pm, 0.0)
     x = torch.zeros_like(r)
     it = torch.zeros(1, dtype=torch.int32, device=r.device)
     st = torch.zeros(1, dtype=torch.int32, device=r.device)
-    _lib.call("fem_pressure_solve", ctx.handle, ptr(r), ptr(x), float(tol), 0.0, 1000, solver.precond, 0, 1, ptr(it),
-              ptr(st), stream())
+    _lib.call("fem_pressure_solve", ctx.handle, ptr(r), ptr(x), float(tol), 0.0, 1000, solver.precond,
+              0 if pinned else 1, 1, ptr(it), ptr(st), stream())
     _check(st, "pressure solve")
     return x
 
@@ -120,8 +125,6 @@ class Projection(torch.autograd.Function):
 
     @staticmethod
     def forward(fctx, U_star, solver, dt, rho, U_d_full, F_p, tol=1e-12):
-        if not solver.cfg.set_zeroP:
-            raise ValueError("Projection covers the pinned-pressure (set_zeroP) form only")
         ctx, pm, dm = _solver_masks(solver)
         M = ctx.element_data()[6]
         k, c = rho / dt, dt / rho
@@ -146,7 +149,8 @@ class Projection(torch.autograd.Function):
         w = (gP.contiguous().clone() if gP is not None else torch.zeros(solver.nn, dtype=torch.float64,
                                                                         device=M.device))
         w = w - c * _div(solver, (gU / M).contiguous())
-        w.masked_fill_(pm, 0.0)
+        if solver.cfg.set_zeroP:
+            w.masked_fill_(pm, 0.0)
         lam = _pressure(solver, w, tol)
         return gU + k * _grad(solver, lam), None, None, None, None, None, None
 
@@ -235,7 +239,8 @@ def _projection_vjp(solver, gU, gP, k, c, tol):
     if dm is not None:
         gU.masked_fill_(dm, 0.0)
     w = gP.contiguous().clone() - c * _div(solver, (gU / M).contiguous())
-    w.masked_fill_(pm, 0.0)
+    if solver.cfg.set_zeroP:
+        w.masked_fill_(pm, 0.0)
     return gU + k * _grad(solver, _pressure(solver, w, tol))
 
 
@@ -244,8 +249,6 @@ class Step(torch.autograd.Function):
 
     @staticmethod
     def forward(fctx, U_n, P_n, solver, nconn, dt, rho, mu, U_d_full, tol=1e-13):
-        if not solver.cfg.set_zeroP:
-            raise ValueError("Step covers the pinned-pressure (set_zeroP) form only")
         theta, beta = 0.5, 0.5
         ctx, pm, dm = _solver_masks(solver)
         Me, Le, M = ctx.element_data()[3].reshape(-1), ctx.element_data()[4].reshape(-1), ctx.element_data()[6]

@@ -53,7 +53,10 @@ def test_projection_vjp_matches_finite_differences(cavity, seed):
 
 
 @pytest.mark.gpu
-def test_projection_refuses_mean_zero_pressure():
+def test_projection_vjp_mean_zero_pressure():
+    """The projection of a periodic problem (mean-zero pressure: rhs and P
+    centred around the solve on the mean-zero subspace) against central
+    differences; the adjoint solve is the same centred solve."""
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     from bench import tg_config
@@ -61,9 +64,24 @@ def test_projection_refuses_mean_zero_pressure():
     from jax_fem_cfd_b200.solvers.adjoint import Projection
     _, timestep, *rest = sim.setup(tg_config(sim, 8))
     solver = timestep.solver
-    u = torch.zeros(solver.ndim * solver.nn, dtype=torch.float64, device="cuda")
-    with pytest.raises(ValueError):
-        Projection.apply(u, solver, 0.01, 1.0, None, None)
+    n2, n = solver.ndim * solver.nn, solver.nn
+    rng = np.random.default_rng(3)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
+    Us, gU, gP, dlt = t(rng.standard_normal(n2)), t(rng.standard_normal(n2)), t(rng.standard_normal(n)), \
+        t(rng.standard_normal(n2))
+
+    def loss(u):
+        U, P = Projection.apply(u, solver, 0.01, 1.0, None, None, 1e-13)
+        return float((gU * U).sum() + (gP * P).sum())
+
+    x = Us.clone().requires_grad_(True)
+    U, P = Projection.apply(x, solver, 0.01, 1.0, None, None, 1e-13)
+    assert abs(float(P.mean())) < 1e-12 * float(P.abs().max())
+    ((gU * U).sum() + (gP * P).sum()).backward()
+    eps = 1e-2
+    fd = (loss(Us + eps * dlt) - loss(Us - eps * dlt)) / (2 * eps)
+    vjp = float((x.grad * dlt).sum())
+    assert abs(vjp - fd) <= 1e-7 * max(abs(fd), 1.0), (vjp, fd)
 
 
 @pytest.mark.gpu
