@@ -230,8 +230,56 @@ def run_ours(args, rank, world, local_rank):
     d2h = h2d
     res = dict(total_ms=total_ms, step_ms=step_ms, stage_ms=(stage_ms / args.steps).tolist(), iters=iters,
                launches=launches, clocks=clk.summary(), e2e_ms=e2e_ms, h2d=h2d, d2h=d2h, nn=nn, ctx=ctx,
-               level_nn=[ctx.level_info(l)[0] for l in range(ctx.nlev)], block_from=None)
+               level_nn=[ctx.level_info(l)[0] for l in range(ctx.nlev)], block_from=None,
+               final=(U.clone(), P.clone()), coords=nc)
     return res
+
+
+def tg_mixed(args, fp64_final, coords):
+    """The same Taylor-Green workload with the mixed-precision pressure solve
+    (StandardSolverConfig(precision="mixed"): FP64 refinement to the step's
+    1e-8 around FP32 Chebyshev-multigrid PCG iterations; momentum stays FP64):
+    warm-up + timed steps exactly as the FP64 run (L2 flushed between timed
+    steps, CUDA events), then the final state against the FP64 run's after the
+    same steps, and both against the analytic decay u0 exp(-2 nu t)."""
+    import torch
+
+    import jax_fem_cfd_b200.setup.simulation as sim
+    cfg = tg_config(sim, args.size)
+    cfg.solver_config.precision = "mixed"
+    compute, timestep, nc, sn, h, nn, gd, Ud = sim.setup(cfg)
+    U0, P0 = tg_initial(nc.cpu().numpy())
+    dt, rho, mu = 1e-3, 1.0, 0.01
+    dev = torch.device("cuda", torch.cuda.current_device())
+    U, P = torch.as_tensor(U0, device=dev), torch.as_tensor(P0, device=dev)
+    Fp, F = compute(Ud, None, 0.0, dt)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        U, P, ui, pi = timestep(U, P, dt, rho, mu, Ud, Fp, F)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ms, cycles = 0.0, []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        U, P, ui, pi = timestep(U, P, dt, rho, mu, Ud, Fp, F)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        cycles.append(int(pi))
+    nsteps = args.warmup + args.steps
+    rel = lambda a, b: float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    Uf, Pf = fp64_final
+    Ua = torch.as_tensor(U0, device=dev) * np.exp(-2 * mu * nsteps * dt)
+    return {"workload": "the same Taylor-Green workload, mixed-precision pressure solve",
+            "steps_per_s": args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+            "pressure_cycles_mean": float(np.mean(cycles)),
+            "pressure_solve": "FP64 refinement to 1e-8, 4 FP32 Chebyshev-multigrid PCG iterations per cycle",
+            "momentum_solve": "FP64 (as the plain step)",
+            "steps_compared": nsteps,
+            "rel_err_vs_fp64": {"U": rel(U, Uf), "P": rel(P, Pf)},
+            "rel_err_vs_analytic_velocity": {"fp64": rel(Uf, Ua), "mixed": rel(U, Ua)}}
 
 
 def _dist_device():
@@ -345,32 +393,46 @@ def poisson_sweep():
     return {f"poisson_{2 ** k}x{2 ** k}_q1": poisson(2 ** k) for k in range(4, 13)}
 
 
-def serving(count, steps):
+def serving(count, steps, plain_sample=128):
     """Request stream of independent wall-bounded solves (sizes uniform over
     32^2..256^2 Q1, viscosity log-uniform 1e-3..1e-1, Fourier initial velocity,
-    `steps` steps each): the plain path (one request at a time on the whole
-    device) against the continuous-batching server, saturated (all requests
-    at t = 0) and under Poisson arrivals at 50 % and 90 % of the saturated
-    throughput. Latency = completion - arrival (plain: service time)."""
+    `steps` steps each): the plain FP64 path (one request at a time on the
+    whole device; timed on the first `plain_sample` requests, whose sizes
+    follow the same distribution) against the continuous-batching server in
+    FP64, saturated (all requests at t = 0) and under Poisson arrivals at
+    50 %, 70 % and 90 % of the saturated throughput, and the server in mixed
+    precision (mixed pressure solve), saturated. Latency = completion -
+    arrival (plain: service time)."""
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")  # streams on separate hardware queues
     from jax_fem_cfd_b200.serving import Server, make_requests, run_plain
     reqs = make_requests(count, seed=0, steps=steps)
     srv = Server(keep_results=False)
     srv.prewarm(reqs)
     bad = lambda d: sum(1 for x in d if x["status"] != 0)
-    dp, plain = run_plain(reqs, srv)
+    sample = reqs[:min(plain_sample, count)]
+    dp, plain = run_plain(sample, srv)
     ds, fixed = srv.run(reqs, realtime=False)
     tune = srv.autotune(reqs)
     srv.prewarm(reqs)
     ds2, sat = srv.run(reqs, realtime=False)
-    out = {"workload": f"{count} requests x {steps} steps, Q1 {{32,64,128,256}}^2 wall-bounded, FP64",
-           "plain": dict(plain, failed=bad(dp)), "served_saturated_untuned": dict(fixed, failed=bad(ds)),
+    out = {"workload": f"{count} requests x {steps} steps, Q1 {{32,64,128,256}}^2 wall-bounded",
+           "plain": dict(plain, failed=bad(dp), sample=f"first {len(sample)} requests of the stream"),
+           "served_saturated_untuned": dict(fixed, failed=bad(ds)),
            "autotune": tune, "served_saturated": dict(sat, failed=bad(ds2)),
            "speedup_solves_per_s": sat["solves_per_s"] / plain["solves_per_s"]}
-    for frac in (0.5, 0.9):
+    for frac in (0.5, 0.7, 0.9):
         rate = frac * sat["solves_per_s"]
         dr, m = srv.run(make_requests(count, seed=0, steps=steps, rate=rate))
         out[f"served_poisson_{int(frac * 100)}pct"] = dict(m, arrival_rate_per_s=rate, failed=bad(dr))
+    del srv
+    import torch
+    torch.cuda.empty_cache()
+    mx = Server(keep_results=False, precision="mixed", share=tune["picked"])
+    mx.prewarm(reqs)
+    mx.run(reqs[:min(16, count)], realtime=False)  # graph builds of the mixed solves, once per pooled solver
+    dm, msat = mx.run(reqs, realtime=False)
+    out["served_saturated_mixed"] = dict(msat, failed=bad(dm))
+    out["speedup_mixed_solves_per_s"] = msat["solves_per_s"] / plain["solves_per_s"]
     return out
 
 
@@ -695,7 +757,7 @@ def main():
     ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse", "channel3d",
                                        "cavity"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
-    ap.add_argument("--requests", type=int, default=64, help="--only serving: requests in the stream")
+    ap.add_argument("--requests", type=int, default=1024, help="--only serving: requests in the stream")
     ap.add_argument("--request-steps", type=int, default=200, help="--only serving: steps per request")
     args = ap.parse_args()
     if args.only:
@@ -724,6 +786,10 @@ def main():
     extra = {}
     if not args.no_extra and rank == 0:
         extra = poisson_and_matvec(args)
+    mixed = None
+    if not args.no_extra and rank == 0 and world == 1:
+        mixed = tg_mixed(args, r["final"], r["coords"])
+    del r["final"]
     hbm, src = measured_peaks()
     K = args.steps
     ms_step = r["total_ms"] / K
@@ -767,6 +833,8 @@ def main():
         "clocks": r["clocks"],
         **extra,
     }
+    if mixed is not None:
+        line["mixed"] = dict(mixed, speedup_vs_fp64=mixed["steps_per_s"] / value)
     if rank == 0 and world == 1 and args.cpu_steps > 0:
         line["cpu_baseline"] = cpu_baseline(args.size, args.cpu_steps)
     if rank == 0:

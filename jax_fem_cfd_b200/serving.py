@@ -26,6 +26,10 @@ The request loop (`Server.run`) is continuous batching, not a queue:
   (fem_step4_graph: the chunk's steps with the request's dt and viscosity).
 - The CTA cap of a request can be picked by `Server.autotune`, which serves a
   short sample of the stream under a few caps and keeps the fastest.
+- precision="mixed" serves every request with the mixed-precision pressure
+  solve (FP64 refinement around FP32 multigrid-PCG, one CUDA graph with a
+  device-side loop per solve); its steps are launched directly (a step that
+  launches its own graph is not captured into a chunk graph).
 - A request's CTA share depends only on its mesh size, so its results are the
   same (bit for bit) alone and in any mix: the solver's reductions are
   deterministic for a given grid.
@@ -100,9 +104,10 @@ def make_requests(count, seed=0, sizes=SIZES, nu_range=(1e-3, 1e-1), steps=200, 
     return out
 
 
-def cavity_config(n):
+def cavity_config(n, precision="fp64"):
     """Wall-bounded unit square, Q1, all four faces Dirichlet (U_d = 0),
-    pinned pressure, MG-PCG (final mesh 4 x 4) at tol 1e-8."""
+    pinned pressure, MG-PCG (final mesh 4 x 4) at tol 1e-8; precision "mixed"
+    solves the pressure by FP64 refinement around FP32 multigrid-PCG."""
     from .setup import simulation as sim
     return sim.Config(mesh="simple", solver="standard",
                       mesh_config=sim.SimpleMeshConfig(num_elem=[n, n], domain_size=[1.0, 1.0], shape_func_ord=1,
@@ -110,15 +115,15 @@ def cavity_config(n):
                       solver_config=sim.StandardSolverConfig(dirichlet_faces=[0, 1, 2, 3], symmetry_faces=[],
                                                              outlet_faces=[], streamline_diff=False, solver_tol=1e-8,
                                                              set_zeroP=True, pressure_precond="multigrid",
-                                                             final_multigrid_mesh=[4, 4]))
+                                                             final_multigrid_mesh=[4, 4], precision=precision))
 
 
 class Slot:
     """Pooled device state of one mesh size: the solver and its buffers."""
 
-    def __init__(self, n):
+    def __init__(self, n, precision="fp64"):
         from .setup import simulation as sim
-        _, timestep, *_rest = sim.setup(cavity_config(n))
+        _, timestep, *_rest = sim.setup(cavity_config(n, precision))
         U_d = _rest[-1]
         self.n = n
         self.solver = timestep.solver
@@ -133,6 +138,13 @@ class Slot:
         self.P_host = torch.empty(nn, dtype=torch.float64).pin_memory()
         self.U0_host = torch.empty(2 * nn, dtype=torch.float64).pin_memory()
         self.status_host = torch.empty(2, dtype=torch.int32).pin_memory()
+        if precision == "mixed":
+            # the mixed pressure solve builds its FP32 hierarchy and its graph on
+            # first use (with a device synchronisation): do it here, not while serving
+            self.steps(0, 1, 1e-3, 1e-2, torch.cuda.current_stream())
+            torch.cuda.synchronize()
+            for b in self.U + self.P:
+                b.zero_()
 
     def set_ctas(self, ctas):
         cap = ctypes.c_int(0)
@@ -183,8 +195,9 @@ class Server:
     solver CTAs per SM, 148 on a B200); chunk: steps per queued chunk;
     hbm_reserve: bytes kept free when building a new solver."""
 
-    def __init__(self, share=37, chunk=10, hbm_reserve=2 << 30, keep_results=True, graphs=True):
+    def __init__(self, share=37, chunk=10, hbm_reserve=2 << 30, keep_results=True, graphs=True, precision="fp64"):
         self.share, self.chunk, self.hbm_reserve = share, chunk + (chunk & 1), hbm_reserve
+        self.precision = precision
         self.keep_results = keep_results
         self.graphs = graphs
         self.graph_error = None
@@ -197,7 +210,7 @@ class Server:
     def _new_slot(self, n):
         torch.cuda.synchronize()
         free0 = torch.cuda.mem_get_info()[0]
-        slot = Slot(n)
+        slot = Slot(n, self.precision)
         torch.cuda.synchronize()
         used = free0 - torch.cuda.mem_get_info()[0]
         self.footprint[n] = max(self.footprint.get(n, 0), used, 1 << 20)
