@@ -213,12 +213,16 @@ int fem_bicgstab_solve(fem_ctx* ctx, int ncomp, double alpha, const double* Ash,
                        double gamma, const double* C, const uint8_t* mask, const double* b, double* x, double tol,
                        double atol, int maxiter, int* iters, int* status, cudaStream_t stream);
 
-/* Precision of fem_step4's pressure solve on a hex8 multigrid context:
- * FEM_PRECISION_FP64 (default, the reference's FP64 CG) or FEM_PRECISION_MIXED
- * (fem_pressure_solve_mixed's scheme: FP64 refinement, `inner` FP32
- * multigrid-PCG iterations per cycle, at most max_cycles cycles; iters[1] of
- * fem_step4 then receives the cycle count). No reference counterpart: the
- * reference solves in FP64 only. */
+/* Precision of fem_step4's solves: FEM_PRECISION_FP64 (default, the
+ * reference's FP64 solvers) or FEM_PRECISION_MIXED. Mixed: the multigrid
+ * pressure solve is fem_pressure_solve_mixed's scheme (FP64 refinement,
+ * `inner` FP32 multigrid-PCG iterations per cycle, at most max_cycles cycles;
+ * iters[1] receives the cycle count), and on 2D meshes the momentum solve is
+ * FP64 refinement around 3 FP32 BiCGSTAB iterations per cycle with FP32 Gauss
+ * factors of the convection (iters[0] receives the cycle count). Each mixed
+ * solve is one CUDA graph with a device-side loop, so a mixed step cannot be
+ * captured (FEM_E_STATE on a capturing stream). Needs the multigrid pressure
+ * preconditioner. No reference counterpart: the reference solves in FP64 only. */
 #define FEM_PRECISION_FP64 0
 #define FEM_PRECISION_MIXED 1
 int fem_ctx_set_precision(fem_ctx* ctx, int precision, int inner, int max_cycles);

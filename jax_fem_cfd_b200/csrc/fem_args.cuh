@@ -132,6 +132,14 @@ int fem_mixed_poisson(const CgArgs& A, int grid, float* work, double* dwork, con
                       int inner, int max_cycles, int* cycles, double* relres, cudaStream_t s, MxGraphCache* gc,
                       cudaStream_t cap);
 
+// mixed-precision momentum solve of the 2D on-the-fly step (k_mixmom.cu)
+struct MixMom;
+int mixmom_create(MixMom** out, const FemGrid& g, int ncomp, int nq, int sms);
+void mixmom_destroy(MixMom* M);
+int mixmom_solve(MixMom* M, const FemQuadTab& qt, const double* fq64, const double* Kd, double cc,
+                 const uint8_t* mask, const double* b, double* x, double tol, int inner, int max_cycles,
+                 int* cycles, int* status, int sms, cudaStream_t s, cudaStream_t cs);
+
 int fem_coop_occupancy_cg(int* occ);
 int fem_coop_occupancy_bi(int* occ);
 int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s);

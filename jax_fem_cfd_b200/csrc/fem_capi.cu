@@ -96,6 +96,8 @@ static FemLattice lattice_of(const FemGrid& g) {
 
 
 #define FEM_FLAG_BOUNDARY_SKIPPED 0
+// FP32 BiCGSTAB iterations per refinement cycle of the mixed momentum solve
+#define FEM_MIXED_MOMENTUM_INNER 3
 
 struct CtxLevel {
   FemGrid g;
@@ -155,6 +157,7 @@ struct fem_ctx {
   MxGraphCache mxg;                   // its captured inner solve
   Mg3* mg3 = nullptr;                 // hex8 multigrid hierarchy and its solve graphs
   Mg3* mg2 = nullptr;                 // 2D hierarchy of the graph-driven mixed-precision solve (first use)
+  MixMom* mixmom = nullptr;           // the mixed-precision momentum solve of fem_step4 (2D, first use)
   int precision = FEM_PRECISION_FP64; // pressure solve of fem_step4
   int mx_inner = 6, mx_cycles = 10;   // its mixed-precision parameters
 };
@@ -282,6 +285,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
   if (c->mx64) cudaFree(c->mx64);
   mg3_destroy(c->mg3);
   mg3_destroy(c->mg2);
+  mixmom_destroy(c->mixmom);
   void* ptrs[] = {c->coords, c->wq, c->N, c->dN, c->Me, c->Le, c->Leoff, c->Ge, c->M, c->Ldiag, c->Kd,
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
@@ -1043,7 +1047,13 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   // 3. BiCGSTAB on (rho/dt) Me + theta (rho Ce + mu Le), identity rows on gamma_d (:20-28, :41)
   FEM_TRY(fem_launch_lincomb(nen * nen, rho / dt, c->Me, theta * mu, c->Le, c->Kd, s));
   stage_mark(c, s);
-  if (otf) {
+  if (otf && c->precision == FEM_PRECISION_MIXED && g.kind != FEM_HEX8) {
+    // FP64 refinement around FP32 BiCGSTAB iterations (k_mixmom.cu)
+    FEM_TRY(mg2_ready(c, s));  // the same capture check and private stream as the mixed pressure solve
+    if (!c->mixmom) FEM_TRY(mixmom_create(&c->mixmom, g, nd, c->nq, c->sms));
+    FEM_TRY(mixmom_solve(c->mixmom, c->qt, c->cvf, c->Kd, theta * rho, S.dmask, c->rhsU, c->Uhat, tol,
+                         FEM_MIXED_MOMENTUM_INNER, c->mx_cycles, iters, status, c->sms, s, c->cap_stream));
+  } else if (otf) {
     const MatCombo op{c->Kd, 1.0, nullptr, 0.0, 0, nullptr, 0.0};
     FEM_TRY(run_bicgstab(c, nd, op, S.dmask, c->rhsU, c->Uhat, tol, 0.0, 0, iters, status, s, c->cvf, theta * rho));
   } else {

@@ -163,3 +163,28 @@ def test_taylor_green_mixed_steps_match_the_oracle(_cuda):
                     np.asarray(P.cpu() if isinstance(P, torch.Tensor) else P)))
     (Um, Pm), (Uo, Po) = res
     assert rel(Um, Uo) < 1e-6 and rel(Pm, Po) < 1e-6, (rel(Um, Uo), rel(Pm, Po))
+
+
+@pytest.mark.gpu
+def test_cavity_mixed_steps_match_fp64(_cuda):
+    """The 64 x 64 quad4 lid-driven cavity (Dirichlet walls: the momentum
+    solve's identity rows) over 20 steps with both solves in mixed precision,
+    against the FP64 steps: within 1e-6, a few refinement cycles per solve."""
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    from jax_fem_cfd_b200.serving import cavity_config
+    out = []
+    for prec in ("fp64", "mixed"):
+        compute, timestep, nc, sn, h, nn, gd, Ud = gsim.setup(cavity_config(64, prec))
+        Ud = gsim.set_face_velocity(Ud, sn[2], gd, 1.0, nn, var=1)
+        U = torch.zeros(2 * nn, dtype=torch.float64, device="cuda")
+        P = torch.zeros(nn, dtype=torch.float64, device="cuda")
+        its = []
+        for s in range(20):
+            Fp, F = compute(Ud, None, s * 0.01, (s + 1) * 0.01)
+            U, P, ui, pi = timestep(U, P, 0.01, 1.0, 0.01, Ud, Fp, F)
+            its.append((int(ui), int(pi)))
+        assert int(timestep.solver.status.max()) == 0
+        out.append((U.cpu().numpy(), P.cpu().numpy(), its))
+    (Uf, Pf, _), (Um, Pm, im) = out
+    assert all(1 <= u <= 5 and 1 <= p <= 5 for u, p in im), im
+    assert rel(Um, Uf) < 1e-6 and rel(Pm, Pf) < 1e-6, (rel(Um, Uf), rel(Pm, Pf))
