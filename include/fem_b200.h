@@ -158,6 +158,15 @@ int fem_convection_build(fem_ctx* ctx, const double* U, double beta, const doubl
 int fem_ctau_tilde_build(fem_ctx* ctx, const double* U, const double* wq, const double* N, const double* Nderiv,
                          double* Ct, cudaStream_t stream);
 
+/* Vector-Jacobian product of the convection operator in its velocity:
+ * y = d/dU <a, Ce(U) b>, y (ndim*nn), for a, b of ncomp components (ncomp*nn,
+ * Ce acting on each) with the divergence weight beta (Ce of
+ * core/element_calc.py:165 conservative_convec_elem_calc). Ce is linear in U,
+ * so y does not depend on U. Deterministic (per-node sums in a fixed order).
+ * No reference counterpart: the reference gets it from jax.grad. */
+int fem_conv_vjp(fem_ctx* ctx, int ncomp, const double* a, const double* b, double beta, double* y,
+                 cudaStream_t stream);
+
 /* Per-element SUPG tau (core/element_calc.py:202 calculate_tau). */
 int fem_supg_tau(fem_ctx* ctx, const double* U, const double* Ce, const double* Ct, double D, double dt, double r,
                  const double* N, double* tau, cudaStream_t stream);

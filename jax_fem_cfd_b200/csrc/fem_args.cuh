@@ -114,6 +114,9 @@ int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double
                             cudaStream_t s);
 int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc,
                           double alpha, const double* Ash, const double* x, double* y, int grid, cudaStream_t s);
+// y = d/dU <a, Ce(U) b> over ncomp components of a and b (ge: ne * dim * nen scratch)
+int fem_launch_conv_vjp(const FemGrid& g, const FemQuadTab& qt, int ncomp, const double* a, const double* b,
+                        double beta, double* ge, double* y, cudaStream_t s);
 // hex8: the Gauss-point factors (32 per element, element-major) and
 // y = alpha Ash x + cc Ce x per component (3 components) from them
 int fem_launch_conv_factors3(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,

@@ -158,6 +158,7 @@ struct fem_ctx {
   Mg3* mg3 = nullptr;                 // hex8 multigrid hierarchy and its solve graphs
   Mg3* mg2 = nullptr;                 // 2D hierarchy of the graph-driven mixed-precision solve (first use)
   MixMom* mixmom = nullptr;           // the mixed-precision momentum solve of fem_step4 (2D, first use)
+  double* vjp = nullptr;              // per-element scratch of fem_conv_vjp (first use)
   int precision = FEM_PRECISION_FP64; // pressure solve of fem_step4
   int mx_inner = 6, mx_cycles = 10;   // its mixed-precision parameters
 };
@@ -290,7 +291,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
                   c->rhsU, c->Uhat, c->gPn, c->Ustar, c->rhsP, c->Ce, c->Ce2, c->Ct, c->Mt, c->Ek, c->tau,
-                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab, c->bs_cnt, c->bs_off, c->bs_list};
+                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab, c->bs_cnt, c->bs_off, c->bs_list, c->vjp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
@@ -1225,6 +1226,13 @@ extern "C" int fem_boundary_flux_noalloc(fem_ctx* c, const int32_t* bconn, const
   const FemBoundaryHash H{FEM_NOALLOC_SLOTS, sc->fe,   sc->keys, sc->cnt,
                           sc->off,           sc->slot, sc->list, c->flags + FEM_FLAG_BOUNDARY_SKIPPED};
   return fem_launch_boundary_hash(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, H, Fp, s);
+}
+
+extern "C" int fem_conv_vjp(fem_ctx* c, int ncomp, const double* a, const double* b, double beta, double* y,
+                            cudaStream_t s) {
+  if (!c || !a || !b || !y || ncomp < 1 || ncomp > c->ndim) return FEM_E_ARG;
+  if (!c->vjp) FEM_ALLOC(c->vjp, (size_t)c->g.ne * c->ndim * c->g.nen);
+  return fem_launch_conv_vjp(c->g, c->qt, ncomp, a, b, beta, c->vjp, y, s);
 }
 
 extern "C" int fem_scatter(const int64_t* idx, const double* vals, double value, int n, double* out,

@@ -788,6 +788,93 @@ int fem_launch_conv_apply3(const FemGrid& g, const FemQuadTab& qt, const double*
   return fem_after_launch("k_conv_apply3");
 }
 
+// ---------------------------------------------------- convection VJP ----
+// d/dU <a, Ce(U) b> (Ce of core/element_calc.py:165-185 acting on each of ncomp
+// components): per element and local node k,
+//   ge[e][d][k] = sum_q w_q (N_k(q) s_d(q) + beta dN_k/dx_d(q) t(q)),
+//   s_d = sum_c A_c d_d B_c,  t = sum_c A_c B_c,
+// A_c, B_c, d_d B_c being a_c, b_c and the derivatives of b_c at the Gauss point;
+// then each node sums its incident elements' entries in a fixed order.
+template <int KIND>
+__global__ void __launch_bounds__(256) k_conv_vjp_elem(FemGrid g, const __grid_constant__ FemQuadTab qt, int ncomp,
+                                                       const double* __restrict__ a, const double* __restrict__ b,
+                                                       double beta, double* __restrict__ ge) {
+  constexpr int NEN = KI<KIND>::NEN, DIM = KI<KIND>::DIM, NQ = (KIND == FEM_Q2_2D) ? 9 : (KIND == FEM_HEX8 ? 8 : 4);
+  const size_t nn = g.nn;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.ne; e += gridDim.x * blockDim.x) {
+    const int ex = e % g.nex, eyz = e / g.nex, ey = eyz % g.ney, ez = eyz / g.ney;
+    int nd[NEN];
+#pragma unroll
+    for (int k = 0; k < NEN; ++k) nd[k] = fem_elem_node(g, ex, ey, ez, k);
+    double out[DIM][NEN];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+      for (int k = 0; k < NEN; ++k) out[d][k] = 0.0;
+    for (int q = 0; q < NQ; ++q) {
+      double sd[DIM], t = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) sd[d] = 0.0;
+      for (int c = 0; c < ncomp; ++c) {
+        double Ac = 0.0, Bc = 0.0, dB[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dB[d] = 0.0;
+#pragma unroll
+        for (int k = 0; k < NEN; ++k) {
+          const double av = a[nd[k] + c * nn], bv = b[nd[k] + c * nn];
+          Ac += qt.N[q][k] * av;
+          Bc += qt.N[q][k] * bv;
+          dB[0] += qt.dx[q][k] * bv;
+          dB[1] += qt.dy[q][k] * bv;
+          if (DIM == 3) dB[DIM - 1] += qt.dz[q][k] * bv;
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) sd[d] += Ac * dB[d];
+        t += Ac * Bc;
+      }
+#pragma unroll
+      for (int k = 0; k < NEN; ++k) {
+        out[0][k] += qt.w[q] * (qt.N[q][k] * sd[0] + beta * qt.dx[q][k] * t);
+        out[1][k] += qt.w[q] * (qt.N[q][k] * sd[1] + beta * qt.dy[q][k] * t);
+        if (DIM == 3) out[DIM - 1][k] += qt.w[q] * (qt.N[q][k] * sd[DIM - 1] + beta * qt.dz[q][k] * t);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+      for (int k = 0; k < NEN; ++k) ge[((size_t)e * DIM + d) * NEN + k] = out[d][k];
+  }
+}
+template <int KIND>
+__global__ void __launch_bounds__(256) k_conv_vjp_gather(FemGrid g, const double* __restrict__ ge,
+                                                         double* __restrict__ y) {
+  constexpr int NEN = KI<KIND>::NEN, DIM = KI<KIND>::DIM;
+  const size_t nn = g.nn;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    fem_ij(g, n, ix, iy, iz);
+    double v[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = 0.0;
+    fem_incident_k<KIND>(g, ix, iy, iz, [&](int, int, int, int e, int k) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) v[d] += ge[((size_t)e * DIM + d) * NEN + k];
+    });
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) y[n + d * nn] = v[d];
+  }
+}
+
+int fem_launch_conv_vjp(const FemGrid& g, const FemQuadTab& qt, int ncomp, const double* a, const double* b,
+                        double beta, double* ge, double* y, cudaStream_t s) {
+  const int be = fem_nblocks(g.ne, 256), bn = fem_nblocks(g.nn, 256);
+  FEM_KIND_DISPATCH(g.kind, KIND, {
+    k_conv_vjp_elem<KIND><<<be, 256, 0, s>>>(g, qt, ncomp, a, b, beta, ge);
+    k_conv_vjp_gather<KIND><<<bn, 256, 0, s>>>(g, ge, y);
+  });
+  return fem_after_launch("k_conv_vjp");
+}
+
 // Self-test of the grid barrier's time limit: one CTA waits at a counter
 // barrier for one more party than the launch has, so the wait can only end
 // through the FEM_BARRIER_TIMEOUT_NS limit. It then sets FEM_ERR_BARRIER_TIMEOUT

@@ -165,9 +165,12 @@ def _ebe(solver, x, alpha, A, beta=0.0, B=None, transB=0, ncomp=None):
 
 
 def conv_vjp_u(solver, nconn, a, b, beta):
-    """d/dU <a, Ce(U) b> (a, b: ndim*nn vectors, Ce acting on each component)."""
-    wq, N, Nd = solver.ctx.element_data()[:3]
-    return conv_vjp_u_elements(wq, N, Nd, solver.ndim, solver.nn, nconn, a, b, beta)
+    """d/dU <a, Ce(U) b> (a, b: ndim*nn vectors, Ce acting on each component),
+    by fem_conv_vjp (conv_vjp_u_elements is its torch restatement)."""
+    a, b = a.detach().contiguous(), b.detach().contiguous()
+    y = torch.empty(solver.ndim * solver.nn, dtype=torch.float64, device=a.device)
+    _lib.call("fem_conv_vjp", solver.ctx.handle, solver.ndim, ptr(a), ptr(b), float(beta), ptr(y), stream())
+    return y
 
 
 def conv_vjp_u_elements(wq, N, Nd, nd, nn, nconn, a, b, beta):

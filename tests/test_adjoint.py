@@ -331,3 +331,35 @@ def test_deferred_status_raises_when_the_block_ends(cavity):
     with deferred_status():
         U, P = Projection.apply(good, solver, 0.01, 1.0, ud, None, 1e-13)
     assert torch.isfinite(U).all() and torch.isfinite(P).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["q1", "q2_periodic", "hex8"])
+def test_conv_vjp_kernel_matches_its_torch_restatement(kind):
+    """fem_conv_vjp (d/dU <a, Ce(U) b>, the velocity side of the step adjoint)
+    against conv_vjp_u_elements, the torch restatement pinned to the oracle's
+    Ce on the CPU (tests/test_adjoint_elements.py)."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import Context, Mesh, ptr, stream
+    from jax_fem_cfd_b200.solvers.adjoint import conv_vjp_u_elements
+    from oracle import mesh as om
+    if kind == "q1":
+        mesh, nconn = Mesh(0, False, 7, 5, 1, 1.4, 1.0), om.create_mesh_2d(7, 5, 1.4, 1.0)[1]
+    elif kind == "q2_periodic":
+        mesh, nconn = (Mesh(1, True, 6, 4, 1, 2 * np.pi, 2 * np.pi),
+                       om.create_periodic_mesh_2d_quad9(6, 4, 2 * np.pi, 2 * np.pi)[1])
+    else:
+        mesh, nconn = Mesh(2, False, 4, 3, 3, 1.0, 0.75, 0.75), om.create_mesh_3d(4, 3, 3, 1.0, 0.75, 0.75)[1]
+    ctx = Context(mesh)
+    nd, nn = ctx.ndim, ctx.nn
+    rng = np.random.default_rng(17)
+    t = lambda a_: torch.as_tensor(a_, dtype=torch.float64, device="cuda")
+    a, b = t(rng.standard_normal(nd * nn)), t(rng.standard_normal(nd * nn))
+    y = torch.empty(nd * nn, dtype=torch.float64, device="cuda")
+    _lib.call("fem_conv_vjp", ctx.handle, nd, ptr(a), ptr(b), 0.5, ptr(y), stream())
+    wq, N, Nd = ctx.element_data()[:3]
+    ref = conv_vjp_u_elements(wq, N, Nd, nd, nn, torch.as_tensor(nconn).cuda(), a, b, 0.5)
+    err = float(torch.linalg.norm(y - ref) / torch.linalg.norm(ref))
+    assert err < 1e-13, err
