@@ -112,7 +112,7 @@ def _fp64_mean_zero(ctx, b):
     x = torch.zeros_like(bg)
     it = torch.zeros(1, dtype=torch.int32, device="cuda")
     st = torch.zeros(1, dtype=torch.int32, device="cuda")
-    _lib.call("fem_pressure_solve", ctx.handle, ptr(bg), ptr(x), 1e-12, 0.0, 1000, _lib.PREC["multigrid"], 1, 1,
+    _lib.call("fem_pressure_solve", ctx.handle, ptr(bg), ptr(x), 1e-10, 0.0, 1000, _lib.PREC["multigrid"], 1, 1,
               ptr(it), ptr(st), stream())
     torch.cuda.synchronize()
     assert int(st.item()) == 0
