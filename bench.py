@@ -569,7 +569,7 @@ def cavity(steps=200, warmup=3, cpu_steps=40):
                          "sample": f"first {cpu_steps} steps of the same workload, numpy oracle, 1 thread"}}}
 
 
-def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid", "multigrid_mixed")):
+def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid", "multigrid_mixed"), nx=256):
     """3D channel: hex8 256 x 64 x 64 on [0,4] x [0,1] x [0,1] (1,048,576
     elements, 1,090,625 nodes), parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
     zero-traction outlet (P = 0) on x = 4, no-slip walls, Re 200 (mu = 1/200,
@@ -579,9 +579,11 @@ def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid"
     Chebyshev degree 3; FP64), and the same multigrid as FP32 inner iterations
     inside FP64 refinement to 1e-8 ("multigrid_mixed", the configuration the
     workload names). One step = the boundary integral plus fem_step4; device
-    time with CUDA events, working set beyond L2 (Ce alone is 537 MB). Each
-    arm's final U and P are compared with the Jacobi arm's (FP64, same
-    tolerance)."""
+    time with CUDA events, working set beyond L2 (the Gauss factors of the
+    convection alone are 268 MB). Each arm's final U and P are compared with
+    the first arm's (FP64, same tolerance). nx < 256 runs the same channel on
+    nx x nx/4 x nx/4 elements (the multigrid still has 4 levels), for
+    profiling on a smaller case."""
     import torch
 
     from jax_fem_cfd_b200.setup import simulation as sim
@@ -591,11 +593,11 @@ def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid"
         prec, extra = pc, {}
         if pc.startswith("multigrid"):
             prec = "multigrid"
-            extra = {"final_multigrid_mesh": [32, 8, 8]}
+            extra = {"final_multigrid_mesh": [nx // 8, nx // 32, nx // 32]}
             if pc.endswith("mixed"):
                 extra["precision"] = "mixed"
         cfg = sim.Config(mesh="simple", solver="standard",
-                         mesh_config=sim.SimpleMeshConfig(num_elem=[256, 64, 64], domain_size=[4.0, 1.0, 1.0],
+                         mesh_config=sim.SimpleMeshConfig(num_elem=[nx, nx // 4, nx // 4], domain_size=[4.0, 1.0, 1.0],
                                                           shape_func_ord=1, periodic=False),
                          solver_config=sim.StandardSolverConfig(dirichlet_faces=[0, 2, 3, 4, 5], symmetry_faces=[],
                                                                 outlet_faces=[1], streamline_diff=False,
@@ -643,7 +645,7 @@ def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid"
         del compute, timestep, solver, bufs, nc, sn, gd, Ud
         torch.cuda.empty_cache()
     del ref
-    return {"channel3d_hex8_256x64x64": {
+    return {f"channel3d_hex8_{nx}x{nx // 4}x{nx // 4}": {
         "workload": "hex8 256x64x64 channel, parabolic inflow, outlet, Re 200, dt 2e-3, tol 1e-8, zero start",
         "timed_steps": steps, "warmup": warmup, **out}}
 
@@ -759,13 +761,17 @@ def main():
                                        "cavity"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=1024, help="--only serving: requests in the stream")
+    ap.add_argument("--channel-nx", type=int, default=256, help="--only channel3d: elements along x (y, z: nx / 4)")
+    ap.add_argument("--preconds", default="jacobi,approx_inv,multigrid,multigrid_mixed",
+                    help="--only channel3d: pressure solves to run")
     ap.add_argument("--request-steps", type=int, default=200, help="--only serving: steps per request")
     args = ap.parse_args()
     if args.only:
         fn = {"matvec": matvec, "poisson_sweep": poisson_sweep,
               "poisson": lambda: {f"poisson_{args.size}x{args.size}_q1": poisson(args.size)},
               "serving": lambda: serving(args.requests, args.request_steps), "inverse": inverse,
-              "channel3d": lambda: channel3d(args.steps), "cavity": cavity}[args.only]
+              "channel3d": lambda: channel3d(args.steps, preconds=tuple(args.preconds.split(",")),
+                                             nx=args.channel_nx), "cavity": cavity}[args.only]
         print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
