@@ -167,6 +167,28 @@ int fem_ctau_tilde_build(fem_ctx* ctx, const double* U, const double* wq, const 
 int fem_conv_vjp(fem_ctx* ctx, int ncomp, const double* a, const double* b, double beta, double* y,
                  cudaStream_t stream);
 
+/* The velocity-dependent element matrices of the passive-scalar step
+ * (solvers/passive_transport.py:80-88 feeding :14-62): the lhs operator is
+ * K_A + E_k and the rhs operator K_B + B_k with the shared K_A = Me/dt + (D/2) Le,
+ * K_B = Me/dt - (D/2) Le and
+ *   SUPG:  E_k = Mtau/dt + (Ce(U) + Ctau)/2,  B_k = Mtau/dt - (Ce(U_n) + Ctau)/2
+ *   plain: E_k = Ce(U)/2,                     B_k = -Ce(U_n)/2
+ * Ek, Bk: ne * nen * nen each, element-major; transpose != 0 writes each
+ * element's block transposed (what the adjoint's transposed solve applies). */
+int fem_transport_elements(fem_ctx* ctx, const double* U_n, const double* U, double dt, double D, int supg,
+                           int transpose, double* Ek, double* Bk, cudaStream_t stream);
+
+/* Velocity side of the adjoint of the passive-scalar step (2D): for
+ * s = <lam, B(U_n) phi_n - E(U_n, U) phi>, with E, B the step's lhs and rhs
+ * operators without their shared parts (solvers/passive_transport.py:14-97;
+ * SUPG with supg != 0: Ce(U), Ctau = tau Ct(U_n), Mtau = tau Ce(U_n)^T and tau
+ * of core/element_calc.py:165-229), gUn = ds/dU_n and gU = ds/dU (2*nn each).
+ * lam is the adjoint solve's solution with its Dirichlet rows zeroed. No
+ * reference counterpart: the reference gets it from jax.grad. */
+int fem_transport_vjp(fem_ctx* ctx, const double* U_n, const double* U, const double* lam, const double* phi_n,
+                      const double* phi, double dt, double D, int supg, double* gU_n, double* gU,
+                      cudaStream_t stream);
+
 /* Per-element SUPG tau (core/element_calc.py:202 calculate_tau). */
 int fem_supg_tau(fem_ctx* ctx, const double* U, const double* Ce, const double* Ct, double D, double dt, double r,
                  const double* N, double* tau, cudaStream_t stream);

@@ -43,6 +43,8 @@ SIGNATURES = {
     "fem_ctau_tilde_build": (c_int, [P, P, P, P, P, P, P]),
     "fem_supg_tau": (c_int, [P, P, P, P, c_double, c_double, c_double, P, P, P]),
     "fem_conv_vjp": (c_int, [P, c_int, P, P, c_double, P, P]),
+    "fem_transport_vjp": (c_int, [P, P, P, P, P, P, c_double, c_double, c_int, P, P, P]),
+    "fem_transport_elements": (c_int, [P, P, P, c_double, c_double, c_int, c_int, P, P, P]),
     "fem_element_matrices": (c_int, [c_int, c_int, c_int, P, P, P, P, P, P, P, P]),
     "fem_assemble_diag": (c_int, [P, P, P, c_int, P, P, P]),
     "fem_lattice_interpolate": (c_int, [c_int, c_int, c_int, c_int, c_int, P, P, P]),

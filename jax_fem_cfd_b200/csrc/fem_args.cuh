@@ -78,8 +78,9 @@ int fem_launch_convection(const FemGrid& g, const FemQuad& Q, const double* U, d
 int fem_launch_supg_tau(const FemGrid& g, const FemQuad& Q, const double* U, const double* Ce, const double* Ct,
                         double D, double dt, double r, double* tau, cudaStream_t s);
 int fem_launch_scale_elem(int ne, int nen, const double* tau, const double* X, int trans, double* out, cudaStream_t s);
+// out = s_m Mt + s_c (C + Ct); transpose_nen = nen writes each element block transposed, 0 as is
 int fem_launch_elem_combine(size_t n, double s_m, const double* Mt, double s_c, const double* C, const double* Ct,
-                            double* out, cudaStream_t s);
+                            double* out, int transpose_nen, cudaStream_t s);
 int fem_launch_lincomb(int n, double a, const double* X, double b, const double* Y, double* out, cudaStream_t s);
 int fem_launch_interp(const FemLattice& H, const FemLattice& h, const double* xH, double* xh, cudaStream_t s);
 int fem_launch_restrict(const FemLattice& h, const FemLattice& H, const double* xh, double* xH, cudaStream_t s);
@@ -117,6 +118,11 @@ int fem_launch_conv_apply(int ncomp, const FemGrid& g, const FemQuadTab& qt, con
 // y = d/dU <a, Ce(U) b> over ncomp components of a and b (ge: ne * dim * nen scratch)
 int fem_launch_conv_vjp(const FemGrid& g, const FemQuadTab& qt, int ncomp, const double* a, const double* b,
                         double beta, double* ge, double* y, cudaStream_t s);
+// velocity side of the passive-scalar step's adjoint (2D): yn = ds/dU_n, yu = ds/dU
+// (ge*: ne * 2 * nen scratch each)
+int fem_launch_transport_vjp(const FemGrid& g, const FemQuadTab& qt, const double* Un, const double* U,
+                             const double* lam, const double* phin, const double* phi, double dt, double D, int supg,
+                             double* gen, double* geu, double* yn, double* yu, cudaStream_t s);
 // hex8: the Gauss-point factors (32 per element, element-major) and
 // y = alpha Ash x + cc Ce x per component (3 components) from them
 int fem_launch_conv_factors3(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,

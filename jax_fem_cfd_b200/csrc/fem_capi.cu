@@ -159,6 +159,7 @@ struct fem_ctx {
   Mg3* mg2 = nullptr;                 // 2D hierarchy of the graph-driven mixed-precision solve (first use)
   MixMom* mixmom = nullptr;           // the mixed-precision momentum solve of fem_step4 (2D, first use)
   double* vjp = nullptr;              // per-element scratch of fem_conv_vjp (first use)
+  double* vjp2 = nullptr;             // per-element scratch of fem_transport_vjp (first use)
   int precision = FEM_PRECISION_FP64; // pressure solve of fem_step4
   int mx_inner = 6, mx_cycles = 10;   // its mixed-precision parameters
 };
@@ -291,7 +292,7 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
                   c->rhsU, c->Uhat, c->gPn, c->Ustar, c->rhsP, c->Ce, c->Ce2, c->Ct, c->Mt, c->Ek, c->tau,
-                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab, c->bs_cnt, c->bs_off, c->bs_list, c->vjp};
+                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab, c->bs_cnt, c->bs_off, c->bs_list, c->vjp, c->vjp2};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
@@ -1091,11 +1092,40 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   return FEM_OK;
 }
 
+static int transport_mats(fem_ctx* c, const double* Un, const double* U, double dt, double D, int supg,
+                          cudaStream_t s);
+
 extern "C" int fem_transport_phi(fem_ctx* c, const double* Un, const double* U, const double* phin, double dt,
                                  double D, int supg, const uint8_t* phi_mask, const double* phid, double tol,
                                  double* phio, int* iters, int* status, cudaStream_t s) {
   if (!c || !Un || !U || !phin || !phio || !iters || !status) return FEM_E_ARG;
   if (phi_mask && !phid) return FEM_E_ARG;
+  const FemGrid& g = c->g;
+  const size_t ntot = (size_t)g.ne * g.nen * g.nen;
+  FEM_TRY(transport_mats(c, Un, U, dt, D, supg, s));
+  // rhs and x0 (solvers/passive_transport.py:26-33 / :50-57)
+  FEM_TRY(fem_launch_phi_rhs(g, c->Me, c->Le, dt, D, c->Mt, c->Ce, c->Ct, phin, phi_mask, phid, c->rhsP, phio, s));
+  // lhs: [(1/dt) Me + 0.5 D Le] + [(1/dt) Mtau + 0.5 (Ce + Ctau)]
+  FEM_TRY(fem_launch_lincomb(g.nen * g.nen, 1.0 / dt, c->Me, 0.5 * D, c->Le, c->Kd, s));
+  FEM_TRY(fem_launch_elem_combine(ntot, 1.0 / dt, c->Mt, 0.5, c->Ce2, c->Ct, c->Ek, 0, s));
+  const MatCombo op{c->Kd, 1.0, c->Ek, 1.0, 0, nullptr, 0.0};
+  return run_bicgstab(c, 1, op, phi_mask, c->rhsP, phio, tol, 0.0, 0, iters, status, s);
+}
+
+extern "C" int fem_transport_elements(fem_ctx* c, const double* Un, const double* U, double dt, double D, int supg,
+                                      int transpose, double* Ek, double* Bk, cudaStream_t s) {
+  if (!c || !Un || !U || !Ek || !Bk) return FEM_E_ARG;
+  const size_t ntot = (size_t)c->g.ne * c->g.nen * c->g.nen;
+  FEM_TRY(transport_mats(c, Un, U, dt, D, supg, s));
+  FEM_TRY(fem_launch_elem_combine(ntot, 1.0 / dt, c->Mt, 0.5, c->Ce2, c->Ct, Ek, transpose ? c->g.nen : 0, s));
+  return fem_launch_elem_combine(ntot, 1.0 / dt, c->Mt, -0.5, c->Ce, c->Ct, Bk, transpose ? c->g.nen : 0, s);
+}
+
+// Element matrices of the passive-scalar step into the context: Ce = Ce(U_n, 1),
+// Ce2 = Ce(U, 1), and with SUPG Ct = tau Ct(U_n), Mt = tau Ce(U_n)^T (both zero
+// without it).
+static int transport_mats(fem_ctx* c, const double* Un, const double* U, double dt, double D, int supg,
+                          cudaStream_t s) {
   const FemGrid& g = c->g;
   const size_t per = (size_t)g.nen * g.nen, ntot = (size_t)g.ne * per;
   if (!c->Ce2) {
@@ -1119,13 +1149,7 @@ extern "C" int fem_transport_phi(fem_ctx* c, const double* Un, const double* U, 
     FEM_CHECK(cudaMemsetAsync(c->Ct, 0, ntot * sizeof(double), s));
     FEM_CHECK(cudaMemsetAsync(c->Mt, 0, ntot * sizeof(double), s));
   }
-  // rhs and x0 (solvers/passive_transport.py:26-33 / :50-57)
-  FEM_TRY(fem_launch_phi_rhs(g, c->Me, c->Le, dt, D, c->Mt, c->Ce, c->Ct, phin, phi_mask, phid, c->rhsP, phio, s));
-  // lhs: [(1/dt) Me + 0.5 D Le] + [(1/dt) Mtau + 0.5 (Ce + Ctau)]
-  FEM_TRY(fem_launch_lincomb(g.nen * g.nen, 1.0 / dt, c->Me, 0.5 * D, c->Le, c->Kd, s));
-  FEM_TRY(fem_launch_elem_combine(ntot, 1.0 / dt, c->Mt, 0.5, c->Ce2, c->Ct, c->Ek, s));
-  const MatCombo op{c->Kd, 1.0, c->Ek, 1.0, 0, nullptr, 0.0};
-  return run_bicgstab(c, 1, op, phi_mask, c->rhsP, phio, tol, 0.0, 0, iters, status, s);
+  return FEM_OK;
 }
 
 extern "C" int fem_boundary_flux(fem_ctx* c, const int32_t* bconn, const double* nvec, int nb, int npf,
@@ -1233,6 +1257,17 @@ extern "C" int fem_conv_vjp(fem_ctx* c, int ncomp, const double* a, const double
   if (!c || !a || !b || !y || ncomp < 1 || ncomp > c->ndim) return FEM_E_ARG;
   if (!c->vjp) FEM_ALLOC(c->vjp, (size_t)c->g.ne * c->ndim * c->g.nen);
   return fem_launch_conv_vjp(c->g, c->qt, ncomp, a, b, beta, c->vjp, y, s);
+}
+
+extern "C" int fem_transport_vjp(fem_ctx* c, const double* Un, const double* U, const double* lam,
+                                 const double* phin, const double* phi, double dt, double D, int supg, double* gUn,
+                                 double* gU, cudaStream_t s) {
+  if (!c || !Un || !U || !lam || !phin || !phi || !gUn || !gU) return FEM_E_ARG;
+  if (c->g.kind == FEM_HEX8) return FEM_E_STATE;
+  if (!c->vjp2) FEM_ALLOC(c->vjp2, (size_t)2 * c->g.ne * c->ndim * c->g.nen);
+  const size_t half = (size_t)c->g.ne * c->ndim * c->g.nen;
+  return fem_launch_transport_vjp(c->g, c->qt, Un, U, lam, phin, phi, dt, D, supg, c->vjp2, c->vjp2 + half, gUn, gU,
+                                  s);
 }
 
 extern "C" int fem_scatter(const int64_t* idx, const double* vals, double value, int n, double* out,

@@ -350,10 +350,19 @@ __global__ void k_scale_elem(int ne, int nen, const double* __restrict__ tau, co
 }
 
 // out = s_m * Mt + s_c * (C + Ct)   (per element, flat)
+// out = s_m Mt + s_c (C + Ct) per element entry; with tn = nen > 0 each element's
+// nen x nen block is written transposed
 __global__ void k_elem_combine(size_t n, double s_m, const double* __restrict__ Mt, double s_c,
-                               const double* __restrict__ C, const double* __restrict__ Ct, double* __restrict__ out) {
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-    out[t] = s_m * Mt[t] + s_c * (C[t] + Ct[t]);
+                               const double* __restrict__ C, const double* __restrict__ Ct, int tn,
+                               double* __restrict__ out) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    size_t o = t;
+    if (tn > 0) {
+      const size_t per = (size_t)tn * tn, e = t / per, ab = t % per;
+      o = e * per + (ab % tn) * tn + ab / tn;
+    }
+    out[o] = s_m * Mt[t] + s_c * (C[t] + Ct[t]);
+  }
 }
 
 // y = alpha S x for an assembled stencil table S (fem_stencil.cuh), one tile of
@@ -543,8 +552,8 @@ int fem_launch_scale_elem(int ne, int nen, const double* tau, const double* X, i
   return fem_after_launch("k_scale_elem");
 }
 int fem_launch_elem_combine(size_t n, double s_m, const double* Mt, double s_c, const double* C, const double* Ct,
-                            double* out, cudaStream_t s) {
-  k_elem_combine<<<fem_nblocks((long long)n, 256), 256, 0, s>>>(n, s_m, Mt, s_c, C, Ct, out);
+                            double* out, int transpose_nen, cudaStream_t s) {
+  k_elem_combine<<<fem_nblocks((long long)n, 256), 256, 0, s>>>(n, s_m, Mt, s_c, C, Ct, transpose_nen, out);
   return fem_after_launch("k_elem_combine");
 }
 int fem_launch_lincomb(int n, double a, const double* X, double b, const double* Y, double* out, cudaStream_t s) {
@@ -863,6 +872,169 @@ __global__ void __launch_bounds__(256) k_conv_vjp_gather(FemGrid g, const double
 #pragma unroll
     for (int d = 0; d < DIM; ++d) y[n + d * nn] = v[d];
   }
+}
+
+// ------------------------------------------------------- transport VJP ----
+// Velocity side of the passive-scalar step's adjoint (solvers/passive_transport.py:
+// 14-97 with the matrices of :80-88): for s = sum_e lam_e^T (B(U_n) phi_n - E(U_n, U) phi)_e,
+// ge_n = ds/dU_n and ge_u = ds/dU per element and local node, with
+//   E = Mtau/dt + (Ce(U) + Ctau)/2,  B = Mtau/dt - (Ce(U_n) + Ctau)/2   (SUPG)
+//   E = Ce(U)/2,                     B = -Ce(U_n)/2                     (plain)
+// Ce with beta = 1 (core/element_calc.py:165-185), Ct = sum_q w dN^T (u u^T) dN
+// (:188-200), tau the r = 2 blend of ce = |Ce(U)|_F, kt = |Ct|_F and the mean
+// |u|^2 over the Gauss points (:202-229), Ctau = tau Ct, Mtau = tau Ce(U_n)^T.
+// The derivative goes through the element matrices: with G = ds/d(matrix),
+// <G, Ce(V)> and <G, Ct(u)> are differentiated at the Gauss points and
+// interpolated back to the nodes.
+template <int KIND>
+__global__ void __launch_bounds__(128) k_transport_vjp_elem(FemGrid g, const __grid_constant__ FemQuadTab qt,
+                                                            const double* __restrict__ Un, const double* __restrict__ U,
+                                                            const double* __restrict__ lam,
+                                                            const double* __restrict__ phin,
+                                                            const double* __restrict__ phi, double dt, double D,
+                                                            int supg, double* __restrict__ gen,
+                                                            double* __restrict__ geu) {
+  constexpr int NEN = KI<KIND>::NEN, NQ = (KIND == FEM_Q2_2D) ? 9 : 4;
+  const size_t nn = g.nn;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.ne; e += gridDim.x * blockDim.x) {
+    const int ex = e % g.nex, ey = e / g.nex;
+    int nd[NEN];
+    double l[NEN], fn[NEN], f[NEN], un[2][NEN], uu[2][NEN];
+#pragma unroll
+    for (int k = 0; k < NEN; ++k) {
+      nd[k] = fem_elem_node(g, ex, ey, 0, k);
+      l[k] = lam[nd[k]];
+      fn[k] = phin[nd[k]];
+      f[k] = phi[nd[k]];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        un[c][k] = Un[nd[k] + c * nn];
+        uu[c][k] = U[nd[k] + c * nn];
+      }
+    }
+    // the element matrices of the step
+    double Cn[NEN][NEN], Cu[NEN][NEN], Ct[NEN][NEN];
+    for (int a = 0; a < NEN; ++a)
+      for (int b = 0; b < NEN; ++b) Cn[a][b] = Cu[a][b] = Ct[a][b] = 0.0;
+    double un2 = 0.0;
+    for (int q = 0; q < NQ; ++q) {
+      double vn[2] = {0.0, 0.0}, vu[2] = {0.0, 0.0}, divn = 0.0, divu = 0.0;
+      for (int k = 0; k < NEN; ++k) {
+        for (int c = 0; c < 2; ++c) {
+          vn[c] += qt.N[q][k] * un[c][k];
+          vu[c] += qt.N[q][k] * uu[c][k];
+        }
+        divn += qt.dx[q][k] * un[0][k] + qt.dy[q][k] * un[1][k];
+        divu += qt.dx[q][k] * uu[0][k] + qt.dy[q][k] * uu[1][k];
+      }
+      un2 += vn[0] * vn[0] + vn[1] * vn[1];
+      const double w = qt.w[q];
+      for (int a = 0; a < NEN; ++a)
+        for (int b = 0; b < NEN; ++b) {
+          const double na = qt.N[q][a], nb = qt.N[q][b];
+          Cn[a][b] += w * na * ((vn[0] * qt.dx[q][b] + vn[1] * qt.dy[q][b]) + divn * nb);
+          Cu[a][b] += w * na * ((vu[0] * qt.dx[q][b] + vu[1] * qt.dy[q][b]) + divu * nb);
+          const double ga = qt.dx[q][a] * vn[0] + qt.dy[q][a] * vn[1], gb = qt.dx[q][b] * vn[0] + qt.dy[q][b] * vn[1];
+          Ct[a][b] += w * ga * gb;
+        }
+    }
+    un2 /= NQ;
+    // G = ds/d(matrix): Gu for Ce(U), Gn for Ce(U_n), Gt for Ct; gu2 for the mean |u|^2
+    double Gu[NEN][NEN], Gn[NEN][NEN], Gt[NEN][NEN], gu2 = 0.0;
+    for (int a = 0; a < NEN; ++a)
+      for (int b = 0; b < NEN; ++b) {
+        Gu[a][b] = -0.5 * l[a] * f[b];
+        Gn[a][b] = -0.5 * l[a] * fn[b];
+        Gt[a][b] = 0.0;
+      }
+    if (supg) {
+      double ce = 0.0, kt = 0.0, sCnT = 0.0, sCt = 0.0;
+      for (int a = 0; a < NEN; ++a)
+        for (int b = 0; b < NEN; ++b) {
+          ce += Cu[a][b] * Cu[a][b];
+          kt += Ct[a][b] * Ct[a][b];
+          sCnT += (fn[a] - f[a]) * Cn[a][b] * l[b];  // lam^T Cn^T (phi_n - phi)
+          sCt += l[a] * Ct[a][b] * (fn[b] + f[b]);
+        }
+      ce = sqrt(ce);
+      kt = sqrt(kt);
+      const double De = D + 1e-6, c = dt / 2;
+      const double t1 = ce / kt, t3 = t1 * (un2 * ce) / (De * kt);
+      const double tau = 1.0 / sqrt(1.0 / (t1 * t1) + 1.0 / (c * c) + 1.0 / (t3 * t3));
+      // d tau = tau^3 (t1^-3 d t1 + t3^-3 d t3), t1 = ce / kt, t3 = un2 ce^2 / (De kt^2)
+      const double tau3 = tau * tau * tau, i1 = 1.0 / (t1 * t1 * t1), i3 = 1.0 / (t3 * t3 * t3);
+      const double dce = tau3 * (i1 / kt + i3 * 2.0 * un2 * ce / (De * kt * kt));
+      const double dkt = tau3 * (-i1 * ce / (kt * kt) - i3 * 2.0 * un2 * ce * ce / (De * kt * kt * kt));
+      const double dun2 = tau3 * i3 * ce * ce / (De * kt * kt);
+      const double gtau = sCnT / dt - 0.5 * sCt;
+      for (int a = 0; a < NEN; ++a)
+        for (int b = 0; b < NEN; ++b) {
+          Gu[a][b] += gtau * dce * Cu[a][b] / ce;
+          Gn[a][b] += (tau / dt) * (fn[a] - f[a]) * l[b];
+          Gt[a][b] = -0.5 * tau * l[a] * (fn[b] + f[b]) + gtau * dkt * Ct[a][b] / kt;
+        }
+      gu2 = gtau * dun2;
+    }
+    // back to the nodes
+    double on[2][NEN], ou[2][NEN];
+    for (int c = 0; c < 2; ++c)
+      for (int k = 0; k < NEN; ++k) on[c][k] = ou[c][k] = 0.0;
+    for (int q = 0; q < NQ; ++q) {
+      const double w = qt.w[q];
+      double vn[2] = {0.0, 0.0};
+      for (int k = 0; k < NEN; ++k) {
+        vn[0] += qt.N[q][k] * un[0][k];
+        vn[1] += qt.N[q][k] * un[1][k];
+      }
+      double Su[2] = {0.0, 0.0}, Tu = 0.0, Sn[2] = {0.0, 0.0}, Tn = 0.0, Gq[2] = {0.0, 0.0};
+      for (int a = 0; a < NEN; ++a) {
+        const double na = qt.N[q][a], ga = qt.dx[q][a] * vn[0] + qt.dy[q][a] * vn[1];
+        for (int b = 0; b < NEN; ++b) {
+          const double nb = qt.N[q][b], dxb = qt.dx[q][b], dyb = qt.dy[q][b];
+          Su[0] += Gu[a][b] * na * dxb;
+          Su[1] += Gu[a][b] * na * dyb;
+          Tu += Gu[a][b] * na * nb;
+          Sn[0] += Gn[a][b] * na * dxb;
+          Sn[1] += Gn[a][b] * na * dyb;
+          Tn += Gn[a][b] * na * nb;
+          if (supg) {
+            const double gb = dxb * vn[0] + dyb * vn[1];
+            Gq[0] += Gt[a][b] * (qt.dx[q][a] * gb + ga * dxb);
+            Gq[1] += Gt[a][b] * (qt.dy[q][a] * gb + ga * dyb);
+          }
+        }
+      }
+      for (int k = 0; k < NEN; ++k) {
+        const double nk = qt.N[q][k];
+        ou[0][k] += w * (nk * Su[0] + qt.dx[q][k] * Tu);
+        ou[1][k] += w * (nk * Su[1] + qt.dy[q][k] * Tu);
+        on[0][k] += w * (nk * Sn[0] + qt.dx[q][k] * Tn) + nk * (w * Gq[0] + gu2 * 2.0 * vn[0] / NQ);
+        on[1][k] += w * (nk * Sn[1] + qt.dy[q][k] * Tn) + nk * (w * Gq[1] + gu2 * 2.0 * vn[1] / NQ);
+      }
+    }
+    for (int c = 0; c < 2; ++c)
+      for (int k = 0; k < NEN; ++k) {
+        gen[((size_t)e * 2 + c) * NEN + k] = on[c][k];
+        geu[((size_t)e * 2 + c) * NEN + k] = ou[c][k];
+      }
+  }
+}
+
+int fem_launch_transport_vjp(const FemGrid& g, const FemQuadTab& qt, const double* Un, const double* U,
+                             const double* lam, const double* phin, const double* phi, double dt, double D, int supg,
+                             double* gen, double* geu, double* yn, double* yu, cudaStream_t s) {
+  if (g.kind == FEM_HEX8) return FEM_E_ARG;
+  const int be = fem_nblocks(g.ne, 128), bn = fem_nblocks(g.nn, 256);
+  if (g.kind == FEM_Q1_2D) {
+    k_transport_vjp_elem<FEM_Q1_2D><<<be, 128, 0, s>>>(g, qt, Un, U, lam, phin, phi, dt, D, supg, gen, geu);
+    k_conv_vjp_gather<FEM_Q1_2D><<<bn, 256, 0, s>>>(g, gen, yn);
+    k_conv_vjp_gather<FEM_Q1_2D><<<bn, 256, 0, s>>>(g, geu, yu);
+  } else {
+    k_transport_vjp_elem<FEM_Q2_2D><<<be, 128, 0, s>>>(g, qt, Un, U, lam, phin, phi, dt, D, supg, gen, geu);
+    k_conv_vjp_gather<FEM_Q2_2D><<<bn, 256, 0, s>>>(g, gen, yn);
+    k_conv_vjp_gather<FEM_Q2_2D><<<bn, 256, 0, s>>>(g, geu, yu);
+  }
+  return fem_after_launch("k_transport_vjp");
 }
 
 int fem_launch_conv_vjp(const FemGrid& g, const FemQuadTab& qt, int ncomp, const double* a, const double* b,

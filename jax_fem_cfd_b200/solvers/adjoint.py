@@ -166,30 +166,11 @@ def _ebe(solver, x, alpha, A, beta=0.0, B=None, transB=0, ncomp=None):
 
 def conv_vjp_u(solver, nconn, a, b, beta):
     """d/dU <a, Ce(U) b> (a, b: ndim*nn vectors, Ce acting on each component),
-    by fem_conv_vjp (conv_vjp_u_elements is its torch restatement)."""
+    by fem_conv_vjp."""
     a, b = a.detach().contiguous(), b.detach().contiguous()
     y = torch.empty(solver.ndim * solver.nn, dtype=torch.float64, device=a.device)
     _lib.call("fem_conv_vjp", solver.ctx.handle, solver.ndim, ptr(a), ptr(b), float(beta), ptr(y), stream())
     return y
-
-
-def conv_vjp_u_elements(wq, N, Nd, nd, nn, nconn, a, b, beta):
-    """conv_vjp_u on explicit element data (wq (nq[, 1]), N (nq, nen), Nd
-    (nq, nd, nen) of a uniform mesh, nconn (ne, nen) int64)."""
-    w = wq.reshape(-1)
-    ae = a.view(nd, nn)[:, nconn]  # (c, e, i)
-    be = b.view(nd, nn)[:, nconn]
-    A = torch.einsum("qi,cei->ceq", N, ae)
-    B = torch.einsum("qi,cei->ceq", N, be)
-    dB = torch.einsum("qdi,cei->ceqd", Nd, be)
-    s_ = torch.einsum("ceq,ceqd->eqd", A, dB)
-    t_ = torch.einsum("ceq,ceq->eq", A, B)
-    ge = torch.einsum("q,qk,eqd->edk", w, N, s_) + beta * torch.einsum("q,qdk,eq->edk", w, Nd, t_)
-    out = torch.zeros(nd, nn, dtype=torch.float64, device=a.device)
-    idx = nconn.reshape(-1)
-    for d in range(nd):
-        out[d].index_add_(0, idx, ge[:, d, :].reshape(-1))
-    return out.reshape(-1)
 
 
 def _bicgstab(solver, Ksh, beta, B, mask, rhs, tol, ncomp=None):
@@ -302,50 +283,37 @@ class Step(torch.autograd.Function):
         return gUn, gPn, None, None, None, None, None, None, None
 
 
-def transport_elements(solver, nconn, Un, U, dt, D, supg):
-    """(E_k, B_k): the per-element parts of the transport step's operators as
-    differentiable torch functions of U_n and U (solvers/passive_transport.py:
-    14-62 with the matrices of :80-88). The lhs is A = K_A + E_k and the rhs
-    operator B = K_B + B_k, with the shared K_A = Me/dt + (D/2) Le and
-    K_B = Me/dt - (D/2) Le. With SUPG:
+def transport_elements(solver, Un, U, dt, D, supg, transpose=False):
+    """(E_k, B_k), (ne, nen, nen) each: the per-element parts of the transport
+    step's operators (solvers/passive_transport.py:14-62 with the matrices of
+    :80-88), built on the device by fem_transport_elements. The lhs is
+    A = K_A + E_k and the rhs operator B = K_B + B_k, with the shared
+    K_A = Me/dt + (D/2) Le and K_B = Me/dt - (D/2) Le. With SUPG:
         E_k = Mtau/dt + (Ce(U) + Ctau)/2,   B_k = Mtau/dt - (Ce(U_n) + Ctau)/2,
         Ctau = tau Ct(U_n),  Mtau = tau Ce(U_n)^T,  tau = tau(U_n, Ce(U), Ct(U_n)),
     without it E_k = Ce(U)/2 and B_k = -Ce(U_n)/2; Ce has beta = 1
     (core/element_calc.py:165-185), Ct = sum_q w dN^T (u u^T) dN (:188-200),
-    tau the r = 2 blend of :202-229."""
-    wq, N, Nd = solver.ctx.element_data()[:3]
-    return transport_element_matrices(wq, N, Nd, solver.ndim, solver.nn, nconn, Un, U, dt, D, supg)
+    tau the r = 2 blend of :202-229. transpose=True returns each block
+    transposed."""
+    ctx = solver.ctx
+    nen = ctx.element_data()[3].shape[-1]
+    Un, U = (t.detach().to(torch.float64).contiguous() for t in (Un, U))
+    Ek = torch.empty(ctx.ne, nen, nen, dtype=torch.float64, device=Un.device)
+    Bk = torch.empty_like(Ek)
+    _lib.call("fem_transport_elements", ctx.handle, ptr(Un), ptr(U), float(dt), float(D), int(bool(supg)),
+              int(bool(transpose)), ptr(Ek), ptr(Bk), stream())
+    return Ek, Bk
 
 
-def transport_element_matrices(wq, N, Nd, nd, nn, nconn, Un, U, dt, D, supg):
-    """transport_elements on explicit element data: wq (nq[, 1]), N (nq, nen),
-    Nd (nq, nd, nen) of a uniform mesh, nconn (ne, nen) int64, U_n and U
-    (nd * nn, component-major); torch tensors on any device."""
-    w = wq.reshape(-1)
-
-    def interp(V):
-        return torch.einsum("qi,dei->eqd", N, V.view(nd, nn)[:, nconn])
-
-    def conv(V):
-        Ve = V.view(nd, nn)[:, nconn]
-        adv = torch.einsum("q,qa,eqd,qdb->eab", w, N, interp(V), Nd)
-        div = torch.einsum("qdi,dei->eq", Nd, Ve)
-        return adv + torch.einsum("q,qa,eq,qb->eab", w, N, div, N)
-
-    Ce_new, Ce_n = conv(U), conv(Un)
-    if not supg:
-        return 0.5 * Ce_new, -0.5 * Ce_n
-    Uq = interp(Un)
-    Ct = torch.einsum("q,qda,eqd,eqk,qkb->eab", w, Nd, Uq, Uq, Nd)
-    ce = torch.sqrt((Ce_new ** 2).sum((1, 2)))
-    kt = torch.sqrt((Ct ** 2).sum((1, 2)))
-    un2 = (Uq ** 2).sum(2).mean(1)
-    tau1 = ce / kt
-    tau3 = tau1 * (un2 * ce) / ((D + 1e-6) * kt)
-    tau = (tau1 ** -2 + (dt / 2) ** -2 + tau3 ** -2) ** -0.5
-    Ctau = tau[:, None, None] * Ct
-    Mtau = tau[:, None, None] * Ce_n.transpose(1, 2)
-    return Mtau / dt + 0.5 * (Ce_new + Ctau), Mtau / dt - 0.5 * (Ce_n + Ctau)
+def transport_vjp(solver, Un, U, lam, phin, phi, dt, D, supg):
+    """(d/dU_n, d/dU) of <lam, B(U_n) phi_n - A(U_n, U) phi> (the velocity
+    dependence of Ce, Ctau, Mtau and tau in the operators of
+    transport_elements) by the fem_transport_vjp kernels."""
+    ctx = solver.ctx
+    gUn, gU = torch.empty_like(Un), torch.empty_like(U)
+    _lib.call("fem_transport_vjp", ctx.handle, ptr(Un), ptr(U), ptr(lam), ptr(phin), ptr(phi), float(dt), float(D),
+              int(bool(supg)), ptr(gUn), ptr(gU), stream())
+    return gUn, gU
 
 
 class Transport(torch.autograd.Function):
@@ -356,8 +324,9 @@ class Transport(torch.autograd.Function):
         A_m^T lam = g        (masked transposed BiCGSTAB, as in MomentumSolve)
         g_phi_n = B^T (P_f lam),   g_phi_d = lam on gamma_d_phi,
         g_U_n, g_U = d/dU <P_f lam, B(U_n, U) phi_n - A(U_n, U) phi>
-    the last by torch autograd over transport_elements (the shared parts of A
-    and B do not depend on the velocity)."""
+    the transposed element matrices from fem_transport_elements and the last
+    line from fem_transport_vjp (the shared parts of A and B do not depend on
+    the velocity)."""
 
     @staticmethod
     def forward(fctx, U_n, U, phi_n, phid_full, solver, nconn, dt, D, supg=False, phi_mask=None, tol=1e-13):
@@ -378,13 +347,11 @@ class Transport(torch.autograd.Function):
     @staticmethod
     def backward(fctx, g):
         solver, nconn, Un, Uc, pn, phi, dt, D, supg, phi_mask, tol = fctx.save
-        Me, Le = solver.ctx.element_data()[3], solver.ctx.element_data()[4]
-        with torch.enable_grad():
-            un, uc = Un.clone().requires_grad_(True), Uc.clone().requires_grad_(True)
-            Ek, Bk = transport_elements(solver, nconn, un, uc, dt, D, supg)
+        ctx = solver.ctx
+        Me, Le = ctx.element_data()[3], ctx.element_data()[4]
+        EkT, BkT = transport_elements(solver, Un, Uc, dt, D, supg, transpose=True)
         KA = (Me / dt + 0.5 * D * Le).reshape(-1).contiguous()
         KB = (Me / dt - 0.5 * D * Le).reshape(-1).contiguous()
-        EkT = Ek.detach().transpose(1, 2).contiguous()
         m = phi_mask.to(torch.bool) if phi_mask is not None else None
         g = g.contiguous()
         b = g.clone()
@@ -395,11 +362,8 @@ class Transport(torch.autograd.Function):
         if m is not None:
             lam_d = g - _ebe(solver, lam, 1.0, KA, 1.0, EkT, ncomp=1)
             g_phid = torch.where(m, lam_d, torch.zeros_like(lam_d))
-        g_phin = _ebe(solver, lam, 1.0, KB, 1.0, Bk.detach().transpose(1, 2).contiguous(), ncomp=1)
-        le, pe, fe = lam[nconn], pn[nconn], phi[nconn]
-        with torch.enable_grad():
-            s = torch.einsum("ea,eab,eb->", le, Bk, pe) - torch.einsum("ea,eab,eb->", le, Ek, fe)
-            gUn, gU = torch.autograd.grad(s, (un, uc))
+        g_phin = _ebe(solver, lam, 1.0, KB, 1.0, BkT, ncomp=1)
+        gUn, gU = transport_vjp(solver, Un, Uc, lam, pn, phi, dt, D, supg)
         return gUn, gU, g_phin, g_phid, None, None, None, None, None, None, None
 
 

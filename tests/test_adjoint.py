@@ -217,17 +217,25 @@ def _transport_case(solver, supg, seed=40):
 @pytest.mark.gpu
 @pytest.mark.parametrize("supg", [False, True])
 def test_transport_elements_reproduce_the_product_step(cavity, supg):
-    """transport_elements (the torch restatement the adjoint differentiates)
-    describes the system fem_transport_phi solves: the product's phi leaves a
-    relative residual at the solver's tolerance in the restated system."""
+    """fem_transport_elements (the element matrices the adjoint solves with)
+    equals the torch restatement, transposed too, and describes the system
+    fem_transport_phi solves: the product's phi leaves a relative residual at
+    the solver's tolerance in that system."""
     from jax_fem_cfd_b200.setup import regular_mesh as rm
     from jax_fem_cfd_b200.solvers.adjoint import Transport, transport_elements
+    from torch_restatement import transport_element_matrices
     solver, _ = cavity
     _, nconn, *_ = rm.create_mesh_2d(16, 16, 1.0, 1.0)
     Un, U, phin, phid, mask, _ = _transport_case(solver, supg)
     dt, D = 0.01, 1e-3
     phi = Transport.apply(Un, U, phin, phid, solver, nconn, dt, D, supg, mask)
-    Ek, Bk = transport_elements(solver, nconn, Un, U, dt, D, supg)
+    Ek, Bk = transport_elements(solver, Un, U, dt, D, supg)
+    EkT, BkT = transport_elements(solver, Un, U, dt, D, supg, transpose=True)
+    wq, N, Nd = solver.ctx.element_data()[:3]
+    Er, Br = transport_element_matrices(wq, N, Nd, 2, solver.nn, nconn, Un, U, dt, D, supg)
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    assert rel(Ek, Er) < 1e-13 and rel(Bk, Br) < 1e-13
+    assert torch.equal(EkT, Ek.transpose(1, 2)) and torch.equal(BkT, Bk.transpose(1, 2))
     Me, Le = solver.ctx.element_data()[3], solver.ctx.element_data()[4]
     n = solver.nn
 
@@ -334,6 +342,45 @@ def test_deferred_status_raises_when_the_block_ends(cavity):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("supg", [False, True])
+@pytest.mark.parametrize("kind", ["q1", "q2_periodic"])
+def test_transport_vjp_kernel_matches_torch_autograd(kind, supg):
+    """fem_transport_vjp (d/dU_n and d/dU of <lam, B_k phi_n - E_k phi>
+    summed over elements) against torch autograd of the torch restatement of
+    E_k and B_k, which tests/test_adjoint_elements.py pins to the oracle."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from jax_fem_cfd_b200.context import Context, Mesh
+    from jax_fem_cfd_b200.solvers.adjoint import transport_vjp
+    from torch_restatement import transport_element_matrices
+    from oracle import mesh as om
+    if kind == "q1":
+        mesh, nconn = Mesh(0, False, 7, 5, 1, 1.4, 1.0), om.create_mesh_2d(7, 5, 1.4, 1.0)[1]
+    else:
+        mesh, nconn = (Mesh(1, True, 6, 4, 1, 2 * np.pi, 2 * np.pi),
+                       om.create_periodic_mesh_2d_quad9(6, 4, 2 * np.pi, 2 * np.pi)[1])
+    ctx = Context(mesh)
+    nn = ctx.nn
+    solver = type("S", (), {"ctx": ctx})()
+    rng = np.random.default_rng(23 + int(supg))
+    t = lambda a_: torch.as_tensor(a_, dtype=torch.float64, device="cuda")
+    Un = t(0.5 * rng.standard_normal(2 * nn))
+    U = Un + t(0.1 * rng.standard_normal(2 * nn))
+    lam, phin, phi = (t(rng.standard_normal(nn)) for _ in range(3))
+    dt, D = 0.01, 1e-3
+    gUn, gU = transport_vjp(solver, Un, U, lam, phin, phi, dt, D, supg)
+    wq, N, Nd = ctx.element_data()[:3]
+    nc = torch.as_tensor(nconn).cuda()
+    un, u = Un.clone().requires_grad_(True), U.clone().requires_grad_(True)
+    Ek, Bk = transport_element_matrices(wq, N, Nd, 2, nn, nc, un, u, dt, D, supg)
+    le, pe, fe = lam[nc], phin[nc], phi[nc]
+    s = torch.einsum("ea,eab,eb->", le, Bk, pe) - torch.einsum("ea,eab,eb->", le, Ek, fe)
+    rn, ru = torch.autograd.grad(s, (un, u))
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    assert rel(gUn, rn) < 1e-12 and rel(gU, ru) < 1e-12, (rel(gUn, rn), rel(gU, ru))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["q1", "q2_periodic", "hex8"])
 def test_conv_vjp_kernel_matches_its_torch_restatement(kind):
     """fem_conv_vjp (d/dU <a, Ce(U) b>, the velocity side of the step adjoint)
@@ -343,7 +390,7 @@ def test_conv_vjp_kernel_matches_its_torch_restatement(kind):
         pytest.skip("no CUDA device")
     from jax_fem_cfd_b200 import _lib
     from jax_fem_cfd_b200.context import Context, Mesh, ptr, stream
-    from jax_fem_cfd_b200.solvers.adjoint import conv_vjp_u_elements
+    from torch_restatement import conv_vjp_u_elements
     from oracle import mesh as om
     if kind == "q1":
         mesh, nconn = Mesh(0, False, 7, 5, 1, 1.4, 1.0), om.create_mesh_2d(7, 5, 1.4, 1.0)[1]

@@ -1,6 +1,6 @@
-"""The torch restatement of the transport step's element matrices that the
-transport adjoint differentiates (solvers.adjoint.transport_element_matrices)
-against the oracle's element functions (core/element_calc.py:165-229 via
+"""The torch restatements in tests/torch_restatement.py (the references for
+the fem_transport_elements, fem_transport_vjp and fem_conv_vjp kernels) against
+the oracle's element functions (core/element_calc.py:165-229 via
 oracle/element.py), on CPU tensors."""
 import numpy as np
 import pytest
@@ -12,7 +12,7 @@ def test_transport_element_matrices_match_the_oracle(supg):
     from oracle import element as oe
     from oracle import mesh as om
     from oracle import shape as osh
-    from jax_fem_cfd_b200.solvers.adjoint import transport_element_matrices
+    from torch_restatement import transport_element_matrices
     coords, nconn, *_ = om.create_mesh_2d(6, 5, 1.2, 1.0)
     wq, N, Nd = osh.quad4_shape_functions(coords[nconn[0]])
     nn, nd, dt, D = coords.shape[0], 2, 0.01, 1e-3
@@ -39,7 +39,7 @@ def test_transport_element_matrices_are_differentiable_in_both_velocities():
     (U_n, U) with SUPG (tau, norms and Ce through autograd)."""
     from oracle import mesh as om
     from oracle import shape as osh
-    from jax_fem_cfd_b200.solvers.adjoint import transport_element_matrices
+    from torch_restatement import transport_element_matrices
     coords, nconn, *_ = om.create_mesh_2d(3, 2, 1.0, 1.0)
     wq, N, Nd = osh.quad4_shape_functions(coords[nconn[0]])
     nn = coords.shape[0]
@@ -65,7 +65,7 @@ def test_convection_vjp_matches_the_oracle(beta):
     from oracle import element as oe
     from oracle import mesh as om
     from oracle import shape as osh
-    from jax_fem_cfd_b200.solvers.adjoint import conv_vjp_u_elements
+    from torch_restatement import conv_vjp_u_elements
     coords, nconn, *_ = om.create_mesh_2d(5, 4, 1.0, 0.8)
     wq, N, Nd = osh.quad4_shape_functions(coords[nconn[0]])
     nn, nd = coords.shape[0], 2
