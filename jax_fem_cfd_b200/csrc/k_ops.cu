@@ -912,13 +912,15 @@ __global__ void __launch_bounds__(128) k_transport_vjp_elem(FemGrid g, const __g
         uu[c][k] = U[nd[k] + c * nn];
       }
     }
-    // the element matrices of the step
-    double Cn[NEN][NEN], Cu[NEN][NEN], Ct[NEN][NEN];
+    // Ce(U) and Ct(U_n) (the ones whose norms enter tau); lam^T Ce(U_n)^T (phi_n - phi)
+    // and lam^T Ct (phi_n + phi) at the Gauss points, without forming Ce(U_n)
+    double Cu[NEN][NEN], Ct[NEN][NEN];
     for (int a = 0; a < NEN; ++a)
-      for (int b = 0; b < NEN; ++b) Cn[a][b] = Cu[a][b] = Ct[a][b] = 0.0;
-    double un2 = 0.0;
+      for (int b = 0; b < NEN; ++b) Cu[a][b] = Ct[a][b] = 0.0;
+    double un2 = 0.0, sCnT = 0.0, sCt = 0.0;
     for (int q = 0; q < NQ; ++q) {
       double vn[2] = {0.0, 0.0}, vu[2] = {0.0, 0.0}, divn = 0.0, divu = 0.0;
+      double dq = 0.0, lq = 0.0, gl = 0.0, gs = 0.0;
       for (int k = 0; k < NEN; ++k) {
         for (int c = 0; c < 2; ++c) {
           vn[c] += qt.N[q][k] * un[c][k];
@@ -926,35 +928,42 @@ __global__ void __launch_bounds__(128) k_transport_vjp_elem(FemGrid g, const __g
         }
         divn += qt.dx[q][k] * un[0][k] + qt.dy[q][k] * un[1][k];
         divu += qt.dx[q][k] * uu[0][k] + qt.dy[q][k] * uu[1][k];
+        dq += qt.N[q][k] * (fn[k] - f[k]);
+        lq += qt.N[q][k] * l[k];
+      }
+      for (int k = 0; k < NEN; ++k) {
+        const double gk = qt.dx[q][k] * vn[0] + qt.dy[q][k] * vn[1];
+        gl += gk * l[k];
+        gs += gk * (fn[k] + f[k]);
       }
       un2 += vn[0] * vn[0] + vn[1] * vn[1];
       const double w = qt.w[q];
-      for (int a = 0; a < NEN; ++a)
-        for (int b = 0; b < NEN; ++b) {
-          const double na = qt.N[q][a], nb = qt.N[q][b];
-          Cn[a][b] += w * na * ((vn[0] * qt.dx[q][b] + vn[1] * qt.dy[q][b]) + divn * nb);
-          Cu[a][b] += w * na * ((vu[0] * qt.dx[q][b] + vu[1] * qt.dy[q][b]) + divu * nb);
-          const double ga = qt.dx[q][a] * vn[0] + qt.dy[q][a] * vn[1], gb = qt.dx[q][b] * vn[0] + qt.dy[q][b] * vn[1];
-          Ct[a][b] += w * ga * gb;
+      // sum_ab d_a Ce(U_n)_ab l_b and sum_ab l_a Ct_ab s_b at this point
+      sCnT += w * dq * (gl + divn * lq);
+      sCt += w * gl * gs;
+      if (supg)
+        for (int a = 0; a < NEN; ++a) {
+          const double na = qt.N[q][a], ga = qt.dx[q][a] * vn[0] + qt.dy[q][a] * vn[1];
+          for (int b = 0; b < NEN; ++b) {
+            const double gb = qt.dx[q][b] * vn[0] + qt.dy[q][b] * vn[1];
+            Cu[a][b] += w * na * ((vu[0] * qt.dx[q][b] + vu[1] * qt.dy[q][b]) + divu * qt.N[q][b]);
+            Ct[a][b] += w * ga * gb;
+          }
         }
     }
     un2 /= NQ;
-    // G = ds/d(matrix): Gu for Ce(U), Gn for Ce(U_n), Gt for Ct; gu2 for the mean |u|^2
-    double Gu[NEN][NEN], Gn[NEN][NEN], Gt[NEN][NEN], gu2 = 0.0;
-    for (int a = 0; a < NEN; ++a)
-      for (int b = 0; b < NEN; ++b) {
-        Gu[a][b] = -0.5 * l[a] * f[b];
-        Gn[a][b] = -0.5 * l[a] * fn[b];
-        Gt[a][b] = 0.0;
-      }
+    // ds/d(matrix), applied without storing it:
+    //   G_u = -lam phi^T / 2 + cu Ce(U)        (Ce(U) through ce in tau)
+    //   G_n = -lam phi_n^T / 2 + (tau/dt) (phi_n - phi) lam^T
+    //   G_t = -(tau/2) lam (phi_n + phi)^T + ct Ct
+    // and gu2 = ds/d(mean |u|^2)
+    double tdt = 0.0, th = 0.0, cu = 0.0, ct = 0.0, gu2 = 0.0;
     if (supg) {
-      double ce = 0.0, kt = 0.0, sCnT = 0.0, sCt = 0.0;
+      double ce = 0.0, kt = 0.0;
       for (int a = 0; a < NEN; ++a)
         for (int b = 0; b < NEN; ++b) {
           ce += Cu[a][b] * Cu[a][b];
           kt += Ct[a][b] * Ct[a][b];
-          sCnT += (fn[a] - f[a]) * Cn[a][b] * l[b];  // lam^T Cn^T (phi_n - phi)
-          sCt += l[a] * Ct[a][b] * (fn[b] + f[b]);
         }
       ce = sqrt(ce);
       kt = sqrt(kt);
@@ -967,49 +976,70 @@ __global__ void __launch_bounds__(128) k_transport_vjp_elem(FemGrid g, const __g
       const double dkt = tau3 * (-i1 * ce / (kt * kt) - i3 * 2.0 * un2 * ce * ce / (De * kt * kt * kt));
       const double dun2 = tau3 * i3 * ce * ce / (De * kt * kt);
       const double gtau = sCnT / dt - 0.5 * sCt;
-      for (int a = 0; a < NEN; ++a)
-        for (int b = 0; b < NEN; ++b) {
-          Gu[a][b] += gtau * dce * Cu[a][b] / ce;
-          Gn[a][b] += (tau / dt) * (fn[a] - f[a]) * l[b];
-          Gt[a][b] = -0.5 * tau * l[a] * (fn[b] + f[b]) + gtau * dkt * Ct[a][b] / kt;
-        }
+      tdt = tau / dt;
+      th = 0.5 * tau;
+      cu = gtau * dce / ce;
+      ct = gtau * dkt / kt;
       gu2 = gtau * dun2;
     }
-    // back to the nodes
+    // back to the nodes: <G, Ce(V)> and <G_t, Ct(u)> differentiated at the Gauss points
     double on[2][NEN], ou[2][NEN];
     for (int c = 0; c < 2; ++c)
       for (int k = 0; k < NEN; ++k) on[c][k] = ou[c][k] = 0.0;
     for (int q = 0; q < NQ; ++q) {
       const double w = qt.w[q];
       double vn[2] = {0.0, 0.0};
+      double lq = 0.0, fq = 0.0, fnq = 0.0, dq = 0.0, dl[2] = {0.0, 0.0}, df[2] = {0.0, 0.0}, dfn[2] = {0.0, 0.0};
+      double gl = 0.0, gs = 0.0, ss[2] = {0.0, 0.0};
       for (int k = 0; k < NEN; ++k) {
-        vn[0] += qt.N[q][k] * un[0][k];
-        vn[1] += qt.N[q][k] * un[1][k];
+        const double nk = qt.N[q][k], xk = qt.dx[q][k], yk = qt.dy[q][k];
+        vn[0] += nk * un[0][k];
+        vn[1] += nk * un[1][k];
+        lq += nk * l[k];
+        fq += nk * f[k];
+        fnq += nk * fn[k];
+        dq += nk * (fn[k] - f[k]);
+        dl[0] += xk * l[k];
+        dl[1] += yk * l[k];
+        df[0] += xk * f[k];
+        df[1] += yk * f[k];
+        dfn[0] += xk * fn[k];
+        dfn[1] += yk * fn[k];
+        ss[0] += xk * (fn[k] + f[k]);
+        ss[1] += yk * (fn[k] + f[k]);
       }
-      double Su[2] = {0.0, 0.0}, Tu = 0.0, Sn[2] = {0.0, 0.0}, Tn = 0.0, Gq[2] = {0.0, 0.0};
-      for (int a = 0; a < NEN; ++a) {
-        const double na = qt.N[q][a], ga = qt.dx[q][a] * vn[0] + qt.dy[q][a] * vn[1];
-        for (int b = 0; b < NEN; ++b) {
-          const double nb = qt.N[q][b], dxb = qt.dx[q][b], dyb = qt.dy[q][b];
-          Su[0] += Gu[a][b] * na * dxb;
-          Su[1] += Gu[a][b] * na * dyb;
-          Tu += Gu[a][b] * na * nb;
-          Sn[0] += Gn[a][b] * na * dxb;
-          Sn[1] += Gn[a][b] * na * dyb;
-          Tn += Gn[a][b] * na * nb;
-          if (supg) {
-            const double gb = dxb * vn[0] + dyb * vn[1];
-            Gq[0] += Gt[a][b] * (qt.dx[q][a] * gb + ga * dxb);
-            Gq[1] += Gt[a][b] * (qt.dy[q][a] * gb + ga * dyb);
+      gl = dl[0] * vn[0] + dl[1] * vn[1];
+      gs = ss[0] * vn[0] + ss[1] * vn[1];
+      // S_d = sum_ab G_ab N_a dN_b/dx_d, T = sum_ab G_ab N_a N_b (rank-one parts in closed form)
+      double Su[2] = {-0.5 * lq * df[0], -0.5 * lq * df[1]}, Tu = -0.5 * lq * fq;
+      double Sn[2] = {-0.5 * lq * dfn[0] + tdt * dq * dl[0], -0.5 * lq * dfn[1] + tdt * dq * dl[1]};
+      double Tn = -0.5 * lq * fnq + tdt * dq * lq;
+      // d/du of sum_ab G_t,ab (dN_a . u)(dN_b . u) = sum_ab G_t,ab (dN_a (dN_b . u) + (dN_a . u) dN_b)
+      double Gq[2] = {-th * (dl[0] * gs + gl * ss[0]), -th * (dl[1] * gs + gl * ss[1])};
+      if (supg)
+        for (int a = 0; a < NEN; ++a) {
+          const double na = qt.N[q][a], ga = qt.dx[q][a] * vn[0] + qt.dy[q][a] * vn[1];
+          for (int b = 0; b < NEN; ++b) {
+            const double dxb = qt.dx[q][b], dyb = qt.dy[q][b], gb = dxb * vn[0] + dyb * vn[1];
+            const double cua = cu * Cu[a][b] * na, cta = ct * Ct[a][b];
+            Su[0] += cua * dxb;
+            Su[1] += cua * dyb;
+            Tu += cua * qt.N[q][b];
+            Gq[0] += cta * (qt.dx[q][a] * gb + ga * dxb);
+            Gq[1] += cta * (qt.dy[q][a] * gb + ga * dyb);
           }
         }
-      }
       for (int k = 0; k < NEN; ++k) {
         const double nk = qt.N[q][k];
         ou[0][k] += w * (nk * Su[0] + qt.dx[q][k] * Tu);
         ou[1][k] += w * (nk * Su[1] + qt.dy[q][k] * Tu);
-        on[0][k] += w * (nk * Sn[0] + qt.dx[q][k] * Tn) + nk * (w * Gq[0] + gu2 * 2.0 * vn[0] / NQ);
-        on[1][k] += w * (nk * Sn[1] + qt.dy[q][k] * Tn) + nk * (w * Gq[1] + gu2 * 2.0 * vn[1] / NQ);
+        if (supg) {
+          on[0][k] += w * (nk * Sn[0] + qt.dx[q][k] * Tn) + nk * (w * Gq[0] + gu2 * 2.0 * vn[0] / NQ);
+          on[1][k] += w * (nk * Sn[1] + qt.dy[q][k] * Tn) + nk * (w * Gq[1] + gu2 * 2.0 * vn[1] / NQ);
+        } else {
+          on[0][k] += w * (nk * Sn[0] + qt.dx[q][k] * Tn);
+          on[1][k] += w * (nk * Sn[1] + qt.dy[q][k] * Tn);
+        }
       }
     }
     for (int c = 0; c < 2; ++c)
