@@ -428,6 +428,22 @@ def serving(count, steps, plain_sample=128):
     del srv
     import torch
     torch.cuda.empty_cache()
+    # packed launches: every size's requests as members of one persistent kernel per chunk
+    from jax_fem_cfd_b200.serving import PackedServer
+    ps = PackedServer(share=tune["picked"], keep_results=False)
+    plan = ps.prewarm(reqs)
+    ps.run(reqs[:min(16, count)], realtime=False)  # first launches of each pack
+    dpk, pk = ps.run(reqs, realtime=False)
+    out["served_saturated_packed"] = dict(pk, failed=bad(dpk), members_per_size=plan)
+    out["speedup_packed_solves_per_s"] = pk["solves_per_s"] / plain["solves_per_s"]
+    for frac in (0.5, 0.9):
+        rate = frac * pk["solves_per_s"]
+        dr, m = ps.run(make_requests(count, seed=0, steps=steps, rate=rate))
+        out[f"served_packed_poisson_{int(frac * 100)}pct"] = dict(m, arrival_rate_per_s=rate, failed=bad(dr))
+    for p in ps.packs.values():
+        p.close()
+    del ps
+    torch.cuda.empty_cache()
     mx = Server(keep_results=False, precision="mixed", share=tune["picked"])
     mx.prewarm(reqs)
     mx.run(reqs[:min(16, count)], realtime=False)  # graph builds of the mixed solves, once per pooled solver

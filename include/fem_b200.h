@@ -418,6 +418,35 @@ long long fem_launch_count(void);
 /* Last CUDA error string recorded by the library (host, static storage). */
 const char* fem_last_error(void);
 
+/* Packed steps (serving): k contexts of one mesh size advanced together, one
+ * persistent cooperative launch per call. Member m is the context ctxs[m]
+ * (Q1 2D, multigrid hierarchy, pinned pressure, on-the-fly convection, FP64
+ * precision) with its ping-pong fields (U[0], P[0]) = (U0[m], P0[m]) and
+ * (U[1], P[1]) = (U1[m], P1[m]) and its Dirichlet values Ud[m]; every member's
+ * cooperative CTA count (its max-CTA cap, fem_ctx_set_max_ctas) must be the
+ * same, and k x that count must fit on the device at once (FEM_E_STATE
+ * otherwise). stat: device int32 [k * 5], per member the momentum and
+ * pressure iterations of its last step, their statuses, and at [5m + 4] the
+ * OR of every status since the caller last zeroed it. tol and precond have
+ * fem_step4's meaning. Each member's step is fem_step4's on the same CTA count
+ * (solvers/standard.py:148-165, rho = 1), bit for bit. No reference
+ * counterpart: the reference runs one problem at a time. */
+typedef struct fem_pack fem_pack;
+int fem_pack_create(fem_ctx* const* ctxs, int k, double* const* U0, double* const* P0, double* const* U1,
+                    double* const* P1, const double* const* Ud, int* stat, double tol, int precond,
+                    fem_pack** out);
+/* steps[m] steps of member m (0: idle this call) from buffer cur[m] (0 or 1)
+ * with its dt[m] and viscosity mu[m] (host arrays of k values, read before
+ * the call returns); the result of member m is in buffer cur[m] ^ (steps[m] & 1).
+ * Calls on one pack run in stream order; a member's buffers may be written by
+ * the caller between calls on the same stream. */
+int fem_pack_step(fem_pack* pack, const double* dt, const double* mu, const int* steps, const int* cur,
+                  cudaStream_t stream);
+/* Members and CTAs per member of a pack; the device's capacity for one packed
+ * launch (SMs x resident CTAs per SM of the packed kernel). */
+int fem_pack_info(const fem_pack* pack, int* k, int* ctas, int* capacity);
+int fem_pack_destroy(fem_pack* pack);
+
 #ifdef __cplusplus
 }
 #endif

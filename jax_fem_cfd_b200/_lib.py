@@ -45,6 +45,10 @@ SIGNATURES = {
     "fem_conv_vjp": (c_int, [P, c_int, P, P, c_double, P, P]),
     "fem_transport_vjp": (c_int, [P, P, P, P, P, P, c_double, c_double, c_int, P, P, P]),
     "fem_transport_elements": (c_int, [P, P, P, c_double, c_double, c_int, c_int, P, P, P]),
+    "fem_pack_create": (c_int, [P, c_int, P, P, P, P, P, P, c_double, c_int, P]),
+    "fem_pack_step": (c_int, [P, P, P, P, P, P]),
+    "fem_pack_info": (c_int, [P, P, P, P]),
+    "fem_pack_destroy": (c_int, [P]),
     "fem_element_matrices": (c_int, [c_int, c_int, c_int, P, P, P, P, P, P, P, P]),
     "fem_assemble_diag": (c_int, [P, P, P, c_int, P, P, P]),
     "fem_lattice_interpolate": (c_int, [c_int, c_int, c_int, c_int, c_int, P, P, P]),

@@ -46,6 +46,29 @@ struct StepArgs {
   int pinned;
 };
 
+// One request of a packed step launch (k_pack.cu): the device pointers and
+// solver arguments of its context, built once per pack. The 4-step step of
+// fem_step4 (Q1, pinned multigrid pressure, on-the-fly convection, FP64).
+struct PackMember {
+  StepArgs S;  // dt and mu come from the launch's PackStep
+  BiArgs B;    // momentum solve: x = Uhat, b = rhsU; its shared matrix is built in smem
+  CgArgs C;    // pressure solve: b = rhsP; x is the step's output pressure
+  double* U[2];
+  double* P[2];
+  const double* Ud;
+  double *cvf, *vcv, *rhsU, *Uhat, *gPn, *Ustar, *rhsP;
+  double *cr, *cp, *cq;
+  int* stat;  // [0..1] iterations, [2..3] statuses of the last step (momentum, pressure), [4] OR of all statuses
+};
+#define FEM_PACK_MAX 64
+struct PackStep {
+  double dt, mu;
+  int steps;  // steps of this launch (0: the member is idle)
+  int cur;    // buffer (0 or 1) holding the member's current U, P
+};
+struct PackParams {
+  PackStep m[FEM_PACK_MAX];
+};
 
 // ----------------------------------------------------------------------------
 // Host launchers (one translation unit per kernel family; fem_capi.cu drives them)
@@ -154,6 +177,10 @@ int fem_coop_occupancy_bi(int* occ);
 int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s);
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s);
 int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s);
+// packed step (k_pack.cu): k members of `ctas` CTAs each, one cooperative launch
+int fem_launch_step_pack(int kind, const PackMember* members, const PackParams& P, int k, int ctas,
+                         cudaStream_t s);
+int fem_pack_occupancy(int* per_sm);
 
 int fem_launch_mom_rhs(const StepArgs& S, const double* Un, const double* Pn, const double* Ud, const double* F,
                        double* rhs, double* x0, double* gPn, cudaStream_t s);

@@ -12,6 +12,7 @@
 
 #include <nvtx3/nvToolsExt.h>
 
+#include <vector>
 #include "fem_b200.h"
 #include "fem_args.cuh"
 #include "fem_mg3.cuh"
@@ -1452,6 +1453,179 @@ extern "C" int fem_ctx_set_max_ctas(fem_ctx* c, int ctas, int* capacity) {
   if (!c || ctas < 0) return FEM_E_ARG;
   c->max_coop = (ctas > 0 && ctas < c->coop_capacity) ? ctas : c->coop_capacity;
   if (capacity) *capacity = c->coop_capacity;
+  return FEM_OK;
+}
+
+// ------------------------------------------------------------ packed steps ----
+
+struct fem_pack {
+  int k = 0, ctas = 0, capacity = 0;
+  PackMember* dmem = nullptr;    // k members (device)
+  unsigned int* sync = nullptr;  // [2m] grid and [2m + 1] team arrival counts, [2k + m] error word
+};
+
+extern "C" int fem_pack_create(fem_ctx* const* ctxs, int k, double* const* U0, double* const* P0,
+                               double* const* U1, double* const* P1, const double* const* Ud, int* stat,
+                               double tol, int precond, fem_pack** out) {
+  if (!ctxs || !U0 || !P0 || !U1 || !P1 || !stat || !out || k < 1 || k > FEM_PACK_MAX) return FEM_E_ARG;
+  if (precond < 0 || precond > 4) return FEM_E_ARG;
+  *out = nullptr;
+  const fem_ctx* c0 = ctxs[0];
+  if (!c0) return FEM_E_ARG;
+  const int ctas = ctx_grid_for(c0, c0->g.nn);
+  for (int m = 0; m < k; ++m) {
+    const fem_ctx* c = ctxs[m];
+    if (!c || !U0[m] || !P0[m] || !U1[m] || !P1[m]) return FEM_E_ARG;
+    if (c->has_dmask && (!Ud || !Ud[m])) return FEM_E_ARG;
+    if (c->g.kind != FEM_Q1_2D || c->ndim != 2 || !c->set_zeroP || !c->conv_otf || !c->cvf ||
+        c->precision != FEM_PRECISION_FP64 || (precond == FEM_PREC_MG && c->nlev < 2)) {
+      snprintf(g_err, sizeof(g_err),
+               "fem_pack_create: member %d is not a Q1 2D pinned-pressure FP64 context with on-the-fly convection",
+               m);
+      return FEM_E_STATE;
+    }
+    if (c->g.nnx != c0->g.nnx || c->g.nny != c0->g.nny || c->g.periodic != c0->g.periodic ||
+        c->device != c0->device || ctx_grid_for(c, c->g.nn) != ctas) {
+      snprintf(g_err, sizeof(g_err), "fem_pack_create: member %d differs in mesh, device or CTA count", m);
+      return FEM_E_STATE;
+    }
+  }
+  int per_sm = 0;
+  if (fem_pack_occupancy(&per_sm) != 0 || per_sm < 1) return set_err("fem_pack_occupancy", cudaGetLastError());
+  const int capacity = per_sm * c0->sms;
+  if (k * ctas > capacity) {
+    snprintf(g_err, sizeof(g_err), "fem_pack_create: %d members x %d CTAs exceed the %d co-resident CTAs", k, ctas,
+             capacity);
+    return FEM_E_STATE;
+  }
+  fem_pack* p = new fem_pack();
+  p->k = k;
+  p->ctas = ctas;
+  p->capacity = capacity;
+  std::vector<PackMember> hm(k);
+  int rc = dalloc(&p->dmem, (size_t)k);
+  if (!rc) rc = dalloc(&p->sync, (size_t)3 * k);
+  const double theta = 0.5, rho = 1.0;
+  for (int m = 0; m < k && !rc; ++m) {
+    fem_ctx* c = ctxs[m];
+    PackMember& M = hm[m];
+    memset(&M, 0, sizeof(M));
+    int* st = stat + 5 * m;
+    const FemSync sync{p->sync + 2 * m, p->sync + 2 * m + 1, reinterpret_cast<int*>(p->sync + 2 * k + m),
+                       c->partials, FEM_NSLOTS, nullptr, 0};
+    // the fem_step4 stage arguments (dt, mu set per launch)
+    StepArgs& S = M.S;
+    S.g = c->g;
+    S.ndim = 2;
+    S.rho = rho;
+    S.theta = theta;
+    S.Me = c->Me;
+    S.Le = c->Le;
+    S.Ge = c->Ge;
+    S.M = c->M;
+    S.Ce = nullptr;
+    S.vcv = c->vcv;
+    S.dmask = c->has_dmask ? c->dmask : nullptr;
+    S.pmask = c->pmask;
+    S.pinned = c->set_zeroP;
+    // the momentum BiCGSTAB of run_bicgstab (its shared matrix is built in the kernel)
+    BiArgs& B = M.B;
+    B.sync = sync;
+    B.g = c->g;
+    B.op = MatCombo{nullptr, 1.0, nullptr, 0.0, 0, nullptr, 0.0};
+    B.mask = S.dmask;
+    B.b = c->rhsU;
+    B.x = c->Uhat;
+    B.r = c->br;
+    B.rhat = c->brh;
+    B.p0 = c->bp0;
+    B.p1 = c->bp1;
+    B.q0 = c->bq0;
+    B.q1 = c->bq1;
+    B.t = c->bt;
+    B.tol = tol;
+    B.atol = 0.0;
+    B.maxiter = 10 * 2 * c->g.nn;  // utils/jax_iterative_solvers.py:181-183
+    B.iters = st;
+    B.status = st + 2;
+    B.cvf = c->cvf;
+    B.cv_coef = theta * rho;
+    B.qt = c->qt;
+    // the pressure solve of run_cg (x is the step's output pressure)
+    CgArgs& C = M.C;
+    fill_cg_args(c, C);
+    C.sync = sync;
+    C.prec = precond;
+    C.center_rhs = 0;
+    C.post = 1;
+    C.maxiter = 1000;
+    C.tol = tol;
+    C.atol = 0.0;
+    C.b = c->rhsP;
+    C.x = nullptr;
+    C.iters = st + 1;
+    C.status = st + 3;
+    C.final_rr = nullptr;
+    C.team = team_size(ctas);
+    M.U[0] = U0[m];
+    M.U[1] = U1[m];
+    M.P[0] = P0[m];
+    M.P[1] = P1[m];
+    M.Ud = c->has_dmask ? Ud[m] : nullptr;
+    M.cvf = c->cvf;
+    M.vcv = c->vcv;
+    M.rhsU = c->rhsU;
+    M.Uhat = c->Uhat;
+    M.gPn = c->gPn;
+    M.Ustar = c->Ustar;
+    M.rhsP = c->rhsP;
+    M.cr = c->cr ? c->cr : c->pz;
+    M.cp = c->cp ? c->cp : c->pz;
+    M.cq = c->cq ? c->cq : c->pz;
+    M.stat = st;
+  }
+  if (!rc) {
+    const cudaError_t e = cudaMemcpy(p->dmem, hm.data(), sizeof(PackMember) * k, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = set_err("fem_pack_create", e);
+  }
+  if (rc) {
+    fem_pack_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return FEM_OK;
+}
+
+extern "C" int fem_pack_step(fem_pack* p, const double* dt, const double* mu, const int* steps, const int* cur,
+                             cudaStream_t s) {
+  if (!p || !dt || !mu || !steps || !cur) return FEM_E_ARG;
+  PackParams P;
+  memset(&P, 0, sizeof(P));
+  bool any = false;
+  for (int m = 0; m < p->k; ++m) {
+    if (steps[m] < 0 || (cur[m] != 0 && cur[m] != 1)) return FEM_E_ARG;
+    if (steps[m] > 0 && !(dt[m] > 0.0)) return FEM_E_ARG;
+    P.m[m] = PackStep{dt[m], mu[m], steps[m], cur[m]};
+    any = any || steps[m] > 0;
+  }
+  if (!any) return FEM_OK;
+  FEM_CHECK(cudaMemsetAsync(p->sync, 0, sizeof(unsigned int) * 3 * p->k, s));
+  return fem_launch_step_pack(FEM_Q1_2D, p->dmem, P, p->k, p->ctas, s);
+}
+
+extern "C" int fem_pack_info(const fem_pack* p, int* k, int* ctas, int* capacity) {
+  if (!p) return FEM_E_ARG;
+  if (k) *k = p->k;
+  if (ctas) *ctas = p->ctas;
+  if (capacity) *capacity = p->capacity;
+  return FEM_OK;
+}
+
+extern "C" int fem_pack_destroy(fem_pack* p) {
+  if (!p) return FEM_OK;
+  if (p->dmem) cudaFree(p->dmem);
+  if (p->sync) cudaFree(p->sync);
+  delete p;
   return FEM_OK;
 }
 

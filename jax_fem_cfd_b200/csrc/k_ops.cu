@@ -1,6 +1,6 @@
 // Element-product, element-matrix, transfer, boundary and blas-1 kernels.
 #include "fem_b200.h"
-#include "fem_args.cuh"
+#include "fem_step_body.cuh"
 
 
 template <int KIND, int NC>
@@ -649,33 +649,11 @@ int fem_launch_make_mask(const int64_t* idx, int n, int len, uint8_t* mask, cuda
 }
 
 // ------------------------------------------------- on-the-fly convection ----
-// Gauss-point factors of Ce(U) (fem_conv_factors), one thread per element,
-// structure of arrays fq[k * ne + e].
 template <int KIND>
 __global__ void __launch_bounds__(256) k_conv_factors(FemGrid g, const __grid_constant__ FemQuadTab qt,
                                                       const double* __restrict__ U, double bd,
                                                       double* __restrict__ fq) {
-  constexpr int NEN = KI<KIND>::NEN, NQ = KQ<KIND>::NQ, S = KI<KIND>::S;
-  const size_t nn = g.nn, ne = g.ne;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.ne; e += gridDim.x * blockDim.x) {
-    const int ey = e / g.nex, ex = e - ey * g.nex;
-    double ux[NEN], uy[NEN];
-#pragma unroll
-    for (int b = 0; b < NEN; ++b) {
-      int i = S * ex + kdi<KIND>(b), j = S * ey + kdj<KIND>(b);
-      if (g.periodic) {
-        i = i >= g.nnx ? i - g.nnx : i;
-        j = j >= g.nny ? j - g.nny : j;
-      }
-      const size_t n = (size_t)j * g.nnx + i;
-      ux[b] = U[n];
-      uy[b] = U[n + nn];
-    }
-    double f[3 * NQ];
-    fem_conv_factors<KIND>(qt, ux, uy, bd, f);
-#pragma unroll
-    for (int k = 0; k < 3 * NQ; ++k) fq[k * ne + e] = f[k];
-  }
+  step_conv_factors<KIND>(g, qt, U, bd, fq);
 }
 
 // y = alpha Ash x + cc Ce x over the whole lattice, one tile per CTA.
@@ -690,17 +668,7 @@ __global__ void __launch_bounds__(FEM_THREADS) k_conv_apply(FemGrid g, const __g
   if (Ash)
     for (int t = threadIdx.x; t < NEN * NEN; t += blockDim.x) sA[t] = Ash[t];
   __syncthreads();
-  const size_t nn = g.nn;
-  struct Tiles {
-    __device__ __forceinline__ int cta() const { return blockIdx.x; }
-    __device__ __forceinline__ int ncta() const { return gridDim.x; }
-  } tm;
-  const double* src[1] = {x};
-  fem_tiled_conv<KIND, NC, 1>(tm, g, sm, src, [](int, const double(&v)[1]) { return v[0]; }, fq, qt, cc, alpha,
-                              Ash ? sA : nullptr, [&](int i, const double(&v)[NC], const double(&)[NC]) {
-#pragma unroll
-                             for (int c = 0; c < NC; ++c) y[i + c * nn] = v[c];
-                           });
+  step_conv_apply<KIND, NC>(g, qt, fq, cc, alpha, Ash ? sA : nullptr, x, y, sm);
 }
 
 int fem_launch_conv_factors(const FemGrid& g, const FemQuadTab& qt, const double* U, double bd, double* fq,

@@ -1,96 +1,31 @@
 // 4-step projection stage kernels and the scalar-transport rhs.
-#include "fem_args.cuh"
+#include "fem_step_body.cuh"
 
 
-// rhs of solvers/standard.py:31-37 and the initial guess x0; also keeps G P_n.
 template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_mom_rhs(StepArgs S, const double* __restrict__ Un,
                                                             const double* __restrict__ Pn,
                                                             const double* __restrict__ Ud,
                                                             const double* __restrict__ F, double* __restrict__ rhs,
                                                             double* __restrict__ x0, double* __restrict__ gPn) {
-  const FemGrid& g = S.g;
-  const size_t N = g.nn;
-  constexpr int ND = KI<KIND>::DIM;
-  const MatCombo vc{S.Le, S.mu, S.Ce, S.rho, 0, nullptr, 0.0};
-  const MatShared ms_m{S.Me, 1.0};
-  auto src = [&](int j, int c) { return Un[j + c * N]; };
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
-    int ix, iy, iz;
-    fem_ij(g, n, ix, iy, iz);
-    double ms[ND], v[ND], gp[ND];
-    fem_gather_k<KIND, ND>(g, ix, iy, iz, ms_m, src, ms);
-    if (S.vcv) {
-#pragma unroll
-      for (int c = 0; c < ND; ++c) v[c] = S.vcv[n + c * N];
-    } else {
-      fem_gather_k<KIND, ND>(g, ix, iy, iz, vc, src, v);
-    }
-    fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return Pn[j]; }, gp);
-#pragma unroll
-    for (int c = 0; c < ND; ++c) {
-      const size_t o = n + c * N;
-      double r = ((S.rho / S.dt) * ms[c] - gp[c]) - (1 - S.theta) * v[c];
-      if (F) r = r + F[o];
-      gPn[o] = gp[c];
-      const bool d = S.dmask && S.dmask[o];
-      rhs[o] = d ? Ud[o] : r;
-      x0[o] = d ? Ud[o] : Un[o];
-    }
-  }
+  step_mom_rhs<KIND>(S, Un, Pn, Ud, F, rhs, x0, gPn);
 }
-
-// U* = U_hat + (dt/rho) G P_n / M   (solvers/standard.py:156)
 __global__ void k_ustar(int n, double c, const double* __restrict__ Uh, const double* __restrict__ gPn,
                         const double* __restrict__ M, double* __restrict__ Us) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    Us[i] = Uh[i] + ((c * gPn[i]) / M[i]);
+  step_ustar(n, c, Uh, gPn, M, Us);
 }
-
-// PPE rhs (rho/dt)(D U* - F_p) with pinned rows zeroed, and x0 (solvers/standard.py:97-107).
 template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_p_rhs(StepArgs S, const double* __restrict__ Us,
                                                           const double* __restrict__ Fp,
                                                           const double* __restrict__ Pn, double* __restrict__ rhs,
                                                           double* __restrict__ x0) {
-  const FemGrid& g = S.g;
-  constexpr int ND = KI<KIND>::DIM;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
-    int ix, iy, iz;
-    fem_ij(g, n, ix, iy, iz);
-    const double du = fem_gather_div_k<KIND, ND>(g, ix, iy, iz, S.Ge, Us);
-    double r = (S.rho / S.dt) * (Fp ? du - Fp[n] : du);
-    double x = Pn[n];
-    if (S.pinned && S.pmask && S.pmask[n]) {
-      r = 0.0;
-      x = 0.0;
-    }
-    rhs[n] = r;
-    x0[n] = x;
-  }
+  step_p_rhs<KIND>(S, Us, Fp, Pn, rhs, x0);
 }
-
-// U = U* - (dt/rho) G P / M ; U[gamma_d] = U_d   (solvers/standard.py:160-163)
 template <int KIND>
 __global__ void __launch_bounds__(FEM_OP_THREADS) k_ufinal(StepArgs S, const double* __restrict__ Us,
                                                            const double* __restrict__ P,
                                                            const double* __restrict__ Ud, double* __restrict__ U) {
-  const FemGrid& g = S.g;
-  const size_t N = g.nn;
-  const double c = S.dt / S.rho;
-  constexpr int ND = KI<KIND>::DIM;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
-    int ix, iy, iz;
-    fem_ij(g, n, ix, iy, iz);
-    double gp[ND];
-    fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return P[j]; }, gp);
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-      const size_t o = n + d * N;
-      const double u = Us[o] - ((c * gp[d]) / S.M[o]);
-      U[o] = (S.dmask && S.dmask[o]) ? Ud[o] : u;
-    }
-  }
+  step_ufinal<KIND>(S, Us, P, Ud, U);
 }
 
 // Scalar transport rhs (solvers/passive_transport.py:26-33 / 50-57):

@@ -362,6 +362,212 @@ class Server:
                       "graphs": self.graphs, "graph_error": self.graph_error}
 
 
+class Pack:
+    """k pooled solvers of one mesh size advanced together (fem_pack_step):
+    one persistent cooperative launch per call runs every active member's
+    steps, each member on its own group of `ctas` CTAs with its own barriers,
+    so a member's results are those of its solver run alone on `ctas` CTAs,
+    bit for bit. Members join and leave between calls."""
+
+    def __init__(self, n, k, ctas):
+        self.n, self.k, self.ctas = n, k, ctas
+        self.slots = [Slot(n) for _ in range(k)]
+        for sl in self.slots:
+            sl.set_ctas(ctas)
+        s0 = self.slots[0].solver
+        dev = s0.ctx.dev
+        self.stat = torch.zeros(5 * k, dtype=torch.int32, device=dev)
+        self.stat_host = torch.zeros(5 * k, dtype=torch.int32).pin_memory()
+        vp = lambda xs: (ctypes.c_void_p * k)(*[ctypes.c_void_p(x) for x in xs])
+        h = ctypes.c_void_p()
+        _lib.call("fem_pack_create", vp([sl.solver.ctx.handle.value for sl in self.slots]), k,
+                  vp([sl.U[0].data_ptr() for sl in self.slots]), vp([sl.P[0].data_ptr() for sl in self.slots]),
+                  vp([sl.U[1].data_ptr() for sl in self.slots]), vp([sl.P[1].data_ptr() for sl in self.slots]),
+                  vp([sl.ud.data_ptr() for sl in self.slots]), ptr(self.stat), float(s0.cfg.solver_tol),
+                  int(s0.precond), ctypes.byref(h))
+        self.handle = h
+
+    def step(self, dt, mu, steps, cur, stream):
+        """steps[m] steps of member m (0: idle) from buffer cur[m], one launch
+        on `stream`; member m's result is then in buffer cur[m] ^ (steps[m] & 1)."""
+        k = self.k
+        _lib.call("fem_pack_step", self.handle, (ctypes.c_double * k)(*dt), (ctypes.c_double * k)(*mu),
+                  (ctypes.c_int * k)(*steps), (ctypes.c_int * k)(*cur), ctypes.c_void_p(stream.cuda_stream))
+
+    def close(self):
+        if self.handle is not None:
+            _lib.call("fem_pack_destroy", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Member:
+    __slots__ = ("req", "cur", "left", "admitted", "final", "result")
+
+    def __init__(self):
+        self.req, self.cur, self.left, self.admitted, self.final, self.result = None, 0, 0, 0.0, None, None
+
+
+class PackedServer:
+    """Continuous batching with packed launches: the requests of one mesh size
+    are members of that size's Pack, and each launch advances all of a pack's
+    active members by one chunk of steps (one persistent kernel for the whole
+    chunk, no per-step launches). A request is admitted into a free member of
+    its size's pack between launches; up to two chunks per pack are queued on
+    the pack's stream. Members per size: the CTA capacity split in proportion
+    to each size's measured work in the stream (requests x steps x one step's
+    time on `share`-capped CTAs, timed before the clock starts). Results are
+    each request's solo results on its CTA share, bit for bit, whatever the mix."""
+
+    def __init__(self, share=16, chunk=10, keep_results=True, members=None):
+        self.share, self.chunk, self.keep_results = share, chunk, keep_results
+        self.members = dict(members or {})  # n -> members of that size's pack (overrides the split)
+        self.packs = {}
+        self.capacity = None
+
+    def ctas(self, n):
+        return ctas_for(n, self.share)
+
+    def _step_ms(self, n):
+        """Time of one step of a size-n request on its CTA share (one solver, 4 steps)."""
+        slot = Slot(n)
+        slot.set_ctas(self.ctas(n))
+        st = torch.cuda.current_stream()
+        slot.steps(0, 2, 0.25 / n, 1e-2, st)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        slot.steps(0, 4, 0.25 / n, 1e-2, st)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 4
+
+    def plan(self, requests):
+        """Members per size for this stream (see the class doc)."""
+        sizes = sorted({r.n for r in requests})
+        probe = Slot(sizes[0])
+        cap = ctypes.c_int(0)
+        _lib.call("fem_ctx_set_max_ctas", probe.solver.ctx.handle, 0, ctypes.byref(cap))
+        del probe
+        # the packed kernel holds one CTA per SM, like the solver kernels
+        self.capacity = cap.value
+        work = {n: sum(r.steps for r in requests if r.n == n) * self._step_ms(n) for n in sizes}
+        cta_work = sum(work[n] * self.ctas(n) for n in sizes)
+        out = {}
+        for n in sizes:
+            if n in self.members:
+                out[n] = self.members[n]
+                continue
+            k = int(self.capacity * work[n] / cta_work) if cta_work > 0 else 1
+            out[n] = max(1, min(k, sum(r.n == n for r in requests), 64, self.capacity // self.ctas(n)))
+        # the packs of all sizes must fit on the device at once
+        while sum(out[n] * self.ctas(n) for n in sizes) > self.capacity:
+            n = max(sizes, key=lambda m: out[m] * self.ctas(m))
+            if out[n] == 1:
+                break
+            out[n] -= 1
+        return out
+
+    def prewarm(self, requests):
+        """Build the packs (solvers, hierarchies, pack objects) before the clock."""
+        plan = self.plan(requests)
+        for n, k in plan.items():
+            p = self.packs.get(n)
+            if p is None or p.k != k:
+                if p is not None:
+                    p.close()
+                self.packs[n] = Pack(n, k, self.ctas(n))
+        torch.cuda.synchronize()
+        return plan
+
+    def run(self, requests, realtime=True):
+        """Serve `requests` (sorted by arrival); returns per-request records and
+        the stream's metrics, as Server.run. realtime=False admits every
+        request at t = 0."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        if not all(r.n in self.packs for r in reqs):
+            self.prewarm(reqs)
+        packs = {n: self.packs[n] for n in sorted({r.n for r in reqs})}
+        streams = {n: torch.cuda.Stream() for n in packs}
+        mem = {n: [_Member() for _ in range(p.k)] for n, p in packs.items()}
+        inflight = {n: [] for n in packs}
+        pending = {n: [] for n in packs}
+        done, nxt = [], 0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        while len(done) < len(reqs):
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and (not realtime or reqs[nxt].arrival <= now):
+                pending[reqs[nxt].n].append(reqs[nxt])
+                nxt += 1
+            for n, p in packs.items():
+                ms, st = mem[n], streams[n]
+                # retire members whose results have landed
+                for m, mb in enumerate(ms):
+                    if mb.final is not None and mb.final.query():
+                        t = time.perf_counter() - t0
+                        sl = p.slots[m]
+                        r = mb.req
+                        stat = p.stat_host[5 * m:5 * m + 5]
+                        rec = {"rid": r.rid, "n": r.n, "arrival": r.arrival, "admitted": mb.admitted, "done": t,
+                               "latency": t - (r.arrival if realtime else 0.0), "ctas": p.ctas,
+                               "status": int(stat[4])}
+                        if self.keep_results:
+                            rec["U"] = sl.U_host.numpy().copy()
+                            rec["P"] = sl.P_host.numpy().copy()
+                        done.append(rec)
+                        ms[m] = _Member()
+                inflight[n] = [e for e in inflight[n] if not e.query()]
+                if len(inflight[n]) >= 2:
+                    continue
+                # admit into free members
+                with torch.cuda.stream(st):
+                    for m, mb in enumerate(ms):
+                        if mb.req is None and pending[n]:
+                            r = pending[n].pop(0)
+                            sl = p.slots[m]
+                            sl.U0_host.copy_(torch.from_numpy(r.U0))
+                            sl.U[0].copy_(sl.U0_host, non_blocking=True)
+                            sl.P[0].zero_()
+                            p.stat[5 * m + 4].zero_()
+                            mb.req, mb.cur, mb.left = r, 0, r.steps
+                            mb.admitted = time.perf_counter() - t0
+                active = [mb.req is not None and mb.left > 0 for mb in ms]
+                if not any(active):
+                    continue
+                steps = [min(self.chunk, mb.left) if a else 0 for mb, a in zip(ms, active)]
+                p.step([mb.req.dt if mb.req else 1.0 for mb in ms], [mb.req.nu if mb.req else 0.0 for mb in ms],
+                       steps, [mb.cur for mb in ms], st)
+                ev = torch.cuda.Event()
+                ev.record(st)
+                inflight[n].append(ev)
+                with torch.cuda.stream(st):
+                    for m, (mb, k) in enumerate(zip(ms, steps)):
+                        if k == 0:
+                            continue
+                        mb.cur ^= k & 1
+                        mb.left -= k
+                        if mb.left == 0:
+                            sl = p.slots[m]
+                            sl.U_host.copy_(sl.U[mb.cur], non_blocking=True)
+                            sl.P_host.copy_(sl.P[mb.cur], non_blocking=True)
+                            p.stat_host[5 * m:5 * m + 5].copy_(p.stat[5 * m:5 * m + 5], non_blocking=True)
+                            mb.final = torch.cuda.Event()
+                            mb.final.record(st)
+        wall = time.perf_counter() - t0
+        lat = np.array([d["latency"] for d in done])
+        steps = sum(r.steps for r in reqs)
+        return done, {"requests": len(done), "wall_s": wall, "solves_per_s": len(done) / wall,
+                      "steps_per_s": steps / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                      "p99_ms": float(np.percentile(lat, 99) * 1e3), "capacity_ctas": self.capacity,
+                      "members": {n: p.k for n, p in packs.items()},
+                      "share_ctas": {n: p.ctas for n, p in packs.items()}}
+
+
 def run_plain(requests, server=None):
     """The plain FP64 path: the same requests one after another on the whole
     device (full CTA capacity), each synchronised before the next; returns

@@ -135,25 +135,30 @@ def test_mixed_q2_periodic_mean_zero_matches_fp64(_cuda, n):
     np.testing.assert_array_equal(xm, xm2)
 
 
-def _tg_mixed_cfg(mod, n, precision=None):
+def _tg_mixed_cfg(mod, n, precision=None, tol=None):
     from bench import tg_config
     cfg = tg_config(mod, n)
     if precision:
         cfg.solver_config.precision = precision
+    if tol is not None:
+        cfg.solver_config.solver_tol = tol
     return cfg
 
 
 @pytest.mark.gpu
 def test_taylor_green_mixed_steps_match_the_oracle(_cuda):
     """Ten 4-step projection steps of the periodic quad9 Taylor-Green vortex
-    (32 x 32 elements, nu 0.01, dt 1e-3) with the mixed-precision pressure
-    solve, against the oracle's FP64 steps: velocity and pressure within 1e-6."""
+    (32 x 32 elements, nu 0.01, dt 1e-3) with the mixed-precision solves
+    (FP64 refinement to 1e-10), against the oracle's FP64 steps solved to
+    1e-12: velocity and pressure within 1e-6. (Two solves that both stop at a
+    relative residual of 1e-8 differ by up to the pressure operator's condition
+    number times 1e-8, a few 1e-6 here, whatever their precision.)"""
     import oracle.simulation as osim
     import jax_fem_cfd_b200.setup.simulation as gsim
     from bench import tg_initial
     res = []
     for mod, prec in ((gsim, "mixed"), (osim, None)):
-        compute, timestep, nc, *_ = mod.setup(_tg_mixed_cfg(mod, 32, prec))
+        compute, timestep, nc, *_ = mod.setup(_tg_mixed_cfg(mod, 32, prec, 1e-10 if prec else 1e-12))
         ncn = nc.cpu().numpy() if isinstance(nc, torch.Tensor) else np.asarray(nc)
         U, P = tg_initial(ncn)
         U, P = np.asarray(U), np.asarray(P)
@@ -168,13 +173,16 @@ def test_taylor_green_mixed_steps_match_the_oracle(_cuda):
 @pytest.mark.gpu
 def test_cavity_mixed_steps_match_fp64(_cuda):
     """The 64 x 64 quad4 lid-driven cavity (Dirichlet walls: the momentum
-    solve's identity rows) over 20 steps with both solves in mixed precision,
-    against the FP64 steps: within 1e-6, a few refinement cycles per solve."""
+    solve's identity rows) over 20 steps with both solves in mixed precision
+    (FP64 refinement to 1e-10), against the FP64 steps solved to 1e-12: within
+    1e-6, a few refinement cycles per solve."""
     import jax_fem_cfd_b200.setup.simulation as gsim
     from jax_fem_cfd_b200.serving import cavity_config
     out = []
     for prec in ("fp64", "mixed"):
-        compute, timestep, nc, sn, h, nn, gd, Ud = gsim.setup(cavity_config(64, prec))
+        cfg = cavity_config(64, prec)
+        cfg.solver_config.solver_tol = 1e-12 if prec == "fp64" else 1e-10
+        compute, timestep, nc, sn, h, nn, gd, Ud = gsim.setup(cfg)
         Ud = gsim.set_face_velocity(Ud, sn[2], gd, 1.0, nn, var=1)
         U = torch.zeros(2 * nn, dtype=torch.float64, device="cuda")
         P = torch.zeros(nn, dtype=torch.float64, device="cuda")
@@ -186,5 +194,5 @@ def test_cavity_mixed_steps_match_fp64(_cuda):
         assert int(timestep.solver.status.max()) == 0
         out.append((U.cpu().numpy(), P.cpu().numpy(), its))
     (Uf, Pf, _), (Um, Pm, im) = out
-    assert all(1 <= u <= 5 and 1 <= p <= 5 for u, p in im), im
+    assert all(1 <= u <= 8 and 1 <= p <= 8 for u, p in im), im
     assert rel(Um, Uf) < 1e-6 and rel(Pm, Pf) < 1e-6, (rel(Um, Uf), rel(Pm, Pf))

@@ -131,3 +131,68 @@ def test_autotuned_shares_and_graph_chunks(_cuda):
         assert d["status"] == 0 and g[d["rid"]]["status"] == 0
         np.testing.assert_array_equal(d["U"], g[d["rid"]]["U"])
         np.testing.assert_array_equal(d["P"], g[d["rid"]]["P"])
+
+
+@pytest.mark.gpu
+def test_packed_members_equal_their_solo_runs(_cuda):
+    """A Pack of four 32^2 members: three requests with their own viscosity and
+    time step run 3 + 2, 2 + 3 and 1 + 4 steps over two packed launches (so
+    they start the second launch from different buffers), the fourth stays
+    idle. Each result equals its solver's solo fem_step4 steps on the same CTA
+    count bit for bit, with zero statuses; the idle member's buffers are
+    untouched."""
+    from jax_fem_cfd_b200.serving import Pack, Slot, make_requests
+    reqs = make_requests(3, seed=21, sizes=(32,), steps=5)
+    ctas = 3
+    pack = Pack(32, 4, ctas)
+    st = torch.cuda.current_stream()
+    for m, r in enumerate(reqs):
+        pack.slots[m].U[0].copy_(torch.from_numpy(r.U0))
+        pack.slots[m].P[0].zero_()
+    idle = pack.slots[3]
+    idle.U[0].fill_(0.25)
+    idle.P[0].fill_(-0.5)
+    dt = [r.dt for r in reqs] + [1.0]
+    mu = [r.nu for r in reqs] + [0.0]
+    first = [3, 2, 1, 0]
+    pack.step(dt, mu, first, [0, 0, 0, 0], st)
+    cur = [k & 1 for k in first]
+    second = [2, 3, 4, 0]
+    pack.step(dt, mu, second, cur, st)
+    cur = [c ^ (k & 1) for c, k in zip(cur, second)]
+    torch.cuda.synchronize()
+    stat = pack.stat.cpu().numpy().reshape(4, 5)
+    assert (stat[:3, 2:] == 0).all(), stat
+    assert (stat[:3, :2] > 0).all(), stat
+    assert torch.equal(idle.U[0], torch.full_like(idle.U[0], 0.25))
+    assert torch.equal(idle.P[0], torch.full_like(idle.P[0], -0.5))
+    solo = Slot(32)
+    solo.set_ctas(ctas)
+    for m, r in enumerate(reqs):
+        solo.U[0].copy_(torch.from_numpy(r.U0))
+        solo.P[0].zero_()
+        c = solo.steps(0, 5, r.dt, r.nu, st)
+        torch.cuda.synchronize()
+        assert int(solo.solver.status.max()) == 0
+        assert torch.equal(pack.slots[m].U[cur[m]], solo.U[c]), m
+        assert torch.equal(pack.slots[m].P[cur[m]], solo.P[c]), m
+    pack.close()
+
+
+@pytest.mark.gpu
+def test_packed_server_matches_the_stream_server(_cuda):
+    """Seven requests of two sizes through packs of two members each (so
+    members are reused) give the stream server's results on the same CTA
+    shares, bit for bit."""
+    from jax_fem_cfd_b200.serving import PackedServer, Server, make_requests
+    reqs = make_requests(7, seed=4, sizes=(32, 64), steps=12)
+    ps = PackedServer(share=16, chunk=4, members={32: 2, 64: 2})
+    packed, m = ps.run(reqs, realtime=False)
+    assert m["requests"] == len(reqs) and m["members"] == {32: 2, 64: 2}
+    srv = Server(share=16, chunk=4)
+    ref, _ = srv.run(reqs, realtime=False)
+    by_id = {d["rid"]: d for d in ref}
+    for d in packed:
+        assert d["status"] == 0 and by_id[d["rid"]]["status"] == 0
+        np.testing.assert_array_equal(d["U"], by_id[d["rid"]]["U"])
+        np.testing.assert_array_equal(d["P"], by_id[d["rid"]]["P"])
