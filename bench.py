@@ -283,6 +283,49 @@ def tg_mixed(args, fp64_final, coords):
             "rel_err_vs_analytic_velocity": {"fp64": rel(Uf, Ua), "mixed": rel(U, Ua)}}
 
 
+def tg_mixed_long(steps=500, size=256):
+    """The Taylor-Green workload over `steps` steps (the config's 500 by
+    default) in FP64 and in mixed precision from the same analytic start, each
+    at the step's tol 1e-8: steps/s of each (CUDA events per step, L2 flushed
+    between steps), the mixed state against the FP64 one after every 100
+    steps, and both against the analytic decay."""
+    import torch
+
+    import jax_fem_cfd_b200.setup.simulation as sim
+    dt, rho, mu = 1e-3, 1.0, 0.01
+    dev = torch.device("cuda", torch.cuda.current_device())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        cfg = tg_config(sim, size)
+        cfg.solver_config.precision = prec
+        compute, timestep, nc, sn, h, nn, gd, Ud = sim.setup(cfg)
+        U0, P0 = tg_initial(nc.cpu().numpy())
+        U, P = torch.as_tensor(U0, device=dev), torch.as_tensor(P0, device=dev)
+        Fp, F = compute(Ud, None, 0.0, dt)
+        ms, snaps = 0.0, []
+        for k in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            U, P, ui, pi = timestep(U, P, dt, rho, mu, Ud, Fp, F)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            if (k + 1) % 100 == 0 or k + 1 == steps:
+                snaps.append((k + 1, U.clone(), P.clone()))
+        runs[prec] = (steps / (ms * 1e-3), snaps, U0)
+    rel = lambda a, b: float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    (v64, s64, U0), (vmx, smx, _) = runs["fp64"], runs["mixed"]
+    errs = {str(k): {"U": rel(Um, Uf), "P": rel(Pm, Pf)} for (k, Uf, Pf), (_, Um, Pm) in zip(s64, smx)}
+    Ua = torch.as_tensor(U0, device=dev) * np.exp(-2 * mu * steps * dt)
+    return {"workload": f"Taylor-Green {size}x{size} Q2 periodic, nu 0.01, dt 1e-3, {steps} steps, tol 1e-8",
+            "fp64_steps_per_s": v64, "mixed_steps_per_s": vmx, "mixed_speedup": vmx / v64,
+            "mixed_rel_err_vs_fp64_by_step": errs,
+            "rel_err_vs_analytic_velocity": {"fp64": rel(s64[-1][1], Ua), "mixed": rel(smx[-1][1], Ua)}}
+
+
 def _dist_device():
     """Device of the collectives' tensors: CUDA under NCCL, host under gloo."""
     import torch.distributed as dist
@@ -774,7 +817,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse", "channel3d",
-                                       "cavity"],
+                                       "cavity", "tg_mixed"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=1024, help="--only serving: requests in the stream")
     ap.add_argument("--channel-nx", type=int, default=256, help="--only channel3d: elements along x (y, z: nx / 4)")
@@ -787,7 +830,8 @@ def main():
               "poisson": lambda: {f"poisson_{args.size}x{args.size}_q1": poisson(args.size)},
               "serving": lambda: serving(args.requests, args.request_steps), "inverse": inverse,
               "channel3d": lambda: channel3d(args.steps, preconds=tuple(args.preconds.split(",")),
-                                             nx=args.channel_nx), "cavity": cavity}[args.only]
+                                             nx=args.channel_nx), "cavity": cavity,
+              "tg_mixed": lambda: tg_mixed_long(500, args.size)}[args.only]
         print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup

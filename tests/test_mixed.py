@@ -196,3 +196,25 @@ def test_cavity_mixed_steps_match_fp64(_cuda):
     (Uf, Pf, _), (Um, Pm, im) = out
     assert all(1 <= u <= 8 and 1 <= p <= 8 for u, p in im), im
     assert rel(Um, Uf) < 1e-6 and rel(Pm, Pf) < 1e-6, (rel(Um, Uf), rel(Pm, Pf))
+
+
+@pytest.mark.gpu
+def test_taylor_green_mixed_500_steps_match_the_oracle(_cuda):
+    """The Taylor-Green vortex over the config's 500 steps (quad9 16 x 16,
+    nu 0.01, dt 1e-3) with both solves in mixed precision (FP64 refinement to
+    1e-10), against the oracle's FP64 steps solved to 1e-12: within 1e-6."""
+    import oracle.simulation as osim
+    import jax_fem_cfd_b200.setup.simulation as gsim
+    from bench import tg_initial
+    res = []
+    for mod, prec in ((gsim, "mixed"), (osim, None)):
+        compute, timestep, nc, *_ = mod.setup(_tg_mixed_cfg(mod, 16, prec, 1e-10 if prec else 1e-12))
+        ncn = nc.cpu().numpy() if isinstance(nc, torch.Tensor) else np.asarray(nc)
+        U, P = tg_initial(ncn)
+        U, P = np.asarray(U), np.asarray(P)
+        for _ in range(500):
+            U, P, ui, pi = timestep(U, P, 1e-3, 1.0, 0.01, None, 0.0, 0.0)
+        res.append((np.asarray(U.cpu() if isinstance(U, torch.Tensor) else U),
+                    np.asarray(P.cpu() if isinstance(P, torch.Tensor) else P)))
+    (Um, Pm), (Uo, Po) = res
+    assert rel(Um, Uo) < 1e-6 and rel(Pm, Po) < 1e-6, (rel(Um, Uo), rel(Pm, Po))
