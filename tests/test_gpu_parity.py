@@ -254,9 +254,12 @@ STEP_CASES = {
     # the lid-driven cavity at its full size and length: 64^2 Q1, Re 100, dt 0.01, 200 steps
     "cavity64_q1_mg_200_steps": (([64, 64], [1, 1], 1, False, [0, 1, 2, 3], "multigrid", True, 1e-8, [4, 4]),
                                  "corners", 200, 0.01, 0.01),
-    # the periodic Taylor-Green workload at full size (256^2 Q2, 263,169 nodes), first 2 steps
-    "tg256_q2p_mg": (([256, 256], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]), None, 2,
+    # the periodic Taylor-Green workload at full size (256^2 Q2, 263,169 nodes), first 10 steps
+    "tg256_q2p_mg": (([256, 256], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]), None, 10,
                      1e-3, 0.01),
+    # the Taylor-Green workload's full length (500 steps) on 64^2 Q2
+    "tg64_q2p_mg_500_steps": (([64, 64], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]),
+                              None, 500, 1e-3, 0.01),
 }
 
 

@@ -196,3 +196,21 @@ def test_packed_server_matches_the_stream_server(_cuda):
         assert d["status"] == 0 and by_id[d["rid"]]["status"] == 0
         np.testing.assert_array_equal(d["U"], by_id[d["rid"]]["U"])
         np.testing.assert_array_equal(d["P"], by_id[d["rid"]]["P"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_served_and_packed_requests_match_the_oracle(_cuda, n):
+    """One request of each larger mesh size, 10 steps, served on its own stream
+    and served as a pack member, against the oracle's steps."""
+    from jax_fem_cfd_b200.serving import PackedServer, Server, make_requests
+    req = make_requests(1, seed=30 + n, sizes=(n,), steps=10)[0]
+    U, P = _oracle_steps(req)
+    served, _ = Server(chunk=2).run([req])
+    ps = PackedServer(chunk=4, members={n: 1})
+    packed, _ = ps.run([req], realtime=False)
+    for p in ps.packs.values():
+        p.close()
+    for d in (served[0], packed[0]):
+        assert d["status"] == 0
+        assert rel(d["U"], U) < SOLVE_TOL and rel(d["P"], P) < SOLVE_TOL, (rel(d["U"], U), rel(d["P"], P))
