@@ -628,6 +628,49 @@ def cavity(steps=200, warmup=3, cpu_steps=40):
                          "sample": f"first {cpu_steps} steps of the same workload, numpy oracle, 1 thread"}}}
 
 
+def mg3_vcycle(nx=256, reps=20, warmup=3):
+    """The hex8 multigrid V-cycle of config 3's pressure solve, alone: the
+    channel's pinned-pressure hierarchy (nx x nx/4 x nx/4 elements, 4 levels,
+    Chebyshev degree 3), FP64, launched directly (fem_mg_vcycle; inside the
+    PCG the same kernels run from a CUDA graph with a device-side loop, which
+    profilers cannot split into kernels). A seeded rhs; device time per
+    V-cycle with CUDA events, an L2-sized buffer written between cycles. The
+    Chebyshev step kernel k_mg3_step on the finest level moves 48 algorithmic
+    bytes per node (x_in, r, d, 1/D read; d, x_out written)."""
+    import torch
+
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import ptr, stream
+    from jax_fem_cfd_b200.setup import simulation as sim
+    cfg = sim.Config(mesh="simple", solver="standard",
+                     mesh_config=sim.SimpleMeshConfig(num_elem=[nx, nx // 4, nx // 4], domain_size=[4.0, 1.0, 1.0],
+                                                      shape_func_ord=1, periodic=False),
+                     solver_config=sim.StandardSolverConfig(dirichlet_faces=[0, 2, 3, 4, 5], symmetry_faces=[],
+                                                            outlet_faces=[1], streamline_diff=False, solver_tol=1e-8,
+                                                            set_zeroP=True, pressure_precond="multigrid",
+                                                            final_multigrid_mesh=[nx // 8, nx // 32, nx // 32]))
+    compute, timestep, nc, sn, h, nn, gd, Ud = sim.setup(cfg)
+    ctx = timestep.solver.ctx
+    r = torch.as_tensor(np.random.default_rng(0).standard_normal(nn), device="cuda")
+    z = torch.empty_like(r)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        _lib.call("fem_mg_vcycle", ctx.handle, ptr(r), ptr(z), stream())
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("fem_mg_vcycle", ctx.handle, ptr(r), ptr(z), stream())
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return {"workload": f"hex8 channel {nx}x{nx // 4}x{nx // 4} pressure V-cycle (4 levels, Chebyshev degree 3, FP64)",
+            "nodes": nn, "ms_per_vcycle_median": float(np.median(ms)), "reps": reps,
+            "finest_step_algorithmic_bytes": 48 * nn, "finite": bool(torch.isfinite(z).all())}
+
+
 def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid", "multigrid_mixed"), nx=256):
     """3D channel: hex8 256 x 64 x 64 on [0,4] x [0,1] x [0,1] (1,048,576
     elements, 1,090,625 nodes), parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
@@ -817,7 +860,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse", "channel3d",
-                                       "cavity", "tg_mixed"],
+                                       "cavity", "tg_mixed", "mg3_vcycle"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=1024, help="--only serving: requests in the stream")
     ap.add_argument("--channel-nx", type=int, default=256, help="--only channel3d: elements along x (y, z: nx / 4)")
@@ -831,7 +874,8 @@ def main():
               "serving": lambda: serving(args.requests, args.request_steps), "inverse": inverse,
               "channel3d": lambda: channel3d(args.steps, preconds=tuple(args.preconds.split(",")),
                                              nx=args.channel_nx), "cavity": cavity,
-              "tg_mixed": lambda: tg_mixed_long(500, args.size)}[args.only]
+              "tg_mixed": lambda: tg_mixed_long(500, args.size),
+              "mg3_vcycle": lambda: mg3_vcycle(args.channel_nx)}[args.only]
         print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup

@@ -424,14 +424,15 @@ class PackedServer:
     time on `share`-capped CTAs, timed before the clock starts). Results are
     each request's solo results on its CTA share, bit for bit, whatever the mix."""
 
-    def __init__(self, share=16, chunk=10, keep_results=True, members=None):
+    def __init__(self, share=16, chunk=10, keep_results=True, members=None, ctas_by_size=None):
         self.share, self.chunk, self.keep_results = share, chunk, keep_results
         self.members = dict(members or {})  # n -> members of that size's pack (overrides the split)
+        self.ctas_by_size = dict(ctas_by_size or {})  # n -> CTAs per member (overrides the share)
         self.packs = {}
         self.capacity = None
 
     def ctas(self, n):
-        return ctas_for(n, self.share)
+        return self.ctas_by_size.get(n) or ctas_for(n, self.share)
 
     def _step_ms(self, n):
         """Time of one step of a size-n request on its CTA share (one solver, 4 steps)."""
@@ -470,6 +471,16 @@ class PackedServer:
             if out[n] == 1:
                 break
             out[n] -= 1
+        # CTAs left over: one more member at a time to the size that would
+        # otherwise finish last
+        count = {n: sum(r.n == n for r in requests) for n in sizes}
+        while True:
+            free = self.capacity - sum(out[n] * self.ctas(n) for n in sizes)
+            grow = [n for n in sizes if n not in self.members and self.ctas(n) <= free and out[n] < min(count[n], 64)]
+            if not grow:
+                break
+            n = max(grow, key=lambda m: work[m] / out[m])
+            out[n] += 1
         return out
 
     def prewarm(self, requests):
