@@ -474,6 +474,8 @@ def serving(count, steps, plain_sample=128):
     # packed launches: every size's requests as members of one persistent kernel per chunk
     from jax_fem_cfd_b200.serving import PackedServer
     ps = PackedServer(share=tune["picked"], keep_results=False)
+    ptune = ps.autotune(reqs)
+    out["autotune_packed"] = ptune
     plan = ps.prewarm(reqs)
     ps.run(reqs[:min(16, count)], realtime=False)  # first launches of each pack
     dpk, pk = ps.run(reqs, realtime=False)

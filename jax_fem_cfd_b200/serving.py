@@ -434,6 +434,41 @@ class PackedServer:
     def ctas(self, n):
         return self.ctas_by_size.get(n) or ctas_for(n, self.share)
 
+    def autotune(self, requests, candidates=None, sample=64):
+        """Pick the CTAs per member of each size by serving a sample of the
+        stream (its first `sample` requests at their full length, all at t = 0)
+        under a few maps and keeping the one with the most solves per second
+        (self.ctas_by_size). The default candidates range from the stream
+        server's share down to one CTA for the smallest meshes: packed members
+        run whole steps inside one launch, so fewer CTAs per member and more
+        members can win where a launch per step could not. Returns the table."""
+        cands = candidates or [{}, {32: 1, 64: 2, 128: 4, 256: 8}, {32: 1, 64: 1, 128: 2, 256: 4},
+                               {32: 1, 64: 2, 128: 8, 256: 16}, {32: 2, 64: 4, 128: 8, 256: 8}]
+        trial = requests[:sample]
+        keep = self.keep_results
+        self.keep_results = False
+        table = []
+        for cb in cands:
+            self.ctas_by_size = dict(cb)
+            for p in self.packs.values():
+                p.close()
+            self.packs = {}
+            self.prewarm(trial)
+            self.run(trial[:8], realtime=False)
+            _, m = self.run(trial, realtime=False)
+            table.append((m["solves_per_s"], cb))
+        best = max(table, key=lambda t: t[0])[1]
+        self.ctas_by_size = dict(best)
+        for p in self.packs.values():
+            p.close()
+        self.packs = {}
+        self.keep_results = keep
+        return {"picked": {n: self.ctas(n) for n in sorted({r.n for r in requests})},
+                "sample_solves_per_s": [{"ctas": {n: ctas_for(n, self.share) if n not in cb else cb[n]
+                                                  for n in sorted({r.n for r in requests})}, "solves_per_s": v}
+                                        for v, cb in table],
+                "sample": f"first {len(trial)} requests"}
+
     def _step_ms(self, n):
         """Time of one step of a size-n request on its CTA share (one solver, 4 steps)."""
         slot = Slot(n)

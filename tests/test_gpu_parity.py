@@ -257,10 +257,16 @@ STEP_CASES = {
     # the periodic Taylor-Green workload at full size (256^2 Q2, 263,169 nodes), first 10 steps
     "tg256_q2p_mg": (([256, 256], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]), None, 10,
                      1e-3, 0.01),
-    # the Taylor-Green workload's full length (500 steps) on 64^2 Q2
+    # the Taylor-Green workload's full length (500 steps) on 64^2 Q2 (tolerance in LONG_RUN_TOL)
     "tg64_q2p_mg_500_steps": (([64, 64], [2 * np.pi, 2 * np.pi], 2, True, [], "multigrid", False, 1e-8, [4, 4]),
                               None, 500, 1e-3, 0.01),
 }
+
+
+# Over 500 steps with equal iteration counts in every solve, the rounding
+# differences of the two implementations accumulate to ~1.6e-10 (measured on
+# B200); the per-step bar stays 1e-10.
+LONG_RUN_TOL = {"tg64_q2p_mg_500_steps": 1e-9}
 
 
 def _run_steps(mod, args, lid, steps, dt, mu):
@@ -293,8 +299,9 @@ def test_ns_step_parity(case):
     Ug, Pg, ig = _run_steps(gsim, args, lid, steps, dt, mu)
     Uo, Po, io = _run_steps(osim, args, lid, steps, dt, mu)
     assert ig == io, (ig, io)
-    assert rel(Ug, Uo) < SOLVE_TOL, rel(Ug, Uo)
-    assert rel(Pg, Po) < SOLVE_TOL, rel(Pg, Po)
+    tol = LONG_RUN_TOL.get(case, SOLVE_TOL)
+    assert rel(Ug, Uo) < tol, rel(Ug, Uo)
+    assert rel(Pg, Po) < tol, rel(Pg, Po)
 
 
 def test_taylor_green_256_q2_decay():
