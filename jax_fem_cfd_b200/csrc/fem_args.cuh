@@ -8,7 +8,7 @@
 #define FEM_THREADS 512
 #define FEM_OP_THREADS 256
 // whole dynamic smem of k_cg / k_vcycle: reduction scratch + tile staging + stencil tables
-#define FEM_DYN_SMEM_MAX ((128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * 8)
+#define FEM_DYN_SMEM_MAX ((128 + FEM_TILE_SMEM + FEM_TAB_SMEM + FEM_BLK_SMEM) * 8)
 // coarse multigrid levels: at most FEM_MG_TEAM CTAs, levels of at most
 // FEM_MG_TEAM_NN nodes (both can be overridden by the environment variables of
 // the same names)

@@ -809,6 +809,31 @@ extern "C" int fem_lattice_restrict(int nhx, int nhy, int nHx, int nHy, int peri
   return fem_launch_restrict(FemLattice{nhx, nhy, periodic ? 1 : 0}, FemLattice{nHx, nHy, periodic ? 1 : 0}, xh, xH, s);
 }
 
+// First multigrid level of the V-cycle run inside CTA 0 from shared memory
+// (mg_block_levels): the coarsest levels, from the team's first level down,
+// whose r and x plus one scratch of the finest of them fit the tile region
+// after the warp CG's buffer and whose 1/D fit FEM_BLK_SMEM; pinned pressure
+// also needs a coarsest level the warp CG takes. c->nlev: none (2D only;
+// FEM_MG_BLOCK=0 turns it off).
+static int mg_block_from(const fem_ctx* c) {
+  const int N = c->nlev;
+  if (N < 2 || c->g.kind == FEM_HEX8) return N;
+  if (const char* ev = getenv("FEM_MG_BLOCK"))
+    if (atoi(ev) == 0) return N;
+  if (c->set_zeroP && c->lv[N - 1].g.nn > FEM_COARSE_WARP_NN) return N;
+  int b = N;
+  long long vec = 0, d = 0;
+  for (int l = N - 1; l >= 1 && l >= c->block_from; --l) {
+    const CtxLevel& L = c->lv[l];
+    if (!L.invD || !L.winvD || !L.r || !L.t) break;
+    vec += 2LL * L.g.nn;
+    d += L.g.nn;
+    if (FEM_COARSE_WARP_NN + vec + L.g.nn > FEM_TILE_SMEM || d > FEM_BLK_SMEM) break;
+    b = l;
+  }
+  return b;
+}
+
 static void fill_cg_args(fem_ctx* c, CgArgs& A) {
   memset(&A, 0, sizeof(A));
   A.sync = FemSync{c->bar, c->bar + 1, c->err, c->partials, FEM_NSLOTS, c->trace, c->trace_cap};
@@ -846,6 +871,7 @@ static void fill_cg_args(fem_ctx* c, CgArgs& A) {
   }
   // level 0 pins of the plain (non-multigrid) solve are the context gamma_p
   if (c->nlev == 1 || !c->lv[0].pin) A.lv[0].pin = c->pmask;
+  A.block_smem_from = mg_block_from(c);
 }
 
 // CTAs of the coarse-level multigrid team for a launch of `grid` CTAs

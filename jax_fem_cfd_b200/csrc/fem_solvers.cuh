@@ -74,7 +74,9 @@ struct CgArgs {
   int* status;         // device out: FEM_ERR_* of this solve
   double* final_rr;    // device out: final r.r (diagnostics)
   int post;            // final pin / mean fix of solvers/standard.py:119-123
+  int block_smem_from; // first level of the V-cycle run inside CTA 0 from shared memory (nlev: none)
   MgLevel lv[FEM_MAX_LEVELS];
+  const double* bd[FEM_MAX_LEVELS];  // per-CTA shared-memory copies of those levels' 1/D (0 on gamma_p if pinned)
 };
 
 __device__ __forceinline__ void fem_zero_partials(const FemSync& s) {
@@ -123,6 +125,29 @@ __device__ void fem_tables_to_smem(CgArgs& sA, double* stab) {
       L.tab = stab + off;
       L.tab_off = stab + off + m;
       off += 2 * m;
+    }
+  }
+  __syncthreads();
+}
+
+// 1/D of the levels that the V-cycle runs inside CTA 0 (pinned: winvD, whose
+// zeros mark gamma_p), copied into this CTA's shared memory once per launch
+// (FEM_BLK_SMEM doubles); sA.bd[l] points at level l's copy.
+#define FEM_BLK_SMEM 2048
+__device__ __forceinline__ void fem_block_levels_to_smem(CgArgs& sA, double* sbd) {
+  int off = 0;
+  for (int l = sA.block_smem_from; l < sA.nlev; ++l) {
+    const MgLevel& L = sA.lv[l];
+    const double* src = sA.pinned ? L.winvD : L.invD;
+    for (int q = threadIdx.x; q < L.g.nn; q += blockDim.x) sbd[off + q] = src[q];
+    off += L.g.nn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    off = 0;
+    for (int l = sA.block_smem_from; l < sA.nlev; ++l) {
+      sA.bd[l] = sbd + off;
+      off += sA.lv[l].g.nn;
     }
   }
   __syncthreads();
@@ -759,6 +784,260 @@ __device__ __noinline__ bool mg_up(const Team& tm, const Red& red, const CgArgs&
   return tm.sync();
 }
 
+// ---------------------------------------------------------------------------
+// The coarse end of the V-cycle inside one CTA, vectors in shared memory
+// ---------------------------------------------------------------------------
+// Levels s = A.block_smem_from .. N-1 run in CTA 0 with __syncthreads only,
+// as core/multigrid.py:231-330 writes them (explicit means, no lazy affine
+// terms): no grid or team barrier and no global-memory round trip inside.
+// In: u_s = R t_{s-1} (lv[s].r, raw, from the phase that restricted it) and,
+// mean-zero, the sum of t_{s-1} (slot SL_T(s-1)). Out: the level's corrected
+// X_s in lv[s].t and, mean-zero, its sums in SL_X(s) (CTA 0's column; the
+// other columns of that slot stay zero), which the up-sweep of level s-1
+// consumes as it would a team level's. Vectors r_l, x_l of every block level
+// and one scratch sit in the tile region after the coarse warp CG's p buffer.
+
+// stencil of level L (table tab) at unique node (ix, iy) on the unique-lattice
+// vector v (wrapped, or clamped where the table's coefficient is zero)
+template <int KIND>
+__device__ __forceinline__ double mg_blk_stencil(const MgLevel& L, const double* __restrict__ tab,
+                                                 const double* __restrict__ v, int ix, int iy) {
+  constexpr int R = KI<KIND>::R, W = KI<KIND>::W, NOFF = KI<KIND>::NOFF;
+  const FemGrid& g = L.g;
+  const int per = g.periodic, nnx = g.nnx, nny = g.nny;
+  const int nc = fem_axis_ncls(KIND, per);
+  const double* c = tab + (size_t)(fem_axis_cls(KIND, per, iy, g.ney) * nc + fem_axis_cls(KIND, per, ix, g.nex)) * NOFF;
+  double y = 0.0;
+#pragma unroll
+  for (int dy = 0; dy < W; ++dy) {
+    int w = iy + dy - R;
+    w = per ? fem_wrap(w, nny) : min(max(w, 0), nny - 1);
+#pragma unroll
+    for (int dx = 0; dx < W; ++dx) {
+      int u = ix + dx - R;
+      u = per ? fem_wrap(u, nnx) : min(max(u, 0), nnx - 1);
+      y += c[dy * W + dx] * v[w * nnx + u];
+    }
+  }
+  return y;
+}
+
+// R t at coarse unique node (Rr, Cc) of the level below F (the sums of mg_down)
+__device__ __forceinline__ double mg_blk_restrict(const FemLattice& F, const double* __restrict__ t, int Rr, int Cc) {
+  const int fy = 2 * Rr, fx = 2 * Cc, ux = F.ux(), uy = F.uy();
+  const bool up = fy + 1 < F.ny, dn = fy - 1 >= 0, rt = fx + 1 < F.nx, lf = fx - 1 >= 0;
+  auto at = [&](int y, int x) -> double {
+    y = y >= uy ? y - uy : y;
+    x = x >= ux ? x - ux : x;
+    return t[y * ux + x];
+  };
+  double e = 0.0, d = 0.0;
+  if (up) e += at(fy + 1, fx);
+  if (dn) e += at(fy - 1, fx);
+  if (rt) e += at(fy, fx + 1);
+  if (lf) e += at(fy, fx - 1);
+  if (up && rt) d += at(fy + 1, fx + 1);
+  if (up && lf) d += at(fy + 1, fx - 1);
+  if (dn && rt) d += at(fy - 1, fx + 1);
+  if (dn && lf) d += at(fy - 1, fx - 1);
+  return at(fy, fx) + 0.5 * e + 0.25 * d;
+}
+
+// P x at fine unique node (fr, fc) from the coarse unique-lattice vector x
+// (core/multigrid.py:90-140, the arithmetic of mg_up)
+__device__ __forceinline__ double mg_blk_prolong(const FemLattice& C, const double* __restrict__ x, int fr, int fc) {
+  const int cux = C.ux(), cuy = C.uy(), Rr = fr >> 1, Cc = fc >> 1;
+  auto xH = [&](int dr, int dc) -> double {
+    int r = Rr + dr, c = Cc + dc;
+    r = r >= cuy ? r - cuy : r;
+    c = c >= cux ? c - cux : c;
+    return x[r * cux + c];
+  };
+  if (!(fr & 1) && !(fc & 1)) return xH(0, 0);
+  if (!(fr & 1)) return 0.5 * xH(0, 0) + 0.5 * xH(0, 1);
+  if (!(fc & 1)) return 0.5 * xH(0, 0) + 0.5 * xH(1, 0);
+  return 0.25 * xH(0, 0) + 0.25 * xH(0, 1) + 0.25 * xH(1, 0) + 0.25 * xH(1, 1);
+}
+
+// mean of a block-local sum (every thread gets it)
+__device__ __forceinline__ double mg_blk_mean(double v, int nn, double* smem) {
+  double a[1] = {v};
+  fem_block_sum<1>(a, smem);
+  return a[0] / nn;
+}
+
+template <int KIND, bool PIN>
+__device__ __noinline__ void mg_block_levels(const GridReducer& gr, const CgArgs& A, double* smem) {
+  const BlockTeam tm;
+  const int N = A.nlev, s = A.block_smem_from;
+  const double w = 2.0 / 3.0;
+  double* base = smem + 128 + FEM_COARSE_WARP_NN;
+  // r_l at base + ro(l), x_l right after it; the scratch after the last level
+  auto ro = [&](int l) {
+    int o = 0;
+    for (int m = s; m < l; ++m) o += 2 * A.lv[m].g.nn;
+    return o;
+  };
+  double* tv = base + ro(N);
+  // 1. the stored rhs of level s: u_s (pinned), or R(t - mean t) - its mean
+  {
+    const MgLevel& L = A.lv[s];
+    const int nn = L.g.nn, ux = L.lat.ux();
+    double* r = base + ro(s);
+    double alpha = 0.0;
+    if (!PIN) {
+      const int sl[1] = {SL_T(s - 1)};
+      double u[1];
+      gr.result_slots<1>(u, sl, smem);
+      alpha = u[0] * A.lv[s - 1].inv_nn;
+    }
+    double a = 0.0;
+    for (int i = tm.rank(); i < nn; i += tm.size()) {
+      double v = L.r[i];
+      if (!PIN) v -= alpha * fem_restrict_rowsum(L.lat, i / ux, i % ux);
+      r[i] = v;
+      a += v;
+    }
+    if (!PIN) {
+      const double beta = mg_blk_mean(a, nn, smem);
+      for (int i = tm.rank(); i < nn; i += tm.size()) r[i] -= beta;
+    }
+    __syncthreads();
+  }
+  // 2. down: pre-smooth from zero, residual, restriction
+  for (int n = s; n < N - 1; ++n) {
+    const MgLevel& L = A.lv[n];
+    const MgLevel& C = A.lv[n + 1];
+    const int nn = L.g.nn, ux = L.lat.ux(), cux = C.lat.ux(), cnn = C.g.nn;
+    const double* __restrict__ d = A.bd[n];
+    double* r = base + ro(n);
+    double* x = r + nn;
+    double* rc = base + ro(n + 1);
+    const double mr = PIN ? 0.0 : mg_blk_mean([&] {
+      double a = 0.0;
+      for (int i = tm.rank(); i < nn; i += tm.size()) a += r[i];
+      return a;
+    }(), nn, smem);
+    double a = 0.0;
+    for (int i = tm.rank(); i < nn; i += tm.size()) {
+      const double rh = PIN ? (d[i] == 0.0 ? 0.0 : r[i]) : r[i] - mr;
+      const double xh = w * rh * d[i];
+      tv[i] = rh;
+      x[i] = xh;
+      a += xh;
+    }
+    if (!PIN) {
+      const double mx = mg_blk_mean(a, nn, smem);
+      for (int i = tm.rank(); i < nn; i += tm.size()) x[i] -= mx;
+    }
+    __syncthreads();
+    a = 0.0;
+    for (int i = tm.rank(); i < nn; i += tm.size()) {
+      double Lx = mg_blk_stencil<KIND>(L, L.tab, x, i % ux, i / ux);
+      if (PIN && d[i] == 0.0) Lx = 0.0;
+      const double t = tv[i] - Lx;
+      tv[i] = t;
+      a += t;
+    }
+    if (!PIN) {
+      const double mt = mg_blk_mean(a, nn, smem);
+      for (int i = tm.rank(); i < nn; i += tm.size()) tv[i] -= mt;
+    }
+    __syncthreads();
+    a = 0.0;
+    for (int I = tm.rank(); I < cnn; I += tm.size()) {
+      const double v = mg_blk_restrict(L.lat, tv, I / cux, I % cux);
+      rc[I] = v;
+      a += v;
+    }
+    if (!PIN) {
+      const double mh = mg_blk_mean(a, cnn, smem);
+      for (int I = tm.rank(); I < cnn; I += tm.size()) rc[I] -= mh;
+    }
+    __syncthreads();
+  }
+  // 3. coarsest level: one Jacobi sweep from zero (mean-zero) or the warp CG (pinned)
+  {
+    const MgLevel& L = A.lv[N - 1];
+    const int nn = L.g.nn;
+    const double* __restrict__ d = A.bd[N - 1];
+    double* r = base + ro(N - 1);
+    double* x = r + nn;
+    if (!PIN) {
+      double a = 0.0;
+      for (int i = tm.rank(); i < nn; i += tm.size()) a += r[i];
+      const double mr = mg_blk_mean(a, nn, smem);
+      a = 0.0;
+      for (int i = tm.rank(); i < nn; i += tm.size()) {
+        const double v = w * (r[i] - mr) * d[i];
+        x[i] = v;
+        a += v;
+      }
+      const double mx = mg_blk_mean(a, nn, smem);
+      for (int i = tm.rank(); i < nn; i += tm.size()) x[i] -= mx;
+    } else if constexpr (PIN && KIND != FEM_HEX8) {
+      for (int i = tm.rank(); i < nn; i += tm.size()) L.r[i] = r[i];
+      __syncthreads();
+      if (threadIdx.x < 32) mg_coarse_warp<KIND>(A, smem + 128);
+      __syncthreads();
+      for (int i = tm.rank(); i < nn; i += tm.size()) x[i] = L.t[i];
+    }
+    __syncthreads();
+  }
+  // 4. up: prolongate, add, one weighted Jacobi sweep
+  for (int n = N - 2; n >= s; --n) {
+    const MgLevel& L = A.lv[n];
+    const MgLevel& C = A.lv[n + 1];
+    const int nn = L.g.nn, ux = L.lat.ux();
+    const double* __restrict__ d = A.bd[n];
+    double* r = base + ro(n);
+    double* x = r + nn;
+    const double* xc = base + ro(n + 1) + C.g.nn;
+    double a = 0.0;
+    for (int i = tm.rank(); i < nn; i += tm.size()) {
+      const double p = mg_blk_prolong(C.lat, xc, i / ux, i % ux);
+      tv[i] = p;
+      a += p;
+    }
+    const double mp = PIN ? 0.0 : mg_blk_mean(a, nn, smem);
+    for (int i = tm.rank(); i < nn; i += tm.size()) {
+      const double y = x[i] + (tv[i] - mp);
+      tv[i] = (PIN && d[i] == 0.0) ? 0.0 : y;
+    }
+    __syncthreads();
+    a = 0.0;
+    for (int i = tm.rank(); i < nn; i += tm.size()) {
+      const double off = mg_blk_stencil<KIND>(L, L.tab_off, tv, i % ux, i / ux);
+      double xn = w * (r[i] - off) * d[i] + (1.0 - w) * tv[i];
+      if (PIN && d[i] == 0.0) xn = 0.0;
+      x[i] = xn;
+      a += xn;
+    }
+    if (!PIN) {
+      const double mj = mg_blk_mean(a, nn, smem);
+      for (int i = tm.rank(); i < nn; i += tm.size()) x[i] -= mj;
+    }
+    __syncthreads();
+  }
+  // 5. X_s out, with its sums for the level above (mean-zero)
+  {
+    const MgLevel& L = A.lv[s];
+    const int nn = L.g.nn, ux = L.lat.ux();
+    const double* x = base + ro(s) + nn;
+    double a[2] = {0.0, 0.0};
+    for (int i = tm.rank(); i < nn; i += tm.size()) {
+      const double v = x[i];
+      L.t[i] = v;
+      if (!PIN) {
+        a[0] += v;
+        a[1] += fem_interp_colsum(L.lat, i / ux, i % ux) * v;
+      }
+    }
+    if (!PIN) gr.reduce<2>(a, SL_X(s), smem);
+    __syncthreads();
+  }
+}
+
 // Full V-cycle on r = lv[0].r; result in lv[0].t (raw; mean-zero subtracts
 // SL_X(0)[0]/nn lazily). Levels < block_from run on the whole grid; levels from
 // block_from down run on the team of the first A.team CTAs (GridTeam::team barriers,
@@ -771,12 +1050,19 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
   const int N = A.nlev, s = A.block_from;
   for (int n = 0; n < s; ++n)
     if (!mg_down<KIND, PIN>(gt, gr, A, n, smem)) return false;
+  const int b = A.block_smem_from < N ? A.block_smem_from : N - 1;  // team levels: [s, b)
   if ((int)blockIdx.x < A.team) {
     const GridTeam tt = GridTeam::team(gt.s, team_round, A.team);
-    for (int n = s; n < N - 1; ++n)
+    for (int n = s; n < b; ++n)
       if (!mg_down<KIND, PIN>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 7);
-    if (blockIdx.x == 0) {
+    if (b < N - 1 || A.block_smem_from == N - 1) {
+      // levels b.. inside CTA 0 from shared memory (2D)
+      if constexpr (KIND != FEM_HEX8) {
+        if (blockIdx.x == 0) mg_block_levels<KIND, PIN>(gr, A, smem);
+      }
+      fem_trace_mark(A.sync, 8);
+    } else if (blockIdx.x == 0) {
       bool warp_solve = false;
       if constexpr (PIN && KIND != FEM_HEX8) warp_solve = A.lv[N - 1].g.nn <= FEM_COARSE_WARP_NN;
       if (warp_solve) {
@@ -804,7 +1090,7 @@ __device__ __noinline__ bool mg_vcycle(const GridTeam& gt, const GridReducer& gr
       }
     }
     if (!tt.sync()) return false;
-    for (int n = N - 2; n >= s; --n)
+    for (int n = b - 1; n >= s; --n)
       if (!mg_up<KIND, PIN>(tt, gr, A, n, smem)) return false;
     fem_trace_mark(A.sync, 10);
   }

@@ -4,12 +4,14 @@
 
 template <int KIND, bool PIN>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q) {
-  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables
+  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables,
+  // [.., +FEM_BLK_SMEM) 1/D of the levels run inside CTA 0
   extern __shared__ double smem[];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
   fem_trace_init(sA.sync);
   fem_tables_to_smem<KIND>(sA, smem + 128 + FEM_TILE_SMEM);
+  fem_block_levels_to_smem(sA, smem + 128 + FEM_TILE_SMEM + FEM_TAB_SMEM);
   __shared__ unsigned int s_round, s_team_round;
   if (threadIdx.x == 0) {
     s_round = 0u;
@@ -21,12 +23,14 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_cg(CgArgs Aparam, double* cg
 template <int KIND, bool PIN>
 __global__ void __launch_bounds__(FEM_THREADS, 1) k_vcycle(CgArgs Aparam, double* cg_r, double* cg_p, double* cg_q,
                                                             double* z) {
-  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables
+  // [0,128) reductions, [128, +FEM_TILE_SMEM) tiles, [.., +FEM_TAB_SMEM) stencil tables,
+  // [.., +FEM_BLK_SMEM) 1/D of the levels run inside CTA 0
   extern __shared__ double smem[];
   __shared__ __align__(16) CgArgs sA;
   fem_stage_args(Aparam, &sA);
   fem_trace_init(sA.sync);
   fem_tables_to_smem<KIND>(sA, smem + 128 + FEM_TILE_SMEM);
+  fem_block_levels_to_smem(sA, smem + 128 + FEM_TILE_SMEM + FEM_TAB_SMEM);
   const CgArgs& A = sA;
   __shared__ unsigned int s_round, s_team_round;
   if (threadIdx.x == 0) {
@@ -86,13 +90,13 @@ int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq,
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq};
   return coop_launch(cg_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_cg",
-                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * sizeof(double));
+                     (size_t)FEM_DYN_SMEM_MAX);
 }
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq, &z};
   return coop_launch(vc_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_vcycle",
-                     (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM) * sizeof(double));
+                     (size_t)FEM_DYN_SMEM_MAX);
 }
 int fem_coop_occupancy_cg(int* occ) {
   int m = 1 << 30;

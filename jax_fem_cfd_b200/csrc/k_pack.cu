@@ -23,8 +23,9 @@
 #include "fem_step_body.cuh"
 
 // dynamic smem (doubles): [0,128) reductions | tiles of the convection apply,
-// the BiCGSTAB operator and the CG phases | CG stencil tables
-#define FEM_PACK_SMEM (128 + FEM_CONV_SMEM + FEM_TAB_SMEM)
+// the BiCGSTAB operator and the CG phases | CG stencil tables | 1/D of the
+// multigrid levels run inside one CTA
+#define FEM_PACK_SMEM (128 + FEM_CONV_SMEM + FEM_TAB_SMEM + FEM_BLK_SMEM)
 static_assert(FEM_CONV_SMEM >= FEM_TILE_SMEM, "the tile region holds the CG tiles too");
 
 template <int KIND>
@@ -44,6 +45,7 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_step_pack(const PackMember* 
   fem_stage_args(M.B, &sB);
   fem_stage_args(M.S, &sS);
   fem_tables_to_smem<KIND>(sC, smem + 128 + FEM_CONV_SMEM);
+  fem_block_levels_to_smem(sC, smem + 128 + FEM_CONV_SMEM + FEM_TAB_SMEM);
   const double theta = 0.5, rho = 1.0, dt = ps.dt, mu = ps.mu;
   // the momentum operator's shared matrix (the solo step's k_lincomb expression)
   const double ka = rho / dt, kb = theta * mu;
