@@ -125,8 +125,12 @@ def test_element_data_and_products(key):
         assert err < OPS_TOL, (key, name, err)
 
 
+@pytest.mark.parametrize("block", ["0", "1"])
 @pytest.mark.parametrize("key", ["q1", "q2", "q1p", "q2p"])
-def test_multigrid_transfers_and_vcycle(key):
+def test_multigrid_transfers_and_vcycle(key, block, monkeypatch):
+    """The golden V-cycles; block = "1" runs the coarsest levels inside CTA 0
+    from shared memory (FEM_MG_BLOCK=1), "0" on the coarse-level team."""
+    monkeypatch.setenv("FEM_MG_BLOCK", block)
     from jax_fem_cfd_b200.core import multigrid as mg
     from jax_fem_cfd_b200.setup import regular_mesh as rm
     from jax_fem_cfd_b200.core import shape_functions as sf
@@ -287,6 +291,14 @@ def _run_steps(mod, args, lid, steps, dt, mu):
         U, P, ui, pi = timestep(U, P, dt, 1.0, mu, Ud, Fp, F)
         its.append((int(ui), int(pi)))
     return np_(U), np_(P), its
+
+
+@pytest.mark.parametrize("case", ["cavity_q1_mg", "tg_q2p_mg", "cavity64_q1_mg", "tg64_q2p_mg"])
+def test_ns_step_parity_block_levels(case, monkeypatch):
+    """The multigrid step cases with the coarsest levels inside CTA 0
+    (FEM_MG_BLOCK=1): equal iteration counts and 1e-10 against the oracle."""
+    monkeypatch.setenv("FEM_MG_BLOCK", "1")
+    test_ns_step_parity(case)
 
 
 @pytest.mark.parametrize("case", list(STEP_CASES))
@@ -456,14 +468,17 @@ def _channel3d_cfg(mod, precond, nel):
                                                              final_multigrid_mesh=None))
 
 
-@pytest.mark.parametrize("precond", ["jacobi", "approx_inv"])
-def test_hex8_channel_step_parity(precond):
+@pytest.mark.parametrize("precond,otf", [("jacobi", "0"), ("approx_inv", "0"), ("jacobi", "1")])
+def test_hex8_channel_step_parity(precond, otf, monkeypatch):
     """The 3D channel's boundary set at a small size (hex8 16 x 8 x 8 on
     [0,4] x [0,1] x [0,1]): parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
     zero-traction outlet (P = 0) on x = 4, no-slip walls, Re 200, dt 2e-3;
-    3 steps of fem_step4 vs the oracle, boundary integral included."""
+    3 steps of fem_step4 vs the oracle, boundary integral included. otf = "1"
+    runs the momentum operator with Ce applied on the fly (FEM_CONV_OTF=1, the
+    TMA-staged hex8 form), "0" with the explicit Ce (the hex8 default)."""
     import oracle.simulation as osim
     import jax_fem_cfd_b200.setup.simulation as gsim
+    monkeypatch.setenv("FEM_CONV_OTF", otf)
     out = []
     for mod in (gsim, osim):
         compute, timestep, nc, sn, h, nn, gd, Ud = mod.setup(_channel3d_cfg(mod, precond, [16, 8, 8]))
