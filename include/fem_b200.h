@@ -424,8 +424,8 @@ const char* fem_last_error(void);
  * precision) with its ping-pong fields (U[0], P[0]) = (U0[m], P0[m]) and
  * (U[1], P[1]) = (U1[m], P1[m]) and its Dirichlet values Ud[m]; every member's
  * cooperative CTA count (its max-CTA cap, fem_ctx_set_max_ctas) must be the
- * same, and k x that count must fit on the device at once (FEM_E_STATE
- * otherwise). stat: device int32 [k * 5], per member the momentum and
+ * same and fit on the device (FEM_E_STATE otherwise); the members active in
+ * one call must fit together. stat: device int32 [k * 5], per member the momentum and
  * pressure iterations of its last step, their statuses, and at [5m + 4] the
  * OR of every status since the caller last zeroed it. tol and precond have
  * fem_step4's meaning. Each member's step is fem_step4's on the same CTA count
@@ -438,6 +438,8 @@ int fem_pack_create(fem_ctx* const* ctxs, int k, double* const* U0, double* cons
 /* steps[m] steps of member m (0: idle this call) from buffer cur[m] (0 or 1)
  * with its dt[m] and viscosity mu[m] (host arrays of k values, read before
  * the call returns); the result of member m is in buffer cur[m] ^ (steps[m] & 1).
+ * Only the members with steps[m] > 0 are launched, so the launch holds
+ * (active members) x ctas CTAs.
  * Calls on one pack run in stream order; a member's buffers may be written by
  * the caller between calls on the same stream. */
 int fem_pack_step(fem_pack* pack, const double* dt, const double* mu, const int* steps, const int* cur,

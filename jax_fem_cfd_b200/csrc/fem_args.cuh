@@ -67,7 +67,8 @@ struct PackStep {
   int cur;    // buffer (0 or 1) holding the member's current U, P
 };
 struct PackParams {
-  PackStep m[FEM_PACK_MAX];
+  PackStep m[FEM_PACK_MAX];  // per member
+  int idx[FEM_PACK_MAX];     // member of each grid row (blockIdx.y): only the active ones are launched
 };
 
 // ----------------------------------------------------------------------------

@@ -1525,8 +1525,8 @@ extern "C" int fem_pack_create(fem_ctx* const* ctxs, int k, double* const* U0, d
   int per_sm = 0;
   if (fem_pack_occupancy(&per_sm) != 0 || per_sm < 1) return set_err("fem_pack_occupancy", cudaGetLastError());
   const int capacity = per_sm * c0->sms;
-  if (k * ctas > capacity) {
-    snprintf(g_err, sizeof(g_err), "fem_pack_create: %d members x %d CTAs exceed the %d co-resident CTAs", k, ctas,
+  if (ctas > capacity) {
+    snprintf(g_err, sizeof(g_err), "fem_pack_create: %d CTAs per member exceed the %d co-resident CTAs", ctas,
              capacity);
     return FEM_E_STATE;
   }
@@ -1633,16 +1633,21 @@ extern "C" int fem_pack_step(fem_pack* p, const double* dt, const double* mu, co
   if (!p || !dt || !mu || !steps || !cur) return FEM_E_ARG;
   PackParams P;
   memset(&P, 0, sizeof(P));
-  bool any = false;
+  int active = 0;
   for (int m = 0; m < p->k; ++m) {
     if (steps[m] < 0 || (cur[m] != 0 && cur[m] != 1)) return FEM_E_ARG;
     if (steps[m] > 0 && !(dt[m] > 0.0)) return FEM_E_ARG;
     P.m[m] = PackStep{dt[m], mu[m], steps[m], cur[m]};
-    any = any || steps[m] > 0;
+    if (steps[m] > 0) P.idx[active++] = m;
   }
-  if (!any) return FEM_OK;
+  if (!active) return FEM_OK;
+  if (active * p->ctas > p->capacity) {
+    snprintf(g_err, sizeof(g_err), "fem_pack_step: %d active members x %d CTAs exceed the %d co-resident CTAs",
+             active, p->ctas, p->capacity);
+    return FEM_E_STATE;
+  }
   FEM_CHECK(cudaMemsetAsync(p->sync, 0, sizeof(unsigned int) * 3 * p->k, s));
-  return fem_launch_step_pack(FEM_Q1_2D, p->dmem, P, p->k, p->ctas, s);
+  return fem_launch_step_pack(FEM_Q1_2D, p->dmem, P, active, p->ctas, s);
 }
 
 extern "C" int fem_pack_info(const fem_pack* p, int* k, int* ctas, int* capacity) {

@@ -1,9 +1,9 @@
 // Packed 4-step projection step for serving: one persistent cooperative launch
 // advances every active request of one mesh size by `steps` steps.
 //
-// Grid (ctas, k): blockIdx.y is the request (member), its blockIdx.x < ctas CTAs
-// are the group that runs the member's whole step, stage after stage, with the
-// member's own barrier counters. Inside a group the stages are the stage bodies
+// Grid (ctas, active members): blockIdx.y picks an active member (a request),
+// its blockIdx.x < ctas CTAs are the group that runs the member's whole step,
+// stage after stage, with the member's own barrier counters. Inside a group the stages are the stage bodies
 // of the solo kernels (fem_step_body.cuh, the BiCGSTAB and MG-PCG solves), run
 // on the same number of CTAs as the member's solo solves, so a packed request's
 // results equal the solo fem_step4's bit for bit. Groups never wait on each other:
@@ -38,9 +38,10 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_step_pack(const PackMember* 
   __shared__ double sKd[81], sLe[81];
   __shared__ unsigned int s_round, s_team_round;
   constexpr int NEN = KI<KIND>::NEN;
-  const PackStep ps = P.m[blockIdx.y];
-  if (ps.steps <= 0) return;  // idle member: its whole group leaves
-  const PackMember& M = mem[blockIdx.y];
+  const int mi = P.idx[blockIdx.y];  // the member this group runs
+  const PackStep ps = P.m[mi];
+  if (ps.steps <= 0) return;  // (not launched by fem_pack_step; a group with nothing to do leaves)
+  const PackMember& M = mem[mi];
   fem_stage_args(M.C, &sC);
   fem_stage_args(M.B, &sB);
   fem_stage_args(M.S, &sS);

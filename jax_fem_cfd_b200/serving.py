@@ -415,18 +415,19 @@ class _Member:
 
 class PackedServer:
     """Continuous batching with packed launches: the requests of one mesh size
-    are members of that size's Pack, and each launch advances all of a pack's
-    active members by one chunk of steps (one persistent kernel for the whole
-    chunk, no per-step launches). A request is admitted into a free member of
-    its size's pack between launches; up to two chunks per pack are queued on
-    the pack's stream. Members per size: the CTA capacity split in proportion
-    to each size's measured work in the stream (requests x steps x one step's
-    time on `share`-capped CTAs, timed before the clock starts). Results are
-    each request's solo results on its CTA share, bit for bit, whatever the mix."""
+    are members of that size's Pack, and each launch advances the pack's active
+    members by one chunk of steps (one persistent kernel for the whole chunk,
+    no per-step launches and no per-request graphs). Launches are elastic: a
+    launch holds only its active members' CTAs, and every size's pack draws on
+    one budget of co-resident CTAs (the device capacity), so when one size's
+    requests run out, the others take its CTAs. A request is admitted into a
+    free member of its size's pack between that pack's launches; the packs are
+    served oldest work first. Results are each request's solo results on its
+    CTA count, bit for bit, whatever the mix."""
 
     def __init__(self, share=16, chunk=10, keep_results=True, members=None, ctas_by_size=None):
         self.share, self.chunk, self.keep_results = share, chunk, keep_results
-        self.members = dict(members or {})  # n -> members of that size's pack (overrides the split)
+        self.members = dict(members or {})  # n -> members of that size's pack (overrides the default)
         self.ctas_by_size = dict(ctas_by_size or {})  # n -> CTAs per member (overrides the share)
         self.packs = {}
         self.capacity = None
@@ -445,85 +446,49 @@ class PackedServer:
         cands = candidates or [{}, {32: 1, 64: 2, 128: 4, 256: 8}, {32: 1, 64: 1, 128: 2, 256: 4},
                                {32: 1, 64: 2, 128: 8, 256: 16}, {32: 2, 64: 4, 128: 8, 256: 8}]
         trial = requests[:sample]
+        sizes = sorted({r.n for r in requests})
         keep = self.keep_results
         self.keep_results = False
         table = []
         for cb in cands:
             self.ctas_by_size = dict(cb)
-            for p in self.packs.values():
-                p.close()
-            self.packs = {}
+            self.close()
             self.prewarm(trial)
             self.run(trial[:8], realtime=False)
             _, m = self.run(trial, realtime=False)
             table.append((m["solves_per_s"], cb))
         best = max(table, key=lambda t: t[0])[1]
         self.ctas_by_size = dict(best)
+        self.close()
+        self.keep_results = keep
+        return {"picked": {n: self.ctas(n) for n in sizes},
+                "sample_solves_per_s": [{"ctas": {n: cb.get(n) or ctas_for(n, self.share) for n in sizes},
+                                         "solves_per_s": v} for v, cb in table],
+                "sample": f"first {len(trial)} requests"}
+
+    def close(self):
         for p in self.packs.values():
             p.close()
         self.packs = {}
-        self.keep_results = keep
-        return {"picked": {n: self.ctas(n) for n in sorted({r.n for r in requests})},
-                "sample_solves_per_s": [{"ctas": {n: ctas_for(n, self.share) if n not in cb else cb[n]
-                                                  for n in sorted({r.n for r in requests})}, "solves_per_s": v}
-                                        for v, cb in table],
-                "sample": f"first {len(trial)} requests"}
-
-    def _step_ms(self, n):
-        """Time of one step of a size-n request on its CTA share (one solver, 4 steps)."""
-        slot = Slot(n)
-        slot.set_ctas(self.ctas(n))
-        st = torch.cuda.current_stream()
-        slot.steps(0, 2, 0.25 / n, 1e-2, st)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        slot.steps(0, 4, 0.25 / n, 1e-2, st)
-        e1.record(st)
-        e1.synchronize()
-        return e0.elapsed_time(e1) / 4
 
     def plan(self, requests):
-        """Members per size for this stream (see the class doc)."""
+        """Members per size: as many as the requests of that size, up to what
+        the CTA capacity can run at once (and 64, the most a pack takes)."""
         sizes = sorted({r.n for r in requests})
         probe = Slot(sizes[0])
         cap = ctypes.c_int(0)
         _lib.call("fem_ctx_set_max_ctas", probe.solver.ctx.handle, 0, ctypes.byref(cap))
         del probe
-        # the packed kernel holds one CTA per SM, like the solver kernels
-        self.capacity = cap.value
-        work = {n: sum(r.steps for r in requests if r.n == n) * self._step_ms(n) for n in sizes}
-        cta_work = sum(work[n] * self.ctas(n) for n in sizes)
-        out = {}
-        for n in sizes:
-            if n in self.members:
-                out[n] = self.members[n]
-                continue
-            k = int(self.capacity * work[n] / cta_work) if cta_work > 0 else 1
-            out[n] = max(1, min(k, sum(r.n == n for r in requests), 64, self.capacity // self.ctas(n)))
-        # the packs of all sizes must fit on the device at once
-        while sum(out[n] * self.ctas(n) for n in sizes) > self.capacity:
-            n = max(sizes, key=lambda m: out[m] * self.ctas(m))
-            if out[n] == 1:
-                break
-            out[n] -= 1
-        # CTAs left over: one more member at a time to the size that would
-        # otherwise finish last
-        count = {n: sum(r.n == n for r in requests) for n in sizes}
-        while True:
-            free = self.capacity - sum(out[n] * self.ctas(n) for n in sizes)
-            grow = [n for n in sizes if n not in self.members and self.ctas(n) <= free and out[n] < min(count[n], 64)]
-            if not grow:
-                break
-            n = max(grow, key=lambda m: work[m] / out[m])
-            out[n] += 1
-        return out
+        self.capacity = cap.value  # the packed kernel holds one CTA per SM, like the solver kernels
+        return {n: self.members.get(n) or max(1, min(sum(r.n == n for r in requests), 64,
+                                                     self.capacity // self.ctas(n))) for n in sizes}
 
     def prewarm(self, requests):
         """Build the packs (solvers, hierarchies, pack objects) before the clock."""
         plan = self.plan(requests)
         for n, k in plan.items():
             p = self.packs.get(n)
-            if p is None or p.k != k:
+            if p is None or p.k != k or p.ctas != self.ctas(n):
                 if p is not None:
                     p.close()
                 self.packs[n] = Pack(n, k, self.ctas(n))
@@ -540,8 +505,9 @@ class PackedServer:
         packs = {n: self.packs[n] for n in sorted({r.n for r in reqs})}
         streams = {n: torch.cuda.Stream() for n in packs}
         mem = {n: [_Member() for _ in range(p.k)] for n, p in packs.items()}
-        inflight = {n: [] for n in packs}
+        inflight = {n: None for n in packs}  # (event, CTAs held) of the pack's launch in flight
         pending = {n: [] for n in packs}
+        used = 0
         done, nxt = [], 0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -551,29 +517,43 @@ class PackedServer:
                 pending[reqs[nxt].n].append(reqs[nxt])
                 nxt += 1
             for n, p in packs.items():
-                ms, st = mem[n], streams[n]
-                # retire members whose results have landed
-                for m, mb in enumerate(ms):
+                if inflight[n] is not None and inflight[n][0].query():
+                    used -= inflight[n][1]
+                    inflight[n] = None
+                ms = mem[n]
+                for m, mb in enumerate(ms):  # retire members whose results have landed
                     if mb.final is not None and mb.final.query():
                         t = time.perf_counter() - t0
                         sl = p.slots[m]
                         r = mb.req
-                        stat = p.stat_host[5 * m:5 * m + 5]
                         rec = {"rid": r.rid, "n": r.n, "arrival": r.arrival, "admitted": mb.admitted, "done": t,
                                "latency": t - (r.arrival if realtime else 0.0), "ctas": p.ctas,
-                               "status": int(stat[4])}
+                               "status": int(p.stat_host[5 * m + 4])}
                         if self.keep_results:
                             rec["U"] = sl.U_host.numpy().copy()
                             rec["P"] = sl.P_host.numpy().copy()
                         done.append(rec)
                         ms[m] = _Member()
-                inflight[n] = [e for e in inflight[n] if not e.query()]
-                if len(inflight[n]) >= 2:
+
+            # packs without a launch in flight: those with requests under way
+            # first (oldest admission first), then those with arrivals only
+            def age(n):
+                a = [mb.admitted for mb in mem[n] if mb.req is not None and mb.left > 0]
+                if a:
+                    return (0, min(a))
+                return (1, pending[n][0].arrival) if pending[n] else (2, 0.0)
+
+            for n in sorted((n for n in packs if inflight[n] is None), key=age):
+                p, ms, st = packs[n], mem[n], streams[n]
+                room = (self.capacity - used) // p.ctas
+                if room <= 0:
                     continue
-                # admit into free members
+                go = [m for m, mb in enumerate(ms) if mb.req is not None and mb.left > 0][:room]
                 with torch.cuda.stream(st):
-                    for m, mb in enumerate(ms):
-                        if mb.req is None and pending[n]:
+                    for m, mb in enumerate(ms):  # admit into free members while there is room
+                        if len(go) >= room or not pending[n]:
+                            break
+                        if mb.req is None:
                             r = pending[n].pop(0)
                             sl = p.slots[m]
                             sl.U0_host.copy_(torch.from_numpy(r.U0))
@@ -582,19 +562,20 @@ class PackedServer:
                             p.stat[5 * m + 4].zero_()
                             mb.req, mb.cur, mb.left = r, 0, r.steps
                             mb.admitted = time.perf_counter() - t0
-                active = [mb.req is not None and mb.left > 0 for mb in ms]
-                if not any(active):
+                            go.append(m)
+                if not go:
                     continue
-                steps = [min(self.chunk, mb.left) if a else 0 for mb, a in zip(ms, active)]
+                gs = set(go)
+                steps = [min(self.chunk, mb.left) if m in gs else 0 for m, mb in enumerate(ms)]
                 p.step([mb.req.dt if mb.req else 1.0 for mb in ms], [mb.req.nu if mb.req else 0.0 for mb in ms],
                        steps, [mb.cur for mb in ms], st)
                 ev = torch.cuda.Event()
                 ev.record(st)
-                inflight[n].append(ev)
+                inflight[n] = (ev, len(go) * p.ctas)
+                used += len(go) * p.ctas
                 with torch.cuda.stream(st):
-                    for m, (mb, k) in enumerate(zip(ms, steps)):
-                        if k == 0:
-                            continue
+                    for m in go:
+                        mb, k = ms[m], steps[m]
                         mb.cur ^= k & 1
                         mb.left -= k
                         if mb.left == 0:

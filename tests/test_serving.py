@@ -214,3 +214,20 @@ def test_served_and_packed_requests_match_the_oracle(_cuda, n):
     for d in (served[0], packed[0]):
         assert d["status"] == 0
         assert rel(d["U"], U) < SOLVE_TOL and rel(d["P"], P) < SOLVE_TOL, (rel(d["U"], U), rel(d["P"], P))
+
+
+@pytest.mark.gpu
+def test_pack_launch_beyond_capacity_is_refused(_cuda):
+    """Two 100-CTA members do not fit on the device together: a call with both
+    active is refused on the host (nothing launched); one active member runs."""
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.serving import Pack
+    pack = Pack(256, 2, 100)
+    st = torch.cuda.current_stream()
+    with pytest.raises(_lib.FemError):
+        pack.step([1e-3, 1e-3], [1e-2, 1e-2], [1, 1], [0, 0], st)
+    pack.step([1e-3, 1e-3], [1e-2, 1e-2], [1, 0], [0, 0], st)
+    torch.cuda.synchronize()
+    stat = pack.stat.cpu().numpy().reshape(2, 5)
+    assert (stat[0, 2:] == 0).all() and (stat[1] == 0).all(), stat
+    pack.close()
