@@ -673,6 +673,50 @@ def mg3_vcycle(nx=256, reps=20, warmup=3):
             "finest_step_algorithmic_bytes": 48 * nn, "finite": bool(torch.isfinite(z).all())}
 
 
+def cg_trace(size=256):
+    """Phase timeline of one pressure solve of the Taylor-Green step (size^2
+    Q2, after 5 warm-up steps): CTA 0 of the persistent solvers stamps
+    %globaltimer at every grid (tag 31) or team (tag 30) barrier and at the
+    multigrid phase marks (fem_ctx_set_trace), and the gaps between
+    consecutive marks are summed by (from, to) tag pair. The trace costs a few
+    percent of the solve; the totals are for reading the phase structure, not
+    a bench value."""
+    import collections
+
+    import torch
+
+    import jax_fem_cfd_b200.setup.simulation as sim
+    from jax_fem_cfd_b200 import _lib
+    from jax_fem_cfd_b200.context import ptr
+    compute, timestep, nc, sn, h, nn, gd, Ud = sim.setup(tg_config(sim, size))
+    U0, P0 = tg_initial(nc.cpu().numpy())
+    U, P = torch.as_tensor(U0).cuda(), torch.as_tensor(P0).cuda()
+    Fp, F = compute(Ud, None, 0.0, 1e-3)
+    for _ in range(5):
+        U, P, ui, pi = timestep(U, P, 1e-3, 1.0, 0.01, Ud, Fp, F)
+    torch.cuda.synchronize()
+    ctx = timestep.solver.ctx
+    cap = 1 << 16
+    buf = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    _lib.call("fem_ctx_set_trace", ctx.handle, ptr(buf), cap)
+    U, P, ui, pi = timestep(U, P, 1e-3, 1.0, 0.01, Ud, Fp, F)
+    torch.cuda.synchronize()
+    _lib.call("fem_ctx_set_trace", ctx.handle, None, 0)
+    b = buf.cpu().numpy().astype(np.uint64)
+    v = b[1:int(b[0]) + 1]
+    tag = (v >> np.uint64(56)).astype(int)
+    t = (v & np.uint64((1 << 56) - 1)).astype(np.int64)
+    pairs = collections.defaultdict(list)
+    for k in range(len(t) - 1):
+        pairs[(int(tag[k]), int(tag[k + 1]))].append((t[k + 1] - t[k]) / 1e3)
+    rows = sorted(pairs.items(), key=lambda kv: -sum(kv[1]))
+    return {"workload": f"Taylor-Green {size}x{size} Q2, one step's BiCGSTAB and MG-PCG launches",
+            "iterations": {"momentum": int(ui), "pressure": int(pi)}, "marks": int(len(t)),
+            "span_us": float((t[-1] - t[0]) / 1e3),
+            "pairs": [{"from": a, "to": b_, "count": len(x), "mean_us": float(np.mean(x)), "total_us": float(np.sum(x))}
+                      for (a, b_), x in rows]}
+
+
 def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid", "multigrid_mixed"), nx=256):
     """3D channel: hex8 256 x 64 x 64 on [0,4] x [0,1] x [0,1] (1,048,576
     elements, 1,090,625 nodes), parabolic inflow u = 16 y(1-y) z(1-z) on x = 0,
@@ -862,7 +906,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--only", choices=["matvec", "poisson", "poisson_sweep", "serving", "inverse", "channel3d",
-                                       "cavity", "tg_mixed", "mg3_vcycle"],
+                                       "cavity", "tg_mixed", "mg3_vcycle", "cg_trace"],
                     help="run one secondary measurement alone and print it (poisson: the --size mesh)")
     ap.add_argument("--requests", type=int, default=1024, help="--only serving: requests in the stream")
     ap.add_argument("--channel-nx", type=int, default=256, help="--only channel3d: elements along x (y, z: nx / 4)")
@@ -877,7 +921,7 @@ def main():
               "channel3d": lambda: channel3d(args.steps, preconds=tuple(args.preconds.split(",")),
                                              nx=args.channel_nx), "cavity": cavity,
               "tg_mixed": lambda: tg_mixed_long(500, args.size),
-              "mg3_vcycle": lambda: mg3_vcycle(args.channel_nx)}[args.only]
+              "mg3_vcycle": lambda: mg3_vcycle(args.channel_nx), "cg_trace": lambda: cg_trace(args.size)}[args.only]
         print(json.dumps(fn()))
         return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
