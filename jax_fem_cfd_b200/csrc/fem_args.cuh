@@ -179,7 +179,7 @@ int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq,
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s);
 int fem_launch_bicgstab(int ncomp, const BiArgs& A, int grid, cudaStream_t s);
 // packed step (k_pack.cu): k members of `ctas` CTAs each, one cooperative launch
-int fem_launch_step_pack(int kind, const PackMember* members, const PackParams& P, int k, int ctas,
+int fem_launch_step_pack(int kind, const PackMember* members, const PackParams& P, int k, int ctas, int blk,
                          cudaStream_t s);
 int fem_pack_occupancy(int* per_sm);
 

@@ -1492,6 +1492,7 @@ extern "C" int fem_ctx_set_max_ctas(fem_ctx* c, int ctas, int* capacity) {
 
 struct fem_pack {
   int k = 0, ctas = 0, capacity = 0;
+  int blk = 0;                   // the members' multigrid runs its coarsest levels inside CTA 0
   PackMember* dmem = nullptr;    // k members (device)
   unsigned int* sync = nullptr;  // [2m] grid and [2m + 1] team arrival counts, [2k + m] error word
 };
@@ -1599,6 +1600,7 @@ extern "C" int fem_pack_create(fem_ctx* const* ctxs, int k, double* const* U0, d
     C.status = st + 3;
     C.final_rr = nullptr;
     C.team = team_size(ctas);
+    if (C.block_smem_from < C.nlev) p->blk = 1;
     M.U[0] = U0[m];
     M.U[1] = U1[m];
     M.P[0] = P0[m];
@@ -1647,7 +1649,7 @@ extern "C" int fem_pack_step(fem_pack* p, const double* dt, const double* mu, co
     return FEM_E_STATE;
   }
   FEM_CHECK(cudaMemsetAsync(p->sync, 0, sizeof(unsigned int) * 3 * p->k, s));
-  return fem_launch_step_pack(FEM_Q1_2D, p->dmem, P, active, p->ctas, s);
+  return fem_launch_step_pack(FEM_Q1_2D, p->dmem, P, active, p->ctas, p->blk, s);
 }
 
 extern "C" int fem_pack_info(const fem_pack* p, int* k, int* ctas, int* capacity) {

@@ -86,17 +86,21 @@ static const void* vc_fn_p(int kind) {
 }
 static const void* cg_fn(int kind, int pinned) { return pinned ? cg_fn_p<true>(kind) : cg_fn_p<false>(kind); }
 static const void* vc_fn(int kind, int pinned) { return pinned ? vc_fn_p<true>(kind) : vc_fn_p<false>(kind); }
+// dynamic smem of a launch: the region of the CTA-0 levels' 1/D only when they run
+// (shared memory taken from the L1 carveout otherwise costs cache for nothing)
+static size_t cg_dyn_smem(const CgArgs& A) {
+  return (size_t)(128 + FEM_TILE_SMEM + FEM_TAB_SMEM + (A.block_smem_from < A.nlev ? FEM_BLK_SMEM : 0)) *
+         sizeof(double);
+}
 int fem_launch_cg(const CgArgs& A, int grid, double* cr, double* cp, double* cq, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq};
-  return coop_launch(cg_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_cg",
-                     (size_t)FEM_DYN_SMEM_MAX);
+  return coop_launch(cg_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_cg", cg_dyn_smem(A));
 }
 int fem_launch_vcycle(const CgArgs& A, int grid, double* cr, double* cp, double* cq, double* z, cudaStream_t s) {
   CgArgs a = A;
   void* args[] = {&a, &cr, &cp, &cq, &z};
-  return coop_launch(vc_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_vcycle",
-                     (size_t)FEM_DYN_SMEM_MAX);
+  return coop_launch(vc_fn(A.lv[0].g.kind, A.pinned), grid, args, s, "k_vcycle", cg_dyn_smem(A));
 }
 int fem_coop_occupancy_cg(int* occ) {
   int m = 1 << 30;

@@ -103,12 +103,13 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_step_pack(const PackMember* 
   }
 }
 
-int fem_launch_step_pack(int kind, const PackMember* members, const PackParams& P, int k, int ctas,
+int fem_launch_step_pack(int kind, const PackMember* members, const PackParams& P, int k, int ctas, int blk,
                          cudaStream_t s) {
   if (kind != FEM_Q1_2D || k < 1 || k > FEM_PACK_MAX || ctas < 1) return FEM_E_ARG;
   const void* fn = (const void*)k_step_pack<FEM_Q1_2D>;
-  const int dyn = FEM_PACK_SMEM * (int)sizeof(double);
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  // the region of the CTA-0 multigrid levels' 1/D only when they run
+  const int dyn = (FEM_PACK_SMEM - (blk ? 0 : FEM_BLK_SMEM)) * (int)sizeof(double);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FEM_PACK_SMEM * (int)sizeof(double));
   const PackMember* m = members;
   PackParams p = P;
   void* args[] = {&m, &p};
