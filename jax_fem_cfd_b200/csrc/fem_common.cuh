@@ -309,6 +309,11 @@ struct FemPartials {
   }
 };
 
+// A party whose wait times out also sets FEM_BAR_ABORT in the arrival counter:
+// every other poller then sees a count at or above its target with that bit
+// set and leaves at this barrier, with no separate load of the error word after
+// each completed wait (counts stay far below the bit: k * parties).
+#define FEM_BAR_ABORT 0x40000000u
 template <class Parts = FemNoPartials>
 __device__ __forceinline__ bool fem_counter_barrier(const FemSync* s, unsigned int* cnt, unsigned int* round,
                                                     int parties, unsigned long long tag, const Parts& parts = Parts(),
@@ -325,20 +330,20 @@ __device__ __forceinline__ bool fem_counter_barrier(const FemSync* s, unsigned i
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(cnt), "r"(1u) : "memory");
     if (parties > 1) {
       const unsigned long long t0 = fem_globaltimer();
-      unsigned int polls = 0;
-      while (fem_ld_acquire(cnt) < target) {
+      unsigned int polls = 0, c;
+      while ((c = fem_ld_acquire(cnt)) < target) {
         if (((++polls) & 63u) == 0u) {
+          // a timeout raised by another party on another counter
           if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) { ok = 0; break; }
           if (fem_globaltimer() - t0 > FEM_BARRIER_TIMEOUT_NS) {
             atomicOr(err, FEM_ERR_BARRIER_TIMEOUT);
+            atomicOr(cnt, FEM_BAR_ABORT);
             ok = 0;
             break;
           }
         }
       }
-      // a timeout raised by another party; a team of one CTA has none, and
-      // skips this global-memory round trip
-      if (*(volatile int*)err & FEM_ERR_BARRIER_TIMEOUT) ok = 0;
+      if (c & FEM_BAR_ABORT) ok = 0;
     }
     s_ok = ok;
     if (s->trace && blockIdx.x == 0) fem_trace_put(s->trace, s->trace_cap, tag);
