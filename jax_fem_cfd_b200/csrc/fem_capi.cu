@@ -144,7 +144,7 @@ struct fem_ctx {
   FemQuadTab qt{};         // Gauss table of the mesh (2D), for on-the-fly convection
   int conv_otf = 0;        // fem_step4 applies Ce without building it
   size_t Fe_cap = 0;       // face entries the boundary-flux scratch holds
-  int *bs_cnt = nullptr, *bs_off = nullptr, *bs_list = nullptr;  // boundary scatter CSR (nn, nn + 1, Fe_cap)
+  int *bs_cnt = nullptr, *bs_off = nullptr, *bs_list = nullptr;  // boundary scatter CSR (nn, nn + 1 + scan chunks, Fe_cap)
   int* flags = nullptr;  // device ints: [FEM_FLAG_BOUNDARY_SKIPPED] faces skipped by the last flux call,
                          // [1], [2] cycles and status of the last hex8 mixed solve
   // optional stage timing
@@ -1206,7 +1206,8 @@ extern "C" int fem_boundary_flux(fem_ctx* c, const int32_t* bconn, const double*
   }
   if (!c->bs_cnt) {
     FEM_ALLOC(c->bs_cnt, (size_t)c->g.nn);
-    FEM_ALLOC(c->bs_off, (size_t)c->g.nn + 1);
+    // offsets, then the chunk sums of their scan (k_ops.cu, FEM_SCAN_CHUNK = 4096 nodes per chunk)
+    FEM_ALLOC(c->bs_off, (size_t)c->g.nn + 1 + (c->g.nn + 4095) / 4096);
   }
   return fem_launch_boundary_csr(c->coords, c->ndim, bconn, nvec, nb, npf, U, c->g.nn, c->Fe, c->bs_cnt, c->bs_off,
                                  c->bs_list, c->flags + FEM_FLAG_BOUNDARY_SKIPPED, Fp, s);

@@ -202,6 +202,64 @@ __device__ __forceinline__ void fem_convection_block(const FemGrid& g, const Fem
   __syncthreads();
 }
 
+// The same build with the element's table sizes known at compile time (loops
+// unrolled, every sum in the order above) and the quadrature tables (w, N, dN)
+// in shared memory: EPB elements per round of three stages.
+template <int NQ, int NEN, int ND, int EPB>
+struct FemCeBlockSmem {
+  double uq[EPB * NQ * 3], div[EPB * NQ], T[EPB * NQ * NEN];
+  double w[NQ], N[NQ * NEN], dN[NQ * ND * NEN];
+};
+template <int NQ, int NEN, int ND, int EPB>
+__device__ __forceinline__ void fem_convection_block_k(const FemGrid& g, const double* __restrict__ U, double beta,
+                                                       double* __restrict__ Ce, int e0, int mode,
+                                                       FemCeBlockSmem<NQ, NEN, ND, EPB>& S) {
+  const int nloc = min(EPB, g.ne - e0);
+  for (int t = threadIdx.x; t < nloc * NQ; t += blockDim.x) {
+    const int le = t / NQ, q = t - le * NQ, e = e0 + le;
+    const int ie = e % g.nex, r = e / g.nex, je = r % g.ney, ke = r / g.ney;
+    double u[3] = {0, 0, 0}, dv = 0.0;
+#pragma unroll
+    for (int I = 0; I < NEN; ++I) {
+      const int j = fem_elem_node(g, ie, je, ke, I);
+      const double NI = S.N[q * NEN + I];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        const double uj = U[j + (size_t)d * g.nn];
+        u[d] += NI * uj;
+        dv += S.dN[(q * ND + d) * NEN + I] * uj;
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) S.uq[(le * NQ + q) * 3 + d] = u[d];
+    S.div[le * NQ + q] = dv;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nloc * NQ * NEN; t += blockDim.x) {
+    const int le = t / (NQ * NEN), rem = t - le * (NQ * NEN), q = rem / NEN, b = rem - q * NEN;
+    double v = 0.0;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) v += S.uq[(le * NQ + q) * 3 + d] * S.dN[(q * ND + d) * NEN + b];
+    if (mode == 0) v += beta * S.div[le * NQ + q] * S.N[q * NEN + b];
+    S.T[(le * NQ + q) * NEN + b] = v;
+  }
+  __syncthreads();
+  constexpr int per = NEN * NEN;
+  for (int t = threadIdx.x; t < nloc * per; t += blockDim.x) {
+    const int le = t / per, ab = t - le * per, a = ab / NEN, b = ab - a * NEN;
+    double v = 0.0;
+    if (mode == 0) {
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) v += (S.N[q * NEN + a] * S.w[q]) * S.T[(le * NQ + q) * NEN + b];
+    } else {
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) v += S.w[q] * S.T[(le * NQ + q) * NEN + a] * S.T[(le * NQ + q) * NEN + b];
+    }
+    Ce[(size_t)e0 * per + t] = v;
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // Multigrid lattice transfers (core/multigrid.py:90-212). Arrays are indexed
 // [row = y][col = x]; "full" extents include the periodic duplicate row/column.

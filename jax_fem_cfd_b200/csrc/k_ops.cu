@@ -53,6 +53,21 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_convection(FemGrid g, FemQua
     fem_convection_block(g, Q, U, beta, Ce, e0, mode, s_uq, s_div, s_T);
 }
 
+// The same build for one element kind (fem_convection_block_k): 32 elements
+// per round, quadrature tables staged in shared memory once per CTA.
+#define FEM_CE_EPB_K 32
+template <int NQ, int NEN, int ND>
+__global__ void __launch_bounds__(FEM_OP_THREADS) k_convection_k(FemGrid g, FemQuad Q, const double* __restrict__ U,
+                                                                 double beta, int mode, double* __restrict__ Ce) {
+  __shared__ FemCeBlockSmem<NQ, NEN, ND, FEM_CE_EPB_K> S;
+  for (int t = threadIdx.x; t < NQ; t += blockDim.x) S.w[t] = Q.wq[t];
+  for (int t = threadIdx.x; t < NQ * NEN; t += blockDim.x) S.N[t] = Q.N[t];
+  for (int t = threadIdx.x; t < NQ * ND * NEN; t += blockDim.x) S.dN[t] = Q.dN[t];
+  __syncthreads();
+  for (int e0 = blockIdx.x * FEM_CE_EPB_K; e0 < g.ne; e0 += gridDim.x * FEM_CE_EPB_K)
+    fem_convection_block_k<NQ, NEN, ND, FEM_CE_EPB_K>(g, U, beta, Ce, e0, mode, S);
+}
+
 // core/element_calc.py:202-229 (per-element tau, r-norm blend).
 __global__ void k_supg_tau(FemGrid g, FemQuad Q, const double* __restrict__ U, const double* __restrict__ Ce,
                            const double* __restrict__ Ct, double D, double dt, double r, double* __restrict__ tau) {
@@ -228,6 +243,103 @@ __global__ void k_bs_scan(const int* __restrict__ cnt, int nn, int* __restrict__
     run += cnt[i];
   }
   if (tid == T - 1) off[nn] = part[T - 1];
+}
+// The same prefix sum over many CTAs, in three passes of FEM_SCAN_CHUNK elements
+// per CTA: chunk sums, their exclusive scan in one CTA, then each chunk scanned
+// from its offset. Integer sums, so off is the single-CTA result exactly.
+#define FEM_SCAN_CHUNK 4096  // 256 threads x 16 consecutive elements
+__device__ __forceinline__ int fem_block_sum_int(int v, int* ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) ws[warp] = v;
+  __syncthreads();
+  int t = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+  return t;
+}
+__global__ void k_scan_chunk_sums(const int* __restrict__ cnt, int n, int* __restrict__ bsum) {
+  __shared__ int ws[32];
+  const int base = blockIdx.x * FEM_SCAN_CHUNK, end = min(n, base + FEM_SCAN_CHUNK);
+  int v = 0;
+  for (int i = base + threadIdx.x; i < end; i += blockDim.x) v += cnt[i];
+  v = fem_block_sum_int(v, ws);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = v;
+}
+// exclusive scan of bsum[0, nb) in place by one CTA; *total = the sum of all
+__global__ void k_scan_chunk_offsets(int* __restrict__ bsum, int nb, int* __restrict__ total) {
+  __shared__ int ws[32];
+  __shared__ int carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < nb; b0 += blockDim.x) {
+    const int i = b0 + threadIdx.x;
+    const int v = i < nb ? bsum[i] : 0;
+    int x = v;  // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[warp] = x;
+    __syncthreads();
+    int before = carry;
+    for (int w = 0; w < warp; ++w) before += ws[w];
+    if (i < nb) bsum[i] = before + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < nw; ++w) t += ws[w];
+      carry += t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+// off[i] for the chunk of this CTA: thread t scans its 16 consecutive elements
+__global__ void k_scan_chunk_apply(const int* __restrict__ cnt, int n, const int* __restrict__ bsum,
+                                   int* __restrict__ off) {
+  __shared__ int ws[32];
+  constexpr int V = FEM_SCAN_CHUNK / 256;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i0 = blockIdx.x * FEM_SCAN_CHUNK + threadIdx.x * V;
+  int v[V], s = 0;
+#pragma unroll
+  for (int k = 0; k < V; ++k) {
+    v[k] = (i0 + k < n) ? cnt[i0 + k] : 0;
+    s += v[k];
+  }
+  int x = s;  // inclusive warp scan of the thread sums
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  int run = bsum[blockIdx.x] + x - s;
+  for (int w = 0; w < warp; ++w) run += ws[w];
+#pragma unroll
+  for (int k = 0; k < V; ++k) {
+    if (i0 + k < n) off[i0 + k] = run;
+    run += v[k];
+  }
+}
+// off[0, n] (n + 1 entries) from cnt[0, n): bsum holds fem_scan_chunks(n) ints
+static inline int fem_scan_chunks(int n) { return (n + FEM_SCAN_CHUNK - 1) / FEM_SCAN_CHUNK; }
+static int fem_launch_scan(const int* cnt, int n, int* off, int* bsum, cudaStream_t s) {
+  if (n <= 0) {
+    if (cudaMemsetAsync(off, 0, sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");
+    return FEM_OK;
+  }
+  const int nb = fem_scan_chunks(n);
+  k_scan_chunk_sums<<<nb, 256, 0, s>>>(cnt, n, bsum);
+  if (int rc = fem_after_launch("k_scan_chunk_sums")) return rc;
+  k_scan_chunk_offsets<<<1, 1024, 0, s>>>(bsum, nb, off + n);
+  if (int rc = fem_after_launch("k_scan_chunk_offsets")) return rc;
+  k_scan_chunk_apply<<<nb, 256, 0, s>>>(cnt, n, bsum, off);
+  return fem_after_launch("k_scan_chunk_apply");
 }
 __global__ void k_bs_fill(const int32_t* __restrict__ bconn, int m, int nn, const int* __restrict__ off,
                           int* __restrict__ cur, int* __restrict__ list) {
@@ -538,6 +650,19 @@ int fem_launch_div(int ndim, const FemGrid& g, const double* Ge, const double* U
 }
 int fem_launch_convection(const FemGrid& g, const FemQuad& Q, const double* U, double beta, int mode, double* out,
                           cudaStream_t s) {
+  const int nbk = fem_nblocks((g.ne + FEM_CE_EPB_K - 1) / FEM_CE_EPB_K, 1, 148 * 16);
+  if (Q.nq == 8 && Q.nen == 8 && Q.ndim == 3) {
+    k_convection_k<8, 8, 3><<<nbk, FEM_OP_THREADS, 0, s>>>(g, Q, U, beta, mode, out);
+    return fem_after_launch("k_convection_k");
+  }
+  if (Q.nq == 9 && Q.nen == 9 && Q.ndim == 2) {
+    k_convection_k<9, 9, 2><<<nbk, FEM_OP_THREADS, 0, s>>>(g, Q, U, beta, mode, out);
+    return fem_after_launch("k_convection_k");
+  }
+  if (Q.nq == 4 && Q.nen == 4 && Q.ndim == 2) {
+    k_convection_k<4, 4, 2><<<nbk, FEM_OP_THREADS, 0, s>>>(g, Q, U, beta, mode, out);
+    return fem_after_launch("k_convection_k");
+  }
   const int nb = fem_nblocks((g.ne + FEM_CE_EPB - 1) / FEM_CE_EPB, 1, 148 * 32);
   k_convection<<<nb, FEM_OP_THREADS, 0, s>>>(g, Q, U, beta, mode, out);
   return fem_after_launch("k_convection");
@@ -606,8 +731,8 @@ int fem_launch_boundary_csr(const double* coords, int dim, const int32_t* bconn,
     k_bs_count<<<fem_nblocks(m, 256), 256, 0, s>>>(bconn, m, nn, cnt);
     if (int rc = fem_after_launch("k_bs_count")) return rc;
   }
-  k_bs_scan<<<1, 1024, 0, s>>>(cnt, nn, off);
-  if (int rc = fem_after_launch("k_bs_scan")) return rc;
+  // off holds nn + 1 offsets, then fem_scan_chunks(nn) chunk sums of the scan
+  if (int rc = fem_launch_scan(cnt, nn, off, off + nn + 1, s)) return rc;
   if (cudaMemsetAsync(cnt, 0, (size_t)nn * sizeof(int), s) != cudaSuccess) return fem_after_launch("memset");
   if (m > 0) {
     k_bs_fill<<<fem_nblocks(m, 256), 256, 0, s>>>(bconn, m, nn, off, cnt, list);
