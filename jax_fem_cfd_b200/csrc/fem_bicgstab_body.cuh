@@ -27,6 +27,11 @@ __device__ __forceinline__ void bi_tiled_apply(const Team& tm, const BiArgs& A, 
     fem_tiled_conv3<NC, NSRC>(tm, A.g, tsm, tma, src, comb, A.cvf, A.qt, A.cv_coef, op.alpha, op.A, body);
   } else if constexpr (OTF) {
     fem_tiled_conv<KIND, NC, NSRC>(tm, A.g, tsm, src, comb, A.cvf, A.qt, A.cv_coef, op.alpha, op.A, body);
+  } else if constexpr (KIND == FEM_HEX8) {
+    // explicit per-element matrices: element-centric (fem_tiled_ebe3e); other
+    // combinations (transposed B, a third matrix) node-centric
+    if (op.B && !op.transB && !op.C) fem_tiled_ebe3e<NC>(tm, A.g, tsm, load, op, body);
+    else fem_tiled_ebe<KIND, NC>(tm, A.g, tsm, load, op, body);
   } else {
     fem_tiled_ebe<KIND, NC>(tm, A.g, tsm, load, op, body);
   }

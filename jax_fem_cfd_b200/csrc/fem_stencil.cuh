@@ -605,3 +605,174 @@ __device__ __forceinline__ void fem_tiled_ebe(const Team& tm, const FemGrid& g, 
     __syncthreads();
   }
 }
+
+// ---------------------------------------------------------------------------
+// Element-centric hex8 product with per-element matrices (the explicit Ce of
+// the momentum operator): y = sum_e P_e^T (alpha A + beta B_e) P_e x for NC
+// components, B_e row-major per element (transB == 0, no C).
+//
+// The CTA owns a tile of EX x EY elements (and the nodes at their low corners;
+// the last tile of each axis also owns the closing node line) and marches a
+// run of z. For each element layer L it forms every row of every element of
+// the tile plus a one-element halo in -x and -y: a warp takes four elements at
+// a time, lane l forms row l % 8 of element l / 8 from its 64-byte row of B_e
+// (four 16-byte loads; the warp reads the four elements' 2 KB whole) and the
+// staged node values, summing over the element's nodes in order, as the
+// node-centric fem_tiled_ebe does. Rows 0-3 (bottom nodes) serve node plane L, rows 4-7 (top
+// nodes) are kept for plane L + 1. Each node then sums its incident elements'
+// rows in the order of fem_incident_k (layer below, then above; y - 1 before
+// y; x - 1 before x), so results are deterministic. The next node plane's
+// values are loaded into registers while a layer computes.
+//
+// Shared memory (doubles): fem_ebe3e_smem(NC). load(j, c): the source value at
+// node j; body(n, y[NC], x_n[NC]) as in fem_tiled_ebe.
+#define FEM_E3_EX 32
+#define FEM_E3_EY 8
+#define FEM_E3_FX (FEM_E3_EX + 1)         // element footprint (halo in -x, -y)
+#define FEM_E3_FY (FEM_E3_EY + 1)
+#define FEM_E3_PX (FEM_E3_EX + 2)         // staged node plane (34 x 10)
+#define FEM_E3_PY (FEM_E3_EY + 2)
+#define FEM_E3_NE (FEM_E3_FX * FEM_E3_FY)  // 297 elements per layer
+__host__ __device__ constexpr int fem_ebe3e_smem(int nc) {
+  return 3 * nc * FEM_E3_PX * FEM_E3_PY + 3 * nc * 4 * FEM_E3_NE;
+}
+template <int NC, class Team, class Load, class Body>
+__device__ __forceinline__ void fem_tiled_ebe3e(const Team& tm, const FemGrid& g, double* __restrict__ sm,
+                                                const Load& load, const MatCombo& op, const Body& body) {
+  constexpr int PX = FEM_E3_PX, PXY = FEM_E3_PX * FEM_E3_PY, FX = FEM_E3_FX, NE = FEM_E3_NE;
+  constexpr int RS = 4 * NE;                   // 4 rows per element, per component
+  double* __restrict__ stg = sm;               // node planes: [slot (z % 3)][c][PXY]
+  double* __restrict__ bot = sm + 3 * NC * PXY;  // rows 0-3 of the current layer: [c][fe * 4 + row]
+  double* __restrict__ top = bot + NC * RS;      // rows 4-7 of layers L & 1: [L & 1][c][fe * 4 + row - 4]
+  const int nex = g.nex, ney = g.ney, nez = g.nez, nnz = nez + 1;
+  const int tnx = (nex + FEM_E3_EX - 1) / FEM_E3_EX, tny = (ney + FEM_E3_EY - 1) / FEM_E3_EY, nt2 = tnx * tny;
+  int nzc = tm.ncta() / nt2;
+  if (nzc < 1) nzc = 1;
+  if (nzc > nnz) nzc = nnz;
+  const int zl = (nnz + nzc - 1) / nzc, nunit = nt2 * ((nnz + zl - 1) / zl);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  // lane l forms row a = l % 8 of the warp's element slot l / 8 (four elements per warp step)
+  const int a = lane & 7, slot = lane >> 3;
+  double sA[8];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) sA[b] = op.A ? op.alpha * op.A[a * 8 + b] : 0.0;
+  const double beta = op.beta;
+  const double* __restrict__ B = op.B;
+  for (int u = tm.cta(); u < nunit; u += tm.ncta()) {
+    const int zc = u / nt2, rr = u - zc * nt2, by = rr / tnx, bx = rr - by * tnx;
+    const int ex0 = bx * FEM_E3_EX, ey0 = by * FEM_E3_EY;
+    const int nx1 = (bx == tnx - 1) ? nex + 1 : ex0 + FEM_E3_EX, ny1 = (by == tny - 1) ? ney + 1 : ey0 + FEM_E3_EY;
+    const int z0 = zc * zl, z1 = min(nnz, z0 + zl);
+    const int Lb = max(z0 - 1, 0), Le = min(z1 - 1, nez - 1);
+    // node (x, y) of plane z at staged cell q of the 34 x 10 window (clamped into the lattice)
+    auto stage_cell = [&](int q, int z, double (&v)[NC]) {
+      const int py = q / PX, px = q - py * PX;
+      int gx = ex0 - 1 + px, gy = ey0 - 1 + py;
+      gx = gx < 0 ? 0 : (gx > nex ? nex : gx);
+      gy = gy < 0 ? 0 : (gy > ney ? ney : gy);
+      const int j = (z * g.nny + gy) * g.nnx + gx;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[c] = load(j, c);
+    };
+    // y of node plane z from the rows kept for it (below: layer z - 1, above: layer z)
+    auto finalize = [&](int z) {
+      const int wx = nx1 - ex0, cnt = wx * (ny1 - ey0);
+      const double* __restrict__ tb = top + ((z - 1) & 1) * NC * RS;
+      for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+        const int qy = q / wx, x = ex0 + (q - qy * wx), y = ey0 + qy;
+        double acc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+#pragma unroll
+        for (int zk = 0; zk < 2; ++zk) {
+          if (zk == 0 ? z < 1 : z >= nez) continue;
+          const double* __restrict__ buf = zk == 0 ? tb : bot;
+#pragma unroll
+          for (int zj = 0; zj < 2; ++zj) {
+            const int ey = zj ? y : y - 1;
+            if (ey < 0 || ey >= ney) continue;
+#pragma unroll
+            for (int zi = 0; zi < 2; ++zi) {
+              const int ex = zi ? x : x - 1;
+              if (ex < 0 || ex >= nex) continue;
+              // row of this node in element (ex, ey): quad4 index of (x - ex, y - ey)
+              const int r = fem_local_index(FEM_HEX8, 1 - zi, 1 - zj, 0);
+              const int fe = (ey - ey0 + 1) * FX + (ex - ex0 + 1);
+#pragma unroll
+              for (int c = 0; c < NC; ++c) acc[c] += buf[c * RS + fe * 4 + r];
+            }
+          }
+        }
+        double ctr[NC];
+        const int cq = (y - ey0 + 1) * PX + (x - ex0 + 1);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) ctr[c] = stg[((z % 3) * NC + c) * PXY + cq];
+        body((z * g.nny + y) * g.nnx + x, acc, ctr);
+      }
+    };
+    if (threadIdx.x < PXY) {
+#pragma unroll
+      for (int pl = 0; pl < 2; ++pl) {
+        double v[NC];
+        stage_cell(threadIdx.x, Lb + pl, v);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) stg[(((Lb + pl) % 3) * NC + c) * PXY + threadIdx.x] = v[c];
+      }
+    }
+    __syncthreads();
+    for (int L = Lb; L <= Le; ++L) {
+      const int s0 = L % 3, s1 = (L + 1) % 3;
+      // plane L + 2 into registers while the layer computes
+      double pv[NC];
+      const bool pf = L + 2 <= nez && threadIdx.x < PXY;
+      if (pf) stage_cell(threadIdx.x, L + 2, pv);
+      double* __restrict__ tw = top + (L & 1) * NC * RS;
+      const size_t lay = (size_t)L * ney;
+      // row a of element fe: sum_b (alpha A[a][b] + beta B_e[a][b]) x(node b), b in order
+      for (int f0 = warp; f0 < NE; f0 += 4 * nwarp) {
+        const int fe = f0 + slot * nwarp, ly = fe / FX, lx = fe - ly * FX;
+        const int ex = ex0 - 1 + lx, ey = ey0 - 1 + ly;
+        if (fe < NE && ex >= 0 && ex < nex && ey >= 0 && ey < ney) {
+          const double2* __restrict__ row = reinterpret_cast<const double2*>(B + ((lay + ey) * nex + ex) * 64 + a * 8);
+          double2 cb[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) cb[q] = __ldg(row + q);
+          double v[8];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            v[2 * q] = sA[2 * q];
+            v[2 * q] += beta * cb[q].x;
+            v[2 * q + 1] = sA[2 * q + 1];
+            v[2 * q + 1] += beta * cb[q].y;
+          }
+          const int w = ly * PX + lx;
+          const double* __restrict__ xl = stg + s0 * NC * PXY + w;  // node plane L at the element's low corner
+          const double* __restrict__ xh = stg + s1 * NC * PXY + w;  // node plane L + 1
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            double p = 0.0;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+              const double* __restrict__ xp = kdk<FEM_HEX8>(b) ? xh : xl;
+              p += v[b] * xp[c * PXY + kdj<FEM_HEX8>(b) * PX + kdi<FEM_HEX8>(b)];
+            }
+            if (a < 4) bot[c * RS + fe * 4 + a] = p;
+            else tw[c * RS + fe * 4 + a - 4] = p;
+          }
+        }
+      }
+      if (pf) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) stg[(((L + 2) % 3) * NC + c) * PXY + threadIdx.x] = pv[c];
+      }
+      __syncthreads();
+      if (L >= z0 && L < z1) finalize(L);
+      __syncthreads();
+    }
+    // the closing node plane z = nez has elements only below
+    if (z0 <= nez && nez < z1) {
+      finalize(nez);
+      __syncthreads();
+    }
+  }
+}

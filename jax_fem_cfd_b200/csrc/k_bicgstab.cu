@@ -38,10 +38,12 @@ static const void* bi_fn(int kind, int ncomp, bool otf) {
   return ncomp == 1 ? (const void*)k_bicgstab<FEM_HEX8, 1, false> : (const void*)k_bicgstab<FEM_HEX8, 3, false>;
 }
 // dynamic smem (doubles) of the tiled operator: the EBE gather of fem_tiled_ebe
-// needs NC (32+2R)(16+2R)(3 in 3D); the on-the-fly convection fem_conv_smem
+// needs NC (32+2R)(16+2R)(3 in 3D); hex8 per-element matrices the element-centric
+// fem_tiled_ebe3e (fem_ebe3e_smem); the on-the-fly convection fem_conv_smem
 static int bi_smem_doubles(int kind, int ncomp, bool otf) {
   if (otf && kind == FEM_HEX8) return FEM_C3_SMEM_MAX;
   if (otf) return FEM_CONV_SMEM;
+  if (kind == FEM_HEX8) return fem_ebe3e_smem(3) > 3 * 1836 ? fem_ebe3e_smem(3) : 3 * 1836;
   return 3 * 1836;
 }
 
