@@ -154,6 +154,9 @@ int fem_launch_conv_factors3(const FemGrid& g, const FemQuadTab& qt, const doubl
 int fem_launch_conv_apply3(const FemGrid& g, const FemQuadTab& qt, const double* fq, double cc, double alpha,
                            const double* Ash, const double* x, double* y, int grid, int* err, cudaStream_t s);
 
+// hex8, 3 components: y = (alpha A + beta B_e) x, element-centric (B per element, not transposed, no C)
+int fem_launch_ebe3e(const FemGrid& g, const MatCombo& m, const double* x, double* y, int grid, cudaStream_t s);
+
 int fem_launch_selftest_barrier(const FemSync& sync, int* status, cudaStream_t s);
 // mixed-precision pinned Poisson solve (k_mixed.cu); work: 6 sum(nn_l) + 3 nn_0
 // floats, dwork: grid + 8 doubles

@@ -1060,6 +1060,9 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   } else {
     FEM_TRY(fem_launch_convection(g, quad_of(c), Un, 0.5, 0, c->Ce, s));
   }
+  // hex8 with the explicit Ce: (mu Le + rho Ce) U_n of the rhs by the element-centric product
+  const bool vcv3 = !otf && g.kind == FEM_HEX8 && nd == 3;
+  if (vcv3) FEM_TRY(fem_launch_ebe3e(g, MatCombo{c->Le, mu, c->Ce, rho, 0, nullptr, 0.0}, Un, c->vcv, c->sms, s));
   stage_mark(c, s);
   // 2. momentum rhs, x0 and G P_n (solvers/standard.py:31-37)
   StepArgs S;
@@ -1074,7 +1077,7 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   S.Ge = c->Ge;
   S.M = c->M;
   S.Ce = otf ? nullptr : c->Ce;
-  S.vcv = otf ? c->vcv : nullptr;
+  S.vcv = (otf || vcv3) ? c->vcv : nullptr;
   S.dmask = c->has_dmask ? c->dmask : nullptr;
   S.pmask = c->pmask;
   S.pinned = c->set_zeroP;

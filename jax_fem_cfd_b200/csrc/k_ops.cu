@@ -1,4 +1,5 @@
 // Element-product, element-matrix, transfer, boundary and blas-1 kernels.
+#include <mutex>
 #include "fem_b200.h"
 #include "fem_step_body.cuh"
 
@@ -51,6 +52,39 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_convection(FemGrid g, FemQua
   __shared__ double s_T[FEM_CE_EPB * 9 * 9];
   for (int e0 = blockIdx.x * FEM_CE_EPB; e0 < g.ne; e0 += gridDim.x * FEM_CE_EPB)
     fem_convection_block(g, Q, U, beta, Ce, e0, mode, s_uq, s_div, s_T);
+}
+
+// y = (alpha A + beta B_e) x on hex8, 3 components, by the element-centric
+// tiles of fem_tiled_ebe3e (one run of z-planes per CTA; no grid barrier).
+struct FemCtaTeam {
+  __device__ __forceinline__ int cta() const { return blockIdx.x; }
+  __device__ __forceinline__ int ncta() const { return gridDim.x; }
+};
+__global__ void __launch_bounds__(FEM_THREADS, 1) k_ebe3e_apply(FemGrid g, MatCombo m, const double* __restrict__ x,
+                                                                double* __restrict__ y) {
+  extern __shared__ __align__(128) double sm[];
+  __shared__ double sA[64];
+  if (m.A) {
+    for (int t = threadIdx.x; t < 64; t += blockDim.x) sA[t] = m.A[t];
+    __syncthreads();
+    m.A = sA;
+  }
+  const size_t N = g.nn;
+  fem_tiled_ebe3e<3>(FemCtaTeam{}, g, sm, [&](int j, int c) { return x[j + c * N]; }, m,
+                     [&](int n, const double(&v)[3], const double(&)[3]) {
+#pragma unroll
+                       for (int c = 0; c < 3; ++c) y[n + c * N] = v[c];
+                     });
+}
+int fem_launch_ebe3e(const FemGrid& g, const MatCombo& m, const double* x, double* y, int grid, cudaStream_t s) {
+  if (g.kind != FEM_HEX8 || !m.B || m.transB || m.C || grid < 1) return FEM_E_ARG;
+  const int dyn = fem_ebe3e_smem(3) * (int)sizeof(double);
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [&] { attr = cudaFuncSetAttribute(k_ebe3e_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn); });
+  if (attr != cudaSuccess) return fem_after_launch("k_ebe3e_apply attribute");
+  k_ebe3e_apply<<<grid, FEM_THREADS, dyn, s>>>(g, m, x, y);
+  return fem_after_launch("k_ebe3e_apply");
 }
 
 // The same build for one element kind (fem_convection_block_k): 32 elements
