@@ -102,6 +102,95 @@ __global__ void __launch_bounds__(FEM_OP_THREADS) k_convection_k(FemGrid g, FemQ
     fem_convection_block_k<NQ, NEN, ND, FEM_CE_EPB_K>(g, U, beta, Ce, e0, mode, S);
 }
 
+// hex8 form of the same build (8 Gauss points, 8 nodes, 3 dimensions), two
+// stages per round of 32 elements: thread (element, q) interpolates u and div u
+// at Gauss point q and writes T[q][b] for its 8 nodes b; thread (element, block)
+// then forms a 2 x 4 block of Ce[a][b] = sum_q (N[q][a] w[q]) T[q][b], loading
+// each factor once per Gauss point for its 8 entries. Every sum has the terms and
+// order of fem_convection_block; the rows of T are padded (66 doubles per
+// element) so the block loads of different elements fall in different banks.
+#define FEM_CE8_EPB 32
+#define FEM_CE8_TS 66
+__global__ void __launch_bounds__(256) k_convection_hex8(FemGrid g, FemQuad Q, const double* __restrict__ U,
+                                                         double beta, int mode, double* __restrict__ Ce) {
+  __shared__ __align__(16) double T[FEM_CE8_EPB * FEM_CE8_TS];
+  __shared__ double sN[64], sNW[64], sdN[192];
+  for (int t = threadIdx.x; t < 64; t += blockDim.x) {
+    sN[t] = Q.N[t];
+    sNW[t] = Q.N[t] * Q.wq[t >> 3];
+  }
+  for (int t = threadIdx.x; t < 192; t += blockDim.x) sdN[t] = Q.dN[t];
+  __syncthreads();
+  const size_t nn = g.nn;
+  for (int e0 = blockIdx.x * FEM_CE8_EPB; e0 < g.ne; e0 += gridDim.x * FEM_CE8_EPB) {
+    const int nloc = min(FEM_CE8_EPB, g.ne - e0);
+    for (int t = threadIdx.x; t < nloc * 8; t += blockDim.x) {
+      const int le = t >> 3, q = t & 7, e = e0 + le;
+      const int ie = e % g.nex, r = e / g.nex, je = r % g.ney, ke = r / g.ney;
+      double u[3] = {0, 0, 0}, dv = 0.0;
+#pragma unroll
+      for (int I = 0; I < 8; ++I) {
+        const int j = fem_elem_node(g, ie, je, ke, I);
+        const double NI = sN[q * 8 + I];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double uj = U[j + (size_t)d * nn];
+          u[d] += NI * uj;
+          dv += sdN[(q * 3 + d) * 8 + I] * uj;
+        }
+      }
+      double* Tq = T + le * FEM_CE8_TS + q * 8;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        double v = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v += u[d] * sdN[(q * 3 + d) * 8 + b];
+        if (mode == 0) v += beta * dv * sN[q * 8 + b];
+        Tq[b] = v;
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nloc * 8; t += blockDim.x) {
+      const int le = t >> 3, blk = t & 7, a0 = 2 * (blk >> 1), b0 = 4 * (blk & 1);
+      const double* Te = T + le * FEM_CE8_TS + b0;
+      double v[2][4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[i][k] = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double2 t01 = *reinterpret_cast<const double2*>(Te + q * 8);
+        const double2 t23 = *reinterpret_cast<const double2*>(Te + q * 8 + 2);
+        const double tb[4] = {t01.x, t01.y, t23.x, t23.y};
+        if (mode == 0) {
+          const double f0 = sNW[q * 8 + a0], f1 = sNW[q * 8 + a0 + 1];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            v[0][k] += f0 * tb[k];
+            v[1][k] += f1 * tb[k];
+          }
+        } else {
+          // Ctau_tilde: w_q T[q][a] T[q][b]
+          const double wq = Q.wq[q];
+          const double ta0 = T[le * FEM_CE8_TS + q * 8 + a0], ta1 = T[le * FEM_CE8_TS + q * 8 + a0 + 1];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            v[0][k] += wq * ta0 * tb[k];
+            v[1][k] += wq * ta1 * tb[k];
+          }
+        }
+      }
+      double2* out = reinterpret_cast<double2*>(Ce + (size_t)(e0 + le) * 64 + a0 * 8 + b0);
+      out[0] = make_double2(v[0][0], v[0][1]);
+      out[1] = make_double2(v[0][2], v[0][3]);
+      out[4] = make_double2(v[1][0], v[1][1]);
+      out[5] = make_double2(v[1][2], v[1][3]);
+    }
+    __syncthreads();
+  }
+}
+
 // core/element_calc.py:202-229 (per-element tau, r-norm blend).
 __global__ void k_supg_tau(FemGrid g, FemQuad Q, const double* __restrict__ U, const double* __restrict__ Ce,
                            const double* __restrict__ Ct, double D, double dt, double r, double* __restrict__ tau) {
@@ -685,9 +774,10 @@ int fem_launch_div(int ndim, const FemGrid& g, const double* Ge, const double* U
 int fem_launch_convection(const FemGrid& g, const FemQuad& Q, const double* U, double beta, int mode, double* out,
                           cudaStream_t s) {
   const int nbk = fem_nblocks((g.ne + FEM_CE_EPB_K - 1) / FEM_CE_EPB_K, 1, 148 * 16);
-  if (Q.nq == 8 && Q.nen == 8 && Q.ndim == 3) {
-    k_convection_k<8, 8, 3><<<nbk, FEM_OP_THREADS, 0, s>>>(g, Q, U, beta, mode, out);
-    return fem_after_launch("k_convection_k");
+  if (Q.nq == 8 && Q.nen == 8 && Q.ndim == 3 && g.kind == FEM_HEX8) {
+    const int nb8 = fem_nblocks((g.ne + FEM_CE8_EPB - 1) / FEM_CE8_EPB, 1, 148 * 16);
+    k_convection_hex8<<<nb8, 256, 0, s>>>(g, Q, U, beta, mode, out);
+    return fem_after_launch("k_convection_hex8");
   }
   if (Q.nq == 9 && Q.nen == 9 && Q.ndim == 2) {
     k_convection_k<9, 9, 2><<<nbk, FEM_OP_THREADS, 0, s>>>(g, Q, U, beta, mode, out);
