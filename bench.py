@@ -235,6 +235,12 @@ def run_ours(args, rank, world, local_rank):
     return res
 
 
+def _mixed_inner():
+    """FP32 inner iterations per FP64 refinement cycle of StandardSolverConfig(precision="mixed")."""
+    from jax_fem_cfd_b200.solvers import standard
+    return standard.MIXED_INNER
+
+
 def tg_mixed(args, fp64_final, coords):
     """The same Taylor-Green workload in mixed precision
     (StandardSolverConfig(precision="mixed"): both solves are FP64 refinement
@@ -276,7 +282,7 @@ def tg_mixed(args, fp64_final, coords):
     return {"workload": "the same Taylor-Green workload, mixed-precision pressure and momentum solves",
             "steps_per_s": args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
             "pressure_cycles_mean": float(np.mean(cycles)),
-            "pressure_solve": "FP64 refinement to 1e-8, 4 FP32 Chebyshev-multigrid PCG iterations per cycle",
+            "pressure_solve": f"FP64 refinement to 1e-8, {_mixed_inner()} FP32 Chebyshev-multigrid PCG iterations per cycle",
             "momentum_solve": "FP64 refinement to 1e-8, 3 FP32 BiCGSTAB iterations per cycle (FP32 Gauss factors)",
             "steps_compared": nsteps,
             "rel_err_vs_fp64": {"U": rel(U, Uf), "P": rel(P, Pf)},
@@ -783,7 +789,7 @@ def channel3d(steps=100, warmup=3, preconds=("jacobi", "approx_inv", "multigrid"
                    "pressure_iters_first_last": [int(it[0, 1]), int(it[-1, 1])],
                    "u_max_after": float(U[:nn].max()), "finite": bool(torch.isfinite(U).all())}
         if pc.endswith("mixed"):
-            out[pc]["pressure_iters_are"] = "FP64 refinement cycles (4 FP32 multigrid-PCG iterations each)"
+            out[pc]["pressure_iters_are"] = f"FP64 refinement cycles ({_mixed_inner()} FP32 multigrid-PCG iterations each)"
         if ref is None:
             ref = (U.clone(), P.clone())
         else:
