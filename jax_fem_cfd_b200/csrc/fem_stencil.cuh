@@ -616,13 +616,14 @@ __device__ __forceinline__ void fem_tiled_ebe(const Team& tm, const FemGrid& g, 
 // run of z. For each element layer L it forms every row of every element of
 // the tile plus a one-element halo in -x and -y: a warp takes four elements at
 // a time, lane l forms row l % 8 of element l / 8 from its 64-byte row of B_e
-// (four 16-byte loads; the warp reads the four elements' 2 KB whole) and the
-// staged node values, summing over the element's nodes in order, as the
-// node-centric fem_tiled_ebe does. Rows 0-3 (bottom nodes) serve node plane L, rows 4-7 (top
-// nodes) are kept for plane L + 1. Each node then sums its incident elements'
-// rows in the order of fem_incident_k (layer below, then above; y - 1 before
-// y; x - 1 before x), so results are deterministic. The next node plane's
-// values are loaded into registers while a layer computes.
+// (four 16-byte loads; each element's 512 bytes are read whole by its 8 lanes)
+// and the staged node values, summing over the element's nodes in order, as
+// the node-centric fem_tiled_ebe does. Rows 0-3 (bottom nodes) serve node
+// plane L, rows 4-7 (top nodes) are kept for plane L + 1. Each node then sums
+// its incident elements' rows in the order of fem_incident_k (layer below,
+// then above; y - 1 before y; x - 1 before x), so results are deterministic.
+// The next node plane's values are loaded into registers while a layer
+// computes.
 //
 // Shared memory (doubles): fem_ebe3e_smem(NC). load(j, c): the source value at
 // node j; body(n, y[NC], x_n[NC]) as in fem_tiled_ebe.
