@@ -44,6 +44,10 @@ struct StepArgs {
   const uint8_t* dmask;             // ndim*nn
   const uint8_t* pmask;             // nn (pinned pressure)
   int pinned;
+  // hex8: assembled stencil tables (FEM_TAB_MAX doubles apart) of Me, Ge_x, Ge_y,
+  // Ge_z and their transposes, used by the step bodies instead of per-node
+  // element gathers; null: gathers
+  const double* tab3 = nullptr;
 };
 
 // One request of a packed step launch (k_pack.cu): the device pointers and

@@ -156,6 +156,7 @@ struct fem_ctx {
   float* mx32 = nullptr;              // FP32 vectors of the mixed-precision solve (first use)
   double* mx64 = nullptr;             // its partial sums and scalars
   MxGraphCache mxg;                   // its captured inner solve
+  double* step_tab = nullptr;         // hex8: stencil tables of Me, Ge_d, Ge_d^T (7 x FEM_TAB_MAX)
   Mg3* mg3 = nullptr;                 // hex8 multigrid hierarchy and its solve graphs
   Mg3* mg2 = nullptr;                 // 2D hierarchy of the graph-driven mixed-precision solve (first use)
   MixMom* mixmom = nullptr;           // the mixed-precision momentum solve of fem_step4 (2D, first use)
@@ -293,7 +294,8 @@ extern "C" void fem_ctx_destroy(fem_ctx* c) {
                   c->dmask, c->pmask, c->aipin, c->cr, c->cp, c->cq, c->bar, c->err, c->partials, c->pr,
                   c->pz, c->pp0, c->pp1, c->pAp, c->pb, c->br, c->brh, c->bp0, c->bp1, c->bq0, c->bq1, c->bt,
                   c->rhsU, c->Uhat, c->gPn, c->Ustar, c->rhsP, c->Ce, c->Ce2, c->Ct, c->Mt, c->Ek, c->tau,
-                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab, c->bs_cnt, c->bs_off, c->bs_list, c->vjp, c->vjp2};
+                  c->dotpart, c->Fe, c->flags, c->vcv, c->cvf, c->ebe_tab, c->bs_cnt, c->bs_off, c->bs_list, c->vjp, c->vjp2,
+                  c->step_tab};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int l = 0; l < FEM_MAX_LEVELS; ++l) {
@@ -465,6 +467,15 @@ static int ctx_create_impl(const fem_mesh_desc* m, int device, fem_ctx* c) {
   FEM_TRY(fem_launch_stencil_build(g, c->Le, 0, 0, L0.tab, s));
   FEM_TRY(fem_launch_stencil_build(g, c->Le, 0, 1, L0.tab_off, s));
   FEM_TRY(fem_launch_invdiag(g.nn, c->Ldiag, c->pmask, L0.invD, L0.winvD, s));
+  if (g.kind == FEM_HEX8) {
+    // assembled stencils of the step's shared matrices: Me, Ge_d, Ge_d^T (StepArgs::tab3)
+    FEM_ALLOC(c->step_tab, 7 * (size_t)FEM_TAB_MAX);
+    FEM_TRY(fem_launch_stencil_build(g, c->Me, 0, 0, c->step_tab, s));
+    for (int d = 0; d < 3; ++d) {
+      FEM_TRY(fem_launch_stencil_build(g, c->Ge + d * 64, 0, 0, c->step_tab + (1 + d) * FEM_TAB_MAX, s));
+      FEM_TRY(fem_launch_stencil_build(g, c->Ge + d * 64, 1, 0, c->step_tab + (4 + d) * FEM_TAB_MAX, s));
+    }
+  }
   c->nlev = 1;
   FEM_CHECK(cudaDeviceSynchronize());
   // Gauss table for the on-the-fly convection of fem_step4
@@ -1078,6 +1089,7 @@ extern "C" int fem_step4(fem_ctx* c, const double* Un, const double* Pn, double 
   S.M = c->M;
   S.Ce = otf ? nullptr : c->Ce;
   S.vcv = (otf || vcv3) ? c->vcv : nullptr;
+  S.tab3 = c->step_tab;
   S.dmask = c->has_dmask ? c->dmask : nullptr;
   S.pmask = c->pmask;
   S.pinned = c->set_zeroP;

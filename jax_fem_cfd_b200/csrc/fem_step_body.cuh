@@ -5,6 +5,40 @@
 #pragma once
 #include "fem_args.cuh"
 
+// hex8: y_t = sum over the 27 lattice offsets of T_t[class][offset] src(node +
+// offset) for NT assembled tables T_t on one source (neighbour values loaded
+// once); the tables are the assembled rows of shared element matrices
+// (fem_stencil_entry), zero where an offset leaves the lattice.
+template <int NT, class Src>
+__device__ __forceinline__ void step_stencil3(const FemGrid& g, const double* const (&tab)[NT], int i, int j, int k,
+                                              const Src& src, double (&y)[NT]) {
+  const int cx = fem_axis_cls(FEM_HEX8, 0, i, g.nex), cy = fem_axis_cls(FEM_HEX8, 0, j, g.ney);
+  const int cz = fem_axis_cls(FEM_HEX8, 0, k, g.nez);
+  const int base = ((cz * 3 + cy) * 3 + cx) * 27;
+  int col[3], row[3], pl[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int v = i + d - 1, w = j + d - 1, z = k + d - 1;
+    col[d] = v < 0 ? 0 : (v >= g.nnx ? g.nnx - 1 : v);
+    row[d] = (w < 0 ? 0 : (w >= g.nny ? g.nny - 1 : w)) * g.nnx;
+    pl[d] = (z < 0 ? 0 : (z >= g.nnz ? g.nnz - 1 : z)) * g.nnx * g.nny;
+  }
+#pragma unroll
+  for (int t = 0; t < NT; ++t) y[t] = 0.0;
+#pragma unroll
+  for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < 3; ++dx) {
+        const int o = (dz * 3 + dy) * 3 + dx;
+        const double v = src(pl[dz] + row[dy] + col[dx]);
+#pragma unroll
+        for (int t = 0; t < NT; ++t) y[t] += __ldg(tab[t] + base + o) * v;
+      }
+}
+#define STEP_TAB(S, t) ((S).tab3 + (size_t)(t) * FEM_TAB_MAX)  // 0: Me, 1-3: Ge_d, 4-6: Ge_d^T
+
 // rhs of solvers/standard.py:31-37 and the initial guess x0; also keeps G P_n.
 template <int KIND>
 __device__ __forceinline__ void step_mom_rhs(const StepArgs& S, const double* __restrict__ Un,
@@ -22,14 +56,32 @@ __device__ __forceinline__ void step_mom_rhs(const StepArgs& S, const double* __
     int ix, iy, iz;
     fem_ij(g, n, ix, iy, iz);
     double ms[ND], v[ND], gp[ND];
-    fem_gather_k<KIND, ND>(g, ix, iy, iz, ms_m, src, ms);
+    bool tabs = false;
+    if constexpr (KIND == FEM_HEX8) {
+      if (S.tab3) {
+        const double* tm[1] = {STEP_TAB(S, 0)};
+#pragma unroll
+        for (int c = 0; c < ND; ++c) {
+          double y1[1];
+          step_stencil3<1>(g, tm, ix, iy, iz, [&](int j) { return Un[j + c * N]; }, y1);
+          ms[c] = y1[0];
+        }
+        const double* tg[3] = {STEP_TAB(S, 1), STEP_TAB(S, 2), STEP_TAB(S, 3)};
+        double g3[3];
+        step_stencil3<3>(g, tg, ix, iy, iz, [&](int j) { return Pn[j]; }, g3);
+#pragma unroll
+        for (int c = 0; c < ND; ++c) gp[c] = g3[c];
+        tabs = true;
+      }
+    }
+    if (!tabs) fem_gather_k<KIND, ND>(g, ix, iy, iz, ms_m, src, ms);
     if (S.vcv) {
 #pragma unroll
       for (int c = 0; c < ND; ++c) v[c] = S.vcv[n + c * N];
     } else {
       fem_gather_k<KIND, ND>(g, ix, iy, iz, vc, src, v);
     }
-    fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return Pn[j]; }, gp);
+    if (!tabs) fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return Pn[j]; }, gp);
 #pragma unroll
     for (int c = 0; c < ND; ++c) {
       const size_t o = n + c * N;
@@ -61,7 +113,25 @@ __device__ __forceinline__ void step_p_rhs(const StepArgs& S, const double* __re
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.nn; n += gridDim.x * blockDim.x) {
     int ix, iy, iz;
     fem_ij(g, n, ix, iy, iz);
-    const double du = fem_gather_div_k<KIND, ND>(g, ix, iy, iz, S.Ge, Us);
+    double du;
+    bool tabs = false;
+    if constexpr (KIND == FEM_HEX8) {
+      if (S.tab3) {
+        // per-component divergence parts, added in component order as the gather does
+        const size_t N = g.nn;
+        double acc[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double* td[1] = {STEP_TAB(S, 4 + d)};
+          double y1[1];
+          step_stencil3<1>(g, td, ix, iy, iz, [&](int j) { return Us[j + d * N]; }, y1);
+          acc[d] = y1[0];
+        }
+        du = acc[0] + acc[1] + acc[2];
+        tabs = true;
+      }
+    }
+    if (!tabs) du = fem_gather_div_k<KIND, ND>(g, ix, iy, iz, S.Ge, Us);
     double r = (S.rho / S.dt) * (Fp ? du - Fp[n] : du);
     double x = Pn[n];
     if (S.pinned && S.pmask && S.pmask[n]) {
@@ -86,7 +156,18 @@ __device__ __forceinline__ void step_ufinal(const StepArgs& S, const double* __r
     int ix, iy, iz;
     fem_ij(g, n, ix, iy, iz);
     double gp[ND];
-    fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return P[j]; }, gp);
+    bool tabs = false;
+    if constexpr (KIND == FEM_HEX8) {
+      if (S.tab3) {
+        const double* tg[3] = {STEP_TAB(S, 1), STEP_TAB(S, 2), STEP_TAB(S, 3)};
+        double g3[3];
+        step_stencil3<3>(g, tg, ix, iy, iz, [&](int j) { return P[j]; }, g3);
+#pragma unroll
+        for (int d = 0; d < ND; ++d) gp[d] = g3[d];
+        tabs = true;
+      }
+    }
+    if (!tabs) fem_gather_grad_k<KIND, ND>(g, ix, iy, iz, S.Ge, [&](int j) { return P[j]; }, gp);
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       const size_t o = n + d * N;
