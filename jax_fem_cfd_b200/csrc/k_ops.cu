@@ -79,10 +79,20 @@ __global__ void __launch_bounds__(FEM_THREADS, 1) k_ebe3e_apply(FemGrid g, MatCo
 int fem_launch_ebe3e(const FemGrid& g, const MatCombo& m, const double* x, double* y, int grid, cudaStream_t s) {
   if (g.kind != FEM_HEX8 || !m.B || m.transB || m.C || grid < 1) return FEM_E_ARG;
   const int dyn = fem_ebe3e_smem(3) * (int)sizeof(double);
-  static std::once_flag once;
-  static cudaError_t attr = cudaSuccess;
-  std::call_once(once, [&] { attr = cudaFuncSetAttribute(k_ebe3e_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn); });
-  if (attr != cudaSuccess) return fem_after_launch("k_ebe3e_apply attribute");
+  // the shared-memory limit is a per-device function attribute: set once per device
+  static std::mutex mu;
+  static unsigned long long done = 0ull;  // bit d: set on device d (devices 0..63)
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fem_after_launch("cudaGetDevice");
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
+    if (!(done & bit)) {
+      if (cudaFuncSetAttribute(k_ebe3e_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess)
+        return fem_after_launch("k_ebe3e_apply attribute");
+      done |= bit;
+    }
+  }
   k_ebe3e_apply<<<grid, FEM_THREADS, dyn, s>>>(g, m, x, y);
   return fem_after_launch("k_ebe3e_apply");
 }
